@@ -1,0 +1,194 @@
+"""Generate the golden fixtures in this folder from the runnable Python reference.
+
+Run in a checkout that has the pySTAMPS reference importable (its path is given
+with --reference); the fixtures are committed so the tests never need it:
+
+    python tests/golden/make_golden.py --reference /path/to/pystamps
+
+Fixtures (all seeded):
+
+* clap_grid.npz       -- pystamps.pipeline.ported._clap_filt_grid_stack_prepared
+                         on the 37x53x3 grid of the reference's own CLAP test
+                         (tests/test_stage2_ported.py:910-960) and on a 64x64x4
+                         grid with the stage-2 Butterworth low pass; complex64
+                         and preserve_precision (complex128) outputs.
+* topofit_rows.npz    -- ported._ps_topofit_single in complex128 on 96 random
+                         rows of 20 interferograms (row-variant bperp), with the
+                         number of near-max candidates per row so the test can
+                         skip rows where the Python near-max rule (tolerance
+                         2e-4) differs from the Rust first-argmax rule.
+* stage2_iter1.npz    -- ported.stage2_estimate_gamma(kernel_backend="python")
+                         on a 3,000 PS x 10 ifg synthetic patch, one iteration
+                         (gamma_max_iterations=1, so the random-phase histogram
+                         does not enter), written as pm1.mat and re-read.
+* stage2_3ps.npz      -- the same entry point on the reference's 3-PS fixture
+                         (native_stage2.rs:2698-2769: empty CLAP, all rows
+                         invalid).
+"""
+from __future__ import annotations
+
+import argparse
+import math
+import os
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+
+
+def _import_reference(ref: Path):
+    sys.path.insert(0, str(ref))
+    from pystamps.pipeline import ported  # noqa: E402
+
+    return ported
+
+
+def make_clap(ported) -> None:
+    rng = np.random.default_rng(0)
+    g1 = (rng.standard_normal((37, 53, 3)) + 1j * rng.standard_normal((37, 53, 3))).astype(np.complex64)
+    lp1 = np.full((32, 32), 0.01, dtype=np.float64)
+    prep1 = ported._prepare_clap_filt_grid_stack(g1.shape, n_win=24, n_pad=8, low_pass=lp1)
+    o1 = ported._clap_filt_grid_stack_prepared(g1, alpha=1.0, beta=0.3, prepared=prep1)
+    o1d = ported._clap_filt_grid_stack_prepared(g1, alpha=1.0, beta=0.3, prepared=prep1, preserve_precision=True)
+
+    rng = np.random.default_rng(11)
+    ph = np.exp(1j * rng.uniform(-np.pi, np.pi, (64, 64, 4)))
+    amp = rng.uniform(0.0, 3.0, (64, 64, 1))
+    g2 = (ph * amp).astype(np.complex64)
+    g2[5, 7, :] = 0
+    opts = ported.StageOptions() if hasattr(ported, "StageOptions") else None
+    n_win = 32
+    freq0 = 1.0 / 800.0
+    freq_i = np.arange(-n_win / 2, n_win / 2) / float(50.0 * n_win)
+    butter = 1.0 / (1.0 + (freq_i / freq0) ** (2 * 5))
+    lp2 = np.fft.fftshift(np.outer(butter, butter)).astype(np.float64)
+    del opts
+    prep2 = ported._prepare_clap_filt_grid_stack(g2.shape, n_win=24, n_pad=8, low_pass=lp2)
+    o2 = ported._clap_filt_grid_stack_prepared(g2, alpha=1.0, beta=0.3, prepared=prep2)
+    o2d = ported._clap_filt_grid_stack_prepared(g2, alpha=1.0, beta=0.3, prepared=prep2, preserve_precision=True)
+    # alpha != 1 exercises the powf branch
+    o3 = ported._clap_filt_grid_stack_prepared(g2, alpha=1.7, beta=0.45, prepared=prep2, preserve_precision=True)
+    np.savez_compressed(
+        HERE / "clap_grid.npz",
+        g1=g1, lp1=lp1, out1=o1, out1_f64=o1d,
+        g2=g2, lp2=lp2, out2=o2, out2_f64=o2d, out3_f64=o3,
+    )
+
+
+def make_topofit(ported) -> None:
+    rng = np.random.default_rng(21)
+    n_row, n_col = 96, 20
+    bp_ifg = rng.uniform(-300, 300, n_col)
+    grad = 1.0 + 0.02 * rng.uniform(-0.5, 0.5, n_row)
+    bperp = (grad[:, None] * bp_ifg[None, :]).astype(np.float64)
+    n_trial_wraps = 4.94
+    k_true = rng.uniform(-0.04, 0.04, n_row)
+    noise = rng.normal(0.0, rng.uniform(0.1, 1.5, n_row)[:, None], (n_row, n_col))
+    cpx = np.exp(1j * (k_true[:, None] * bperp + noise)) * rng.uniform(0.5, 1.5, (n_row, n_col))
+    cpx = cpx.astype(np.complex128)
+    K = np.empty(n_row); C = np.empty(n_row); coh = np.empty(n_row)
+    res = np.empty((n_row, n_col), np.complex128)
+    n_cand = np.empty(n_row, np.int64)
+    for r in range(n_row):
+        k, c, h, pr = ported._ps_topofit_single(cpx[r], bperp[r], n_trial_wraps)
+        K[r], C[r], coh[r] = k, c, h
+        res[r] = pr
+        # count near-max candidates exactly as the Python rule does
+        bp = bperp[r]
+        rngb = float(bp.max() - bp.min()) or 1.0
+        tm = ported._stage2_trial_values(n_trial_wraps)
+        tp = bp / rngb * (np.pi / 4.0)
+        ct = np.abs(np.sum(np.exp(-1j * (tp[:, None] * tm[None, :])) * cpx[r][:, None], axis=0))
+        ct = ct / np.sum(np.abs(cpx[r]))
+        n_cand[r] = ported._ps_topofit_near_max_trial_indices(ct).size
+    np.savez_compressed(HERE / "topofit_rows.npz", cpx=cpx, bperp=bperp, n_trial_wraps=n_trial_wraps,
+                        K=K, C=C, coh=coh, residual=res, n_candidates=n_cand)
+
+
+def _write_patch(ported, patch: Path, p: dict) -> None:
+    from scipy.io import savemat
+
+    patch.mkdir(parents=True, exist_ok=True)
+    n_ps, n_full = p["ph"].shape
+    savemat(patch / "ps1.mat", {
+        "n_ps": float(n_ps), "n_ifg": float(n_full), "n_image": float(n_full), "master_ix": float(p["master_ix"]),
+        "bperp": p["bperp"].reshape(1, -1), "xy": p["xy"], "mean_incidence": float(p["mean_incidence"]),
+    })
+    savemat(patch / "ph1.mat", {"ph": p["ph"]})
+    if p.get("bperp_mat") is not None:
+        savemat(patch / "bp1.mat", {"bperp_mat": np.asarray(p["bperp_mat"], dtype=np.float64)})
+    if p.get("D_A") is not None:
+        savemat(patch / "da1.mat", {"D_A": np.asarray(p["D_A"], dtype=np.float64).reshape(-1, 1)})
+    if p.get("inc") is not None:
+        savemat(patch / "inc1.mat", {"inc": np.asarray(p["inc"], dtype=np.float64).reshape(-1, 1)})
+    if p.get("la") is not None:
+        savemat(patch / "la1.mat", {"la": np.asarray(p["la"], dtype=np.float64).reshape(-1, 1)})
+    savemat(patch / "parms.mat", p["parms"])
+
+
+def _run_python_stage2(ported, p: dict) -> dict:
+    from scipy.io import loadmat
+
+    with tempfile.TemporaryDirectory() as tmp:
+        os.environ["HOME"] = tmp  # the reference caches its random histogram under ~/.cache
+        patch = Path(tmp) / "PATCH_1"
+        _write_patch(ported, patch, p)
+        ported.stage2_estimate_gamma(patch, kernel_backend="python")
+        pm = loadmat(patch / "pm1.mat")
+    keys = ["K_ps", "C_ps", "coh_ps", "N_opt", "ph_res", "ph_patch", "ph_grid", "ph_weight", "grid_ij",
+            "n_trial_wraps", "i_loop", "coh_ps_save", "gamma_change_save", "low_pass", "grid_size"]
+    return {k: np.asarray(pm[k]) for k in keys if k in pm}
+
+
+def make_stage2_iter1(ported) -> None:
+    sys.path.insert(0, str(HERE.parents[1]))
+    from pystamps_b200 import synth
+
+    p = synth.make_patch(3000, 10, 31, 21, seed=777, max_topo_err=20.0, gamma_max_iterations=1)
+    p["inc"] = np.full(p["ph"].shape[0], p["mean_incidence"])
+    pm = _run_python_stage2(ported, p)
+    np.savez_compressed(
+        HERE / "stage2_iter1.npz",
+        ph=p["ph"], bperp=p["bperp"], bperp_mat=p["bperp_mat"], D_A=p["D_A"], xy=p["xy"],
+        mean_incidence=p["mean_incidence"], max_topo_err=20.0,
+        **{"pm_" + k: v for k, v in pm.items()},
+    )
+
+
+def make_stage2_3ps(ported) -> None:
+    inc = math.radians(23.0)
+    p = {
+        "ph": np.asarray([[1.0, 0.8 + 0.2j, 0.6 + 0.4j], [1.0, 0.7 + 0.3j, 0.5 + 0.5j], [1.0, 0.9 + 0.1j, 0.4 + 0.6j]],
+                         dtype=np.complex64),
+        "bperp": np.asarray([0.0, 15.0, 30.0]),
+        "master_ix": 1,
+        "bperp_mat": np.asarray([[15.0, 30.0]] * 3),
+        "D_A": np.ones(3),
+        "xy": np.asarray([[1, 0, 0], [2, 5, 5], [3, 10, 10]], dtype=np.float32),
+        "mean_incidence": inc,
+        "la": np.full(3, inc),
+        "parms": {"gamma_max_iterations": 1.0, "filter_grid_size": 50.0},
+    }
+    pm = _run_python_stage2(ported, p)
+    np.savez_compressed(HERE / "stage2_3ps.npz", **{"pm_" + k: v for k, v in pm.items()})
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", required=True, type=Path)
+    ap.add_argument("--only", default="")
+    a = ap.parse_args()
+    ported = _import_reference(a.reference)
+    todo = {"clap": make_clap, "topofit": make_topofit, "iter1": make_stage2_iter1, "3ps": make_stage2_3ps}
+    for name, fn in todo.items():
+        if a.only and name not in a.only.split(","):
+            continue
+        fn(ported)
+        print("wrote", name)
+
+
+if __name__ == "__main__":
+    main()
