@@ -1,0 +1,387 @@
+"""Benchmark: stage-2 PS x ifg per second per gamma iteration on B200.
+
+Workload: the full-scale stage-2 patch (2,000,000 PS candidates, 150
+interferograms, 256x256 grid at 50 m, 161 trial multipliers), seeded synthetic
+data from pystamps_b200.synth. One step = one gamma iteration (bin -> CLAP ->
+resample -> topofit -> convergence / P-square update) over the whole patch.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank runs its own replica of the patch (the
+single-patch path has no cross-GPU exchange; weak scaling), the timed region is
+bracketed by barriers and the max over ranks is reported by rank 0.
+
+value  : device-resident inputs, K iterations timed with CUDA events on the
+         library's stream, N_ps * N_ifg * K / t (whole job: summed over ranks).
+e2e    : one public-API stage-2 run per step from pinned host buffers (upload,
+         layout, iterate to convergence, download of K/C/coh/N_opt), metric =
+         N_ps * N_ifg * iterations / t.
+--impl reference : the CPU restatement of the reference's native stage 2 on all
+         host cores, a bounded sample per step (see cpu_baseline.sample).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Stage-2 PS×ifg/s per gamma iter, FP32 vs plain FP64 GPU at max|Δγ|≤1e-4"
+UNIT = "PS*ifg/s"
+FP32_LANES_PER_SM = 128
+# DRAM bytes per topofit launch from the committed ncu capture (profiles/), scaled
+# to the full-scale workload; None until measured.
+TOPOFIT_TRAFFIC_BYTES = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="E", help="A, B, D or E (default E, the full-scale patch)")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- clocks ----
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------- workload -----
+def make_workload(name: str, rank: int):
+    from pystamps_b200 import synth
+
+    w = synth.ALIASES.get(name) or synth.WORKLOADS[name]
+    patch = synth.make_workload(w, patch_id=rank)
+    return w, patch
+
+
+def load_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0, "fallback": True}
+
+
+# ------------------------------------------------------------ CPU leg -------
+def cpu_sample(w, patch, prep, rows: int = 20_000, ifgs_clap: int = 4, threads: int = 0) -> dict:
+    """Per-iteration time of the oracle (CPU restatement of the reference's
+    native stage 2) on the full workload, from a bounded sample: the row-wise
+    steps (fill, bin, extract, topofit) on `rows` PS x all ifgs, scaled by
+    N_ps / rows, plus CLAP on the full grid for `ifgs_clap` ifgs, scaled by
+    N_ifg / ifgs_clap."""
+    from oracle import oracle as O
+
+    n, m = prep.n_ps, prep.n_ifg
+    rows = min(rows, n)
+    sub = slice(0, rows)
+    ph_nm = np.ascontiguousarray(prep.ph_nm[sub])
+    bp = prep.bperp.astype(np.float64) if prep.row_invariant else np.ascontiguousarray(prep.bperp[sub], dtype=np.float64)
+    k = np.zeros(rows)
+    wv = np.ascontiguousarray(prep.weight0[sub])
+    gl = prep.grid_lin[sub]
+    t0 = time.perf_counter()
+    pw = O.fill_phase_weight(ph_nm, bp, k, wv, threads=threads)
+    grid = O.accumulate_grid(pw, gl, prep.n_i, prep.n_j)
+    patch_ph = O.extract_patch_phase(grid, gl, threads=threads)  # stands in for the filtered grid (same access)
+    O.fit_rows(patch_ph, ph_nm, bp, prep.n_trial_wraps, threads=threads)
+    t_rows = time.perf_counter() - t0
+    rng = np.random.default_rng(0)
+    g = (rng.standard_normal((prep.n_i, prep.n_j, ifgs_clap)) +
+         1j * rng.standard_normal((prep.n_i, prep.n_j, ifgs_clap))).astype(np.complex64)
+    t0 = time.perf_counter()
+    O.clap_filter_grid_stack(g, prep.clap_alpha, prep.clap_beta, prep.low_pass, n_win=prep.clap_window,
+                             threads=threads)
+    t_clap = time.perf_counter() - t0
+    t_iter = t_rows * (n / rows) + t_clap * (m / ifgs_clap)
+    return {"t_iter_s": t_iter, "t_rows_s": t_rows, "t_clap_s": t_clap, "rows": rows, "ifgs_clap": ifgs_clap,
+            "value": n * m / t_iter}
+
+
+def ncores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    from pystamps_b200 import stage2 as S
+
+    w, patch = make_workload(args.workload, 0)
+    prep = S.prepare_patch(patch, nr=np.ones(100), nr_max_nz_ix=100.0)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_sample(w, patch, prep)
+        if i >= args.warmup:
+            vals.append(r)
+    v = statistics.median([r["value"] for r in vals])
+    t_iter = statistics.median([r["t_iter_s"] for r in vals])
+    sample = (f"per step: oracle fill+bin+extract+topofit on {vals[0]['rows']} of {prep.n_ps} PS x {prep.n_ifg} ifg "
+              f"(scaled x{prep.n_ps / vals[0]['rows']:.0f}) + CLAP on the full {prep.n_i}x{prep.n_j} grid for "
+              f"{vals[0]['ifgs_clap']} of {prep.n_ifg} ifg (scaled x{prep.n_ifg / vals[0]['ifgs_clap']:.1f})")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_iter * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, pystamps_b200.synth)",
+        "config": {"workload": w.name, "n_ps": prep.n_ps, "n_ifg": prep.n_ifg, "grid": [prep.n_i, prep.n_j],
+                   "trials": 2 * math.ceil(8 * prep.n_trial_wraps) + 1},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": ncores(), "kind": "port", "sample": sample,
+                         "what": "C++ restatement of crates/pystamps-core/src/native_stage2.rs (Rust toolchain absent)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------- GPU leg ------
+def run_ours(args, rank: int, world: int, dist):
+    import torch
+
+    from pystamps_b200 import stage2 as S
+    from pystamps_b200 import _lib
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    w, patch = make_workload(args.workload, rank)
+    t0 = time.perf_counter()
+    prep = S.prepare_patch(patch)
+    t_prep = time.perf_counter() - t0
+    inc = float(patch["mean_incidence"])
+    lam = float(patch["parms"].get("lambda", 0.0555))
+    del patch
+    n, m = prep.n_ps, prep.n_ifg
+    T = 2 * math.ceil(8 * prep.n_trial_wraps) + 1
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    # ---------------- value: device-resident inputs -------------------------
+    ctx = S.Stage2Context(dev)
+    ctx.load(prep, "fp32")
+    ctx.iterate(max(args.warmup, 1))
+    barrier()
+    clk = ClockSampler(dev)
+    clk.start()
+    ctx.iterate(args.steps)
+    total_ms, per = ctx.timing()
+    launches = ctx.launch_count()
+    clocks = clk.stop()
+    barrier()
+    t_max = total_ms
+    if dist is not None:
+        tt = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    value = world * n * m * args.steps / (t_max / 1e3)
+    ms_per_step = t_max / args.steps
+    topo_ms = per[2] / args.steps
+    bin_ms = per[0] / args.steps
+    clap_ms = per[1] / args.steps
+    # roofline of the dominant kernel (topofit): algorithmic flops per launch
+    flops = (8 * T + 32) * n * m
+    sm_max = float(load_peaks().get("sm_max_mhz", 1965.0))
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    fp32_peak_tflops = 2 * FP32_LANES_PER_SM * sms * sm_max * 1e6 / 1e12
+    achieved = flops / (topo_ms / 1e3) / 1e12
+    peaks = load_peaks()
+    bin_bytes = n * m * (8 + (0 if prep.row_invariant else 4)) + prep.n_i * prep.n_j * m * 8
+    roofline = {
+        "kernel": "k_topofit_f32", "bound": "fp32", "achieved": achieved, "peak": fp32_peak_tflops,
+        "unit": "TFLOP/s", "frac": achieved / fp32_peak_tflops,
+        "traffic": TOPOFIT_TRAFFIC_BYTES,
+        "algorithmic": f"(8*T+32) flop per PS x ifg, T={T}: {flops:.3e} flop per launch",
+        "peak_source": f"nominal FP32 FMA rate {sms} SM x {FP32_LANES_PER_SM} lanes x 2 x {sm_max:.0f} MHz "
+                       "(MEASURED_PEAKS.json has no FP32 figure)",
+        "share_of_step": topo_ms / ms_per_step,
+    }
+    bin_roof = {"kernel": "k_bin", "bound": "hbm", "achieved": bin_bytes / (bin_ms / 1e3) / 1e9,
+                "peak": float(peaks.get("hbm_gbs", 6650.0)), "unit": "GB/s",
+                "frac": bin_bytes / (bin_ms / 1e3) / 1e9 / float(peaks.get("hbm_gbs", 6650.0)),
+                "algorithmic": "12 B per PS x ifg (ph_nm c64 + bperp f32) + 8 B per cell x ifg"}
+    ctx.close()
+
+    # ---------------- plain FP64 GPU path ------------------------------------
+    fp64 = None
+    if not args.no_fp64:
+        c64 = S.Stage2Context(dev)
+        c64.load(prep, "fp64")
+        c64.iterate(1)
+        k64 = 2
+        c64.iterate(k64)
+        t64, per64 = c64.timing()
+        fp64 = {"value": world * n * m * k64 / (t64 / 1e3), "ms_per_step": t64 / k64,
+                "topofit_ms": per64[2] / k64}
+        c64.close()
+
+    # ---------------- e2e: public API from pinned host buffers ---------------
+    pin = {}
+    for name, arr in (("ph_nm", prep.ph_nm), ("bperp", prep.bperp), ("grid_lin", prep.grid_lin),
+                      ("weight0", prep.weight0)):
+        t = torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()
+        pin[name] = t.numpy()
+    import dataclasses
+
+    prep_pinned = dataclasses.replace(prep, **pin)
+    h2d = (prep.ph_nm.nbytes + prep.bperp.nbytes + prep.grid_lin.nbytes + prep.weight0.nbytes +
+           prep.low_pass.nbytes + prep.nr.nbytes)
+    d2h = 4 * n * 8
+    e2e_vals, iters = [], []
+    ectx = S.Stage2Context(dev)
+    for i in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
+        barrier()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        tw = time.perf_counter()
+        ev0.record()
+        ectx.load(prep_pinned, "fp32")
+        st = ectx.run()
+        out = ectx.download(["K_ps", "C_ps", "coh_ps", "N_opt"])
+        ev1.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - tw
+        if i == 0:
+            continue  # warm-up
+        t = max(ev0.elapsed_time(ev1) / 1e3, wall)
+        if dist is not None:
+            tt = torch.tensor([t], dtype=torch.float64, device=f"cuda:{dev}")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        e2e_vals.append(world * n * m * st["i_loop"] / t)
+        iters.append(st["i_loop"])
+    ectx.close()
+    e2e = None if not e2e_vals else {"value": statistics.median(e2e_vals), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "iterations_per_step": iters,
+           "what": "per step: ps2_load_patch (H2D + cell layout) + ps2_run_to_convergence + ps2_download(K,C,coh,N_opt)"}
+
+    # ---------------- precision vs the plain FP64 path -----------------------
+    prec = None
+    if fp64 is not None:
+        a = S.run_stage2(prep, precision="fp32", keys=["coh_ps", "K_ps"])
+        b = S.run_stage2(prep, precision="fp64", keys=["coh_ps", "K_ps"])
+        d = np.abs(a["coh_ps"] - b["coh_ps"])
+        kconv = lam * 830_000.0 * math.sin(inc) / (4 * math.pi)  # rad/m -> m of DEM error
+        dk = np.abs(a["K_ps"] - b["K_ps"]) * kconv
+        prec = {"iterations_fp32": a["i_loop"], "iterations_fp64": b["i_loop"],
+                "dgamma_median": float(np.median(d)), "dgamma_p99": float(np.quantile(d, 0.99)),
+                "dgamma_max": float(d.max()), "dK_m_median": float(np.nanmedian(dk)),
+                "dK_m_p99": float(np.nanquantile(dk, 0.99))}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        r = cpu_sample(w, None, prep)
+        cpu = {"value": r["value"], "unit": UNIT, "cores": ncores(), "kind": "port",
+               "sample": f"oracle row steps on {r['rows']} PS x {m} ifg scaled x{n / r['rows']:.0f} + CLAP on the "
+                         f"full grid for {r['ifgs_clap']} ifg scaled x{m / r['ifgs_clap']:.1f}; "
+                         f"t_iter={r['t_iter_s']:.2f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator pystamps_b200.synth)",
+            "config": {"workload": w.name, "n_ps": n, "n_ifg": m, "grid": [prep.n_i, prep.n_j], "trials": T,
+                       "l2": f"inputs larger than L2 (ph_nm {prep.ph_nm.nbytes / 1e9:.2f} GB per step)",
+                       "per_kernel_ms": {"bin": bin_ms, "clap": clap_ms, "topofit": topo_ms,
+                                         "finalize": per[3] / args.steps},
+                       "prepare_s": t_prep, "parallelism": f"replicas x{world}"},
+            "roofline": roofline, "roofline_bin": bin_roof, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clocks, "fp64_gpu": fp64,
+            "fp32_over_fp64": (value / fp64["value"]) if fp64 else None, "precision_vs_fp64": prec,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        dist = tdist
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

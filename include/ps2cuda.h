@@ -1,0 +1,156 @@
+/*
+ * ps2cuda — B200 (sm_100a) stage-2 gamma estimation for pySTAMPS
+ * (the StaMPS ps_est_gamma_quick loop: bin -> CLAP -> resample -> topofit ->
+ * gamma convergence).
+ *
+ * Plain C ABI: host or device pointers and sizes, no C++ or torch types.
+ * Every function returns 0 on success or a negative PS2_ERR_* code; the text
+ * of the last error of the calling thread is returned by ps2_last_error().
+ *
+ * Reference interfaces replaced (pySTAMPS, paths within that project):
+ *  - ps2_create / ps2_load_patch / ps2_run_to_convergence / ps2_download
+ *    replace the body of run_stage2_native_with_options
+ *    (crates/pystamps-core/src/native_stage2.rs:208-413): a Rust caller keeps
+ *    prepare_stage2_inputs (:415-561) and write_pm1 (:1899-1965) and calls
+ *    these in place of the gamma loop (:261-406). The dispatch point is
+ *    run_native_stage (2, Patch) in crates/pystamps-core/src/bin/pystamps-native.rs:198-201.
+ *  - ps2_grid_accumulate replaces accumulate_weighted_grid (src/lib.rs:1013-1087)
+ *    behind the Python registry kernel "stage2_grid_accumulate"
+ *    (pystamps/kernels/accelerated.py:410, 429-443).
+ *  - ps2_topofit replaces ps_topofit_batch_generic_f32 / _generic
+ *    (src/lib.rs:1159-1247) behind "stage2_topofit" (accelerated.py:411, 446-460)
+ *    with the native driver's first-argmax peak rule (native_stage2.rs:1207-1257).
+ *  - ps2_clap_filter_grid replaces clap_filter_grid_stack
+ *    (native_stage2.rs:742-922) / ported._clap_filt_grid_stack_prepared
+ *    (pystamps/pipeline/ported.py:1208-1298).
+ *  - ps2_random_coherence_histogram replaces random_coherence_histogram
+ *    (native_stage2.rs:1310-1512) / the "stage2_topofit_coh_row_invariant" +
+ *    "stage2_histogram" registry kernels (accelerated.py:414-427).
+ */
+#ifndef PS2CUDA_H
+#define PS2CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PS2_OK 0
+#define PS2_ERR_INVALID_ARG (-1)
+#define PS2_ERR_CUDA (-2)
+#define PS2_ERR_NOT_LOADED (-3)
+#define PS2_ERR_UNSUPPORTED (-4)
+#define PS2_ERR_OUT_OF_MEMORY (-5)
+
+#define PS2_PRECISION_FP32 0 /* FP32 compute, FP64 only in K refinement and weighting */
+#define PS2_PRECISION_FP64 1 /* plain FP64 everywhere (direct sincos, no recurrence) */
+
+#define PS2_COH_BINS 100
+
+typedef struct ps2_ctx ps2_ctx;
+
+/* Prepared stage-2 inputs (the output of prepare_stage2_inputs,
+ * native_stage2.rs:415-561). Row-major arrays; complex values are
+ * interleaved (re, im) float pairs. */
+typedef struct ps2_patch_desc {
+  int64_t n_ps;        /* PS candidates (rows) */
+  int64_t n_ifg;       /* non-master interferograms (columns) */
+  const float* ph_nm;  /* complex64 [n_ps, n_ifg], unit magnitude (0 stays 0) */
+  const float* amp;    /* NULL, or f32 [n_ps, n_ifg] magnitudes (SNR weighting only) */
+  const float* bperp;  /* f32 [n_ps, n_ifg], or [n_ifg] when bperp_row_invariant */
+  int32_t bperp_row_invariant;
+  const int64_t* grid_lin; /* [n_ps] 0-based cell (i-1)*n_j + (j-1) */
+  int64_t n_i, n_j;        /* grid cells */
+  const double* weight0;   /* [n_ps] initial weighting 1/D_A (0 where D_A == 0) */
+  const double* low_pass;  /* [n_win_ex * n_win_ex] Butterworth low pass (fftshifted) */
+  int64_t n_win_ex;        /* CLAP FFT size, round(clap_win) = 32 */
+  int64_t clap_window;     /* CLAP window, round(0.75 * clap_win) = 24 */
+  double clap_alpha, clap_beta;
+  double n_trial_wraps;    /* trials = -ceil(8*n)..ceil(8*n) */
+  const double* nr;        /* [PS2_COH_BINS] random-phase coherence histogram */
+  double nr_max_nz_ix;     /* 1-based index of the last non-zero Nr bin */
+  int64_t low_coh_thresh;  /* 31 (15 for small baselines) */
+  int32_t psquare;         /* 1: P-square weighting, 0: SNR weighting */
+  double gamma_change_convergence;
+  int64_t gamma_max_iterations;
+  int32_t precision;       /* PS2_PRECISION_* */
+  int32_t pointers_on_device; /* 1: the array pointers above are device pointers */
+} ps2_patch_desc;
+
+typedef struct ps2_iter_stats {
+  int64_t i_loop;            /* 1-based iteration that produced these numbers */
+  double gamma_change_rms;   /* sqrt(mean((coh - coh_prev)^2)) */
+  double gamma_change_delta; /* gamma_change_rms - previous gamma_change_rms */
+  int32_t stop;              /* convergence or iteration cap reached */
+  int32_t n_invalid;         /* rows with a zero element in conj(ph_patch)*ph_nm */
+} ps2_iter_stats;
+
+/* Host buffers for the pm1.mat variables (native_stage2.rs:1899-1965);
+ * NULL members are skipped. Row order is the caller's original PS order. */
+typedef struct ps2_outputs {
+  double* K_ps;        /* [n_ps] rad/m; NaN for invalid rows */
+  double* C_ps;        /* [n_ps] */
+  double* coh_ps;      /* [n_ps] */
+  double* N_opt;       /* [n_ps] */
+  float* ph_res;       /* [n_ps, n_ifg] */
+  float* ph_patch;     /* complex64 [n_ps, n_ifg] */
+  float* ph_grid;      /* complex64 [n_i, n_j, n_ifg] */
+  float* ph_weight;    /* complex64 [n_ps, n_ifg] */
+  double* coh_ps_save; /* [n_ps] */
+  double* Nr;          /* [PS2_COH_BINS] Nr as scaled by the last P-square update */
+  double* gamma_change_save;
+  int64_t* i_loop;
+  double* ph_res_f64;   /* FP64 precision only: [n_ps, n_ifg] */
+  double* ph_patch_f64; /* FP64 precision only: complex128 [n_ps, n_ifg] */
+  double* ph_grid_f64;  /* FP64 precision only: complex128 [n_i, n_j, n_ifg] */
+  double* ph_weight_f64;/* FP64 precision only: complex128 [n_ps, n_ifg] */
+} ps2_outputs;
+
+/* ---------------------------------------------------------- context API -- */
+int ps2_create(ps2_ctx** out, int device);
+void ps2_destroy(ps2_ctx* ctx);
+const char* ps2_last_error(void);
+/* Uploads and lays out one patch (cell-sorted rows). Copies the inputs; no
+ * caller pointer is retained after return. */
+int ps2_load_patch(ps2_ctx* ctx, const ps2_patch_desc* desc);
+/* Runs n_iter gamma iterations whatever the convergence test says (for
+ * timing); stats may be NULL or hold n_iter entries. */
+int ps2_iterate(ps2_ctx* ctx, int64_t n_iter, ps2_iter_stats* stats);
+/* Runs iterations until the reference's stop rule holds
+ * (|delta gamma_change| < gamma_change_convergence or i_loop >= max). */
+int ps2_run_to_convergence(ps2_ctx* ctx, ps2_iter_stats* last);
+/* Resets the loop state of the loaded patch to iteration 1 (K=0, w=weight0). */
+int ps2_reset(ps2_ctx* ctx);
+int ps2_download(ps2_ctx* ctx, ps2_outputs* out);
+/* Device time in milliseconds (CUDA events on the context's stream) of the
+ * last ps2_iterate call from its first launch to its last (for
+ * ps2_run_to_convergence: the sum of the iterations), and the summed time of
+ * each kernel family in it: [0] binning, [1] CLAP windows + overlap-add,
+ * [2] topofit, [3] convergence / weighting update. */
+int ps2_last_timing(const ps2_ctx* ctx, double* total_ms, double* per_kernel_ms /*[4] or NULL*/);
+/* Number of kernel launches issued by the last iterate/run call. */
+int64_t ps2_last_launch_count(const ps2_ctx* ctx);
+
+/* ------------------------------------------------- stateless kernels ---- */
+/* All pointers are host pointers unless stated otherwise. */
+int ps2_grid_accumulate(const float* ph_weight, const int64_t* grid_lin, int64_t n_ps, int64_t n_ifg, int64_t n_i,
+                        int64_t n_j, float* out /* complex64 [n_i, n_j, n_ifg] */);
+int ps2_topofit(const float* cpxphase /* complex64 [n, m] */, const float* bperp /* [n, m] or [m] */,
+                int32_t bperp_row_invariant, double n_trial_wraps, int64_t n, int64_t m, double* K, double* C,
+                double* coh, float* residual /* complex64 [n, m] or NULL */);
+int ps2_clap_filter_grid(const float* ph_grid /* complex64 [n_i, n_j, m] */, int64_t n_i, int64_t n_j, int64_t m,
+                         int64_t clap_window, double alpha, double beta, const double* low_pass, int64_t n_win_ex,
+                         float* out /* complex64 [n_i, n_j, m] */);
+/* Setup histogram of the coherence of 300,000 (n_rand) random-phase rows, in
+ * FP64 on the GPU; the MATLAB v5 uniform generator (seed 2005) runs on the
+ * host. ifgday_ix ([n_ifg, 2], 1-based) and n_image are used only when
+ * small_baseline != 0. */
+int ps2_random_coherence_histogram(const double* bperp_nm, int64_t n_ifg, double n_trial_wraps, int64_t n_rand,
+                                   int32_t small_baseline, const int64_t* ifgday_ix, int64_t n_image,
+                                   double* nr_out /* [PS2_COH_BINS] */, double* nr_max_nz_ix);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PS2CUDA_H */

@@ -1,0 +1,1065 @@
+// Host side of libps2cuda: the stage-2 context (device-resident patch, the
+// gamma loop driver) and the C ABI declared in include/ps2cuda.h.
+//
+// Layout in HBM (per loaded patch; N PS, M interferograms, G = n_i*n_j cells,
+// Mp = M rounded up to a multiple of 4, W CLAP windows):
+//   ph_nm   complex64 [N, M]   rows stably sorted by grid cell (counting sort)
+//   bp      f32 [N, M] sorted (or [M] when every row has the same baselines)
+//   K[2]    real [N]           ping-pong: K used by this iteration's binning /
+//                              K written by this iteration's topofit
+//   w, coh, C                  real [N], nopt u8 [N]
+//   grid    complex [G, Mp]    binned phase (the reference's ph_grid)
+//   win     complex [W, 576, Mp] weighted CLAP window outputs
+//   filt    complex [G, Mp]    CLAP-filtered grid
+// Real/complex are f32/complex64 for PS2_PRECISION_FP32 and f64/complex128
+// for PS2_PRECISION_FP64.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ps2cuda.h"
+#include "interp10_taps.h"
+#include "ps2_kernels.cuh"
+
+using namespace ps2;
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(call)                                                                                              \
+  do {                                                                                                        \
+    cudaError_t e__ = (call);                                                                                 \
+    if (e__ != cudaSuccess) {                                                                                 \
+      return set_err(e__ == cudaErrorMemoryAllocation ? PS2_ERR_OUT_OF_MEMORY : PS2_ERR_CUDA, "%s: %s (%s:%d)", \
+                     #call, cudaGetErrorString(e__), __FILE__, __LINE__);                                     \
+    }                                                                                                         \
+  } while (0)
+
+// Device allocation owned by a context.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  cudaError_t alloc(size_t n) {
+    release();
+    if (n == 0) n = 16;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e == cudaSuccess) bytes = n;
+    else p = nullptr;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <typename T>
+  T* as() const { return static_cast<T*>(p); }
+};
+
+// MATLAB rand('state', seed) / v5 uniform generator (native_stage2.rs:1785-1873):
+// 32-word subtract-with-borrow lagged-Fibonacci state, xorshift-32 mantissa
+// scrambling of the 53-bit result.
+class V5Uniform {
+ public:
+  explicit V5Uniform(uint32_t seed) : j_(seed == 0 ? (1u << 31) : seed) {
+    uint32_t s = j_;
+    for (int k = 0; k < 32; ++k) {
+      uint64_t x = 0;
+      for (int b = 0; b < 53; ++b) {
+        s = xs32(s);
+        x = (x << 1) | ((s >> 19) & 1u);
+      }
+      st_[k] = static_cast<double>(x) * kUlp;
+    }
+  }
+  double next() {
+    double v = st_[(ix_ + 20) & 31] - st_[(ix_ + 5) & 31] - borrow_;
+    if (v < 0.0) {
+      v += 1.0;
+      borrow_ = kUlp;
+    } else {
+      borrow_ = 0.0;
+    }
+    st_[ix_] = v;
+    ix_ = (ix_ + 1) & 31;
+    const uint32_t lo = j_, hi = xs32(lo);
+    j_ = hi;
+    const uint64_t mask = ((static_cast<uint64_t>(hi) << 32) & ((uint64_t(1) << 52) - 1)) ^ lo;
+    if (v == 0.0) return std::ldexp(static_cast<double>(mask), -53);
+    uint64_t bits;
+    std::memcpy(&bits, &v, 8);
+    const int eb = static_cast<int>((bits >> 52) & 0x7ff);
+    uint64_t mant = bits & ((uint64_t(1) << 52) - 1);
+    int ex;
+    if (eb == 0) {
+      const int lead = 63 - __builtin_clzll(mant);
+      ex = lead - 1073;
+      mant <<= (52 - lead);
+    } else {
+      ex = eb - 1022;
+      mant |= (uint64_t(1) << 52);
+    }
+    return std::ldexp(static_cast<double>(mant ^ mask), ex - 53);
+  }
+
+ private:
+  static constexpr double kUlp = 1.1102230246251565e-16;  // 2^-53
+  static uint32_t xs32(uint32_t v) {
+    v ^= v << 13;
+    v ^= v >> 17;
+    v ^= v << 5;
+    return v;
+  }
+  double st_[32];
+  int ix_ = 0;
+  double borrow_ = 0.0;
+  uint32_t j_;
+};
+
+void coh_bin_rule(double* cutoff0, double* d) {
+  // centres 0.005 + 0.01*i (native_stage2.rs:510-512), equal-spacing rule (:1593-1607)
+  const double c0 = 0.005 + 0.01 * 0.0, c1 = 0.005 + 0.01 * 1.0, c99 = 0.005 + 0.01 * 99.0;
+  *d = (c99 - c0) / 99.0;
+  *cutoff0 = (c0 + c1) / 2.0;
+}
+
+void gauss7(double* g, double* sum) {
+  // gausswin(7, 2.5) (native_stage2.rs:1685-1699); the same values are the
+  // CLAP |H| smoothing taps (:1044-1053)
+  const double sd = (7.0 - 1.0) / (2.0 * 2.5);
+  double s = 0.0;
+  for (int i = 0; i < 7; ++i) {
+    const double x = static_cast<double>(i) - 3.0;
+    g[i] = std::exp(-0.5 * (x / sd) * (x / sd));
+    s += g[i];
+  }
+  if (sum) *sum = s;
+}
+
+void twiddles(Twiddles32f* tf, Twiddles32d* td) {
+  for (int k = 0; k < 16; ++k) {
+    const double a = -2.0 * M_PI * k / 32.0;
+    td->w[k] = make_double2(std::cos(a), std::sin(a));
+    tf->w[k] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(std::sin(a)));
+  }
+}
+
+// pyramid overlap weight (clap_window_weight, native_stage2.rs:1014-1037) / n_ex^2
+std::vector<double> window_weight_scaled(int n_win, int n_ex) {
+  const int h = n_win / 2;
+  std::vector<double> out(static_cast<size_t>(n_win) * n_win, 0.0);
+  for (int r = 0; r < h; ++r)
+    for (int c = 0; c < h; ++c) {
+      out[r * n_win + c] = static_cast<double>(r) + static_cast<double>(c) + 1.0e-6;
+      out[r * n_win + h + c] = static_cast<double>(r) + static_cast<double>(h - 1 - c) + 1.0e-6;
+    }
+  for (int r = 0; r < h; ++r)
+    for (int c = 0; c < n_win; ++c) out[(h + r) * n_win + c] = out[(h - 1 - r) * n_win + c];
+  const double inv = 1.0 / static_cast<double>(n_ex * n_ex);
+  for (auto& v : out) v *= inv;
+  return out;
+}
+
+}  // namespace
+
+struct ps2_ctx {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t st = nullptr;
+  bool loaded = false;
+  bool fp64 = false;
+  int64_t N = 0, G = 0;
+  int M = 0, Mp = 0, n_i = 0, n_j = 0, n_win = 24, n_inc = 6, nwi = 0, nwj = 0, nchunk = 0, n_half = 0;
+  int bp_row_inv = 0, psquare = 1, low_coh_thresh = 31, alpha_is_one = 1;
+  double alpha = 1.0, beta = 0.3, conv = 0.005, nr_max_nz_ix = 1.0;
+  int64_t max_iter = 25;
+  double cutoff0 = 0.01, dbin = 0.01;
+  double g7[7], g7sum = 0.0;
+  Twiddles32f twf;
+  Twiddles32d twd;
+  DevBuf ph_nm, bp, amp, perm, cell_start, cell_of, w0, K[2], w, coh, C, nopt, grid, win, filt, low_pass, wscaled,
+      taps, lut, nr0, nr_scaled, state, stats, hist, n_invalid, rms_partial, ph_res, scratch;
+  int kcur = 0;
+  int topo_blocks = 0;
+  int64_t iters_done = 0;  // since load/reset
+  double* h_stats = nullptr;  // pinned [8]
+  ps2_iter_stats last{};
+  double last_ms = 0.0, kernel_ms[4] = {0, 0, 0, 0};
+  int64_t launches = 0;
+  std::vector<cudaEvent_t> evpool;
+};
+
+namespace {
+
+size_t rsz(const ps2_ctx* c) { return c->fp64 ? sizeof(double) : sizeof(float); }
+size_t csz(const ps2_ctx* c) { return 2 * rsz(c); }
+
+int ensure_events(ps2_ctx* c, size_t n) {
+  while (c->evpool.size() < n) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    c->evpool.push_back(e);
+  }
+  return PS2_OK;
+}
+
+BinArgs bin_args(ps2_ctx* c, int mode, const void* K) {
+  BinArgs a{};
+  a.ph_nm = c->ph_nm.p;
+  a.bp = c->bp.as<float>();
+  a.bp_row_inv = c->bp_row_inv;
+  a.cell_start = c->cell_start.as<int32_t>();
+  a.G = c->G;
+  a.M = c->M;
+  a.Mp = c->Mp;
+  a.nchunk = c->nchunk;
+  a.K = K;
+  a.w = c->w.p;
+  a.coh = c->coh.p;
+  a.lut = c->lut.as<double>();
+  a.lut_len = 1001;
+  a.mode = mode;
+  a.grid = c->grid.p;
+  return a;
+}
+
+ClapArgs clap_args(ps2_ctx* c, const void* grid, void* win) {
+  ClapArgs a{};
+  a.grid = grid;
+  a.n_i = c->n_i;
+  a.n_j = c->n_j;
+  a.M = c->M;
+  a.Mp = c->Mp;
+  a.n_win = c->n_win;
+  a.nwi = c->nwi;
+  a.nwj = c->nwj;
+  a.alpha_is_one = c->alpha_is_one;
+  a.alpha = c->alpha;
+  a.beta = c->beta;
+  a.low_pass = c->low_pass.as<double>();
+  a.wscaled = c->wscaled.as<double>();
+  for (int i = 0; i < 7; ++i) a.g7[i] = c->g7[i];
+  a.win_out = win;
+  return a;
+}
+
+OverlapArgs overlap_args(ps2_ctx* c, const void* win, void* filt) {
+  OverlapArgs o{};
+  o.win_out = win;
+  o.filt = filt;
+  o.n_i = c->n_i;
+  o.n_j = c->n_j;
+  o.M = c->M;
+  o.Mp = c->Mp;
+  o.n_win = c->n_win;
+  o.n_inc = c->n_inc;
+  o.nwi = c->nwi;
+  o.nwj = c->nwj;
+  return o;
+}
+
+TopoArgs topo_args(ps2_ctx* c, void* K_out, void* C_out, void* coh_io) {
+  TopoArgs t{};
+  t.ph_nm = c->ph_nm.p;
+  t.filt = c->filt.p;
+  t.cell_of = c->cell_of.as<int32_t>();
+  t.cpx = nullptr;
+  t.bp = c->bp.as<float>();
+  t.bp_row_inv = c->bp_row_inv;
+  t.N = c->N;
+  t.M = c->M;
+  t.Mp = c->Mp;
+  t.n_half = c->n_half;
+  t.zero_mode = 0;
+  t.K_out = K_out;
+  t.C_out = C_out;
+  t.coh_io = coh_io;
+  t.nopt = c->nopt.as<uint8_t>();
+  t.rms_partial = c->rms_partial.as<double>();
+  t.hist = c->hist.as<int32_t>();
+  t.n_invalid = c->n_invalid.as<int32_t>();
+  t.cutoff0 = c->cutoff0;
+  t.dbin = c->dbin;
+  t.accumulate_stats = 1;
+  return t;
+}
+
+// CLAP window geometry shared by the context and the stateless entry point.
+int clap_geometry(int64_t n_i, int64_t n_j, int64_t n_win, int* n_inc, int* nwi, int* nwj) {
+  if (n_win < 4 || n_win > 32) return set_err(PS2_ERR_UNSUPPORTED, "CLAP window %lld unsupported (4..32)", (long long)n_win);
+  *n_inc = static_cast<int>(std::max<int64_t>(n_win / 4, 1));
+  const int64_t a = static_cast<int64_t>(std::ceil(static_cast<double>(n_i) / *n_inc)) - 3;
+  const int64_t b = static_cast<int64_t>(std::ceil(static_cast<double>(n_j) / *n_inc)) - 3;
+  if (a > 0 && b > 0 && (n_i < n_win || n_j < n_win))
+    return set_err(PS2_ERR_INVALID_ARG,
+                   "grid %lldx%lld is smaller than the %lld-cell CLAP window but yields windows "
+                   "(the reference's window placement underflows for 19-23 cells per side)",
+                   (long long)n_i, (long long)n_j, (long long)n_win);
+  *nwi = a > 0 && b > 0 ? static_cast<int>(a) : 0;
+  *nwj = a > 0 && b > 0 ? static_cast<int>(b) : 0;
+  return PS2_OK;
+}
+
+int copy_in(ps2_ctx* c, DevBuf& dst, const void* src, size_t bytes, bool on_device) {
+  CK(dst.alloc(bytes));
+  CK(cudaMemcpyAsync(dst.p, src, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->st));
+  return PS2_OK;
+}
+
+int run_one_iteration(ps2_ctx* c, bool force_continue, cudaEvent_t* ev) {
+  const bool fp64 = c->fp64;
+  const int cur = c->kcur;
+  int64_t launched = 0;
+  if (ev) CK(cudaEventRecord(ev[0], c->st));
+  if (!c->psquare && c->iters_done > 0) {
+    TopoArgs t = topo_args(c, nullptr, nullptr, nullptr);
+    t.ph_res = c->ph_res.p;
+    CK(launch_snr_weight(t, c->amp.as<float>(), c->w.p, fp64, c->sm_count, c->st));
+    ++launched;
+  }
+  CK(cudaMemsetAsync(c->hist.p, 0, sizeof(int32_t) * PS2_COH_BINS, c->st));
+  CK(cudaMemsetAsync(c->n_invalid.p, 0, sizeof(int32_t), c->st));
+  const int mode = (c->iters_done > 0 && c->psquare) ? 1 : 0;
+  CK(launch_bin(bin_args(c, mode, c->K[cur].p), fp64, c->sm_count, c->st));
+  ++launched;
+  if (ev) CK(cudaEventRecord(ev[1], c->st));
+  CK(launch_clap(clap_args(c, c->grid.p, c->win.p), fp64, c->twf, c->twd, c->sm_count, c->st));
+  CK(launch_overlap(overlap_args(c, c->win.p, c->filt.p), fp64, c->st));
+  launched += 2;
+  if (ev) CK(cudaEventRecord(ev[2], c->st));
+  TopoArgs t = topo_args(c, c->K[1 - cur].p, c->C.p, c->coh.p);
+  if (!c->psquare) t.ph_res = c->ph_res.p;
+  CK(launch_topofit(t, fp64, c->topo_blocks, c->st));
+  ++launched;
+  if (ev) CK(cudaEventRecord(ev[3], c->st));
+  FinalizeArgs f{};
+  f.rms_partial = c->rms_partial.as<double>();
+  f.n_partial = static_cast<int>(std::min<int64_t>(c->topo_blocks, (c->N + 7) / 8));
+  f.N = c->N;
+  f.hist = c->hist.as<int32_t>();
+  f.nr_scaled = c->nr_scaled.as<double>();
+  f.nr_max_nz_ix = c->nr_max_nz_ix;
+  f.low_coh_thresh = c->low_coh_thresh;
+  f.psquare = c->psquare;
+  f.gamma_change_convergence = c->conv;
+  f.gamma_max_iterations = c->max_iter;
+  for (int i = 0; i < 7; ++i) f.g7w[i] = c->g7[i];
+  f.g7sum = c->g7sum;
+  f.taps79 = c->taps.as<double>();
+  f.lut = c->lut.as<double>();
+  f.state = c->state.as<double>();
+  f.stats_out = c->stats.as<double>();
+  f.n_invalid = c->n_invalid.as<int32_t>();
+  f.force_continue = force_continue ? 1 : 0;
+  CK(launch_finalize(f, c->st));
+  ++launched;
+  if (ev) CK(cudaEventRecord(ev[4], c->st));
+  c->kcur = 1 - cur;
+  c->iters_done += 1;
+  c->launches += launched;
+  return PS2_OK;
+}
+
+void fill_stats(const double* h, ps2_iter_stats* s) {
+  s->i_loop = static_cast<int64_t>(h[0]);
+  s->gamma_change_rms = h[1];
+  s->gamma_change_delta = h[2];
+  s->stop = h[3] != 0.0 ? 1 : 0;
+  s->n_invalid = static_cast<int32_t>(h[4]);
+}
+
+int reset_state(ps2_ctx* c) {
+  CK(launch_init_state(c->w0.as<double>(), c->perm.as<int32_t>(), c->N, c->K[0].p, c->w.p, c->coh.p, c->fp64, c->st));
+  CK(cudaMemsetAsync(c->K[1].p, 0, rsz(c) * c->N, c->st));
+  CK(cudaMemcpyAsync(c->nr_scaled.p, c->nr0.p, sizeof(double) * PS2_COH_BINS, cudaMemcpyDeviceToDevice, c->st));
+  double st0[4] = {0.0, 1.0, 0.0, 0.0};
+  CK(cudaMemcpyAsync(c->state.p, st0, sizeof(st0), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->kcur = 0;
+  c->iters_done = 0;
+  c->last = ps2_iter_stats{};
+  return PS2_OK;
+}
+
+}  // namespace
+
+// ====================================================================== ABI
+extern "C" {
+
+const char* ps2_last_error(void) { return g_err.c_str(); }
+
+int ps2_create(ps2_ctx** out, int device) {
+  if (!out) return set_err(PS2_ERR_INVALID_ARG, "ps2_create: out is NULL");
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return set_err(PS2_ERR_INVALID_ARG, "device %d out of range (%d devices)", device, ndev);
+  CK(cudaSetDevice(device));
+  ps2_ctx* c = new ps2_ctx();
+  c->device = device;
+  cudaDeviceProp prop;
+  cudaError_t e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) {
+    delete c;
+    return set_err(PS2_ERR_CUDA, "cudaGetDeviceProperties: %s", cudaGetErrorString(e));
+  }
+  c->sm_count = prop.multiProcessorCount;
+  e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&c->h_stats), 8 * sizeof(double));
+  if (e != cudaSuccess) {
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+    return set_err(PS2_ERR_CUDA, "ps2_create: %s", cudaGetErrorString(e));
+  }
+  twiddles(&c->twf, &c->twd);
+  gauss7(c->g7, &c->g7sum);
+  coh_bin_rule(&c->cutoff0, &c->dbin);
+  *out = c;
+  return PS2_OK;
+}
+
+void ps2_destroy(ps2_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->st) cudaStreamSynchronize(c->st);
+  DevBuf* bufs[] = {&c->ph_nm, &c->bp, &c->amp, &c->perm, &c->cell_start, &c->cell_of, &c->w0, &c->K[0], &c->K[1],
+                    &c->w, &c->coh, &c->C, &c->nopt, &c->grid, &c->win, &c->filt, &c->low_pass, &c->wscaled,
+                    &c->taps, &c->lut, &c->nr0, &c->nr_scaled, &c->state, &c->stats, &c->hist, &c->n_invalid,
+                    &c->rms_partial, &c->ph_res, &c->scratch};
+  for (DevBuf* b : bufs) b->release();
+  for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
+  if (c->h_stats) cudaFreeHost(c->h_stats);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+int ps2_load_patch(ps2_ctx* c, const ps2_patch_desc* d) {
+  if (!c || !d) return set_err(PS2_ERR_INVALID_ARG, "ps2_load_patch: NULL argument");
+  if (d->n_ps <= 0 || d->n_ifg <= 0) return set_err(PS2_ERR_INVALID_ARG, "n_ps and n_ifg must be positive");
+  if (d->n_ifg > 256) return set_err(PS2_ERR_UNSUPPORTED, "n_ifg %lld > 256 is not supported", (long long)d->n_ifg);
+  if (d->n_ps > INT32_MAX - 1) return set_err(PS2_ERR_UNSUPPORTED, "n_ps too large");
+  if (!d->ph_nm || !d->bperp || !d->grid_lin || !d->weight0 || !d->low_pass || !d->nr)
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_load_patch: a required array is NULL");
+  if (d->n_i <= 0 || d->n_j <= 0) return set_err(PS2_ERR_INVALID_ARG, "grid size must be positive");
+  if (d->n_win_ex != 32) return set_err(PS2_ERR_UNSUPPORTED, "CLAP FFT size %lld unsupported (32)", (long long)d->n_win_ex);
+  if (d->precision != PS2_PRECISION_FP32 && d->precision != PS2_PRECISION_FP64)
+    return set_err(PS2_ERR_INVALID_ARG, "unknown precision %d", d->precision);
+  if (!d->psquare && !d->amp) return set_err(PS2_ERR_INVALID_ARG, "SNR weighting needs amp");
+  if (d->low_coh_thresh < 0 || d->low_coh_thresh > PS2_COH_BINS)
+    return set_err(PS2_ERR_INVALID_ARG, "low_coh_thresh %lld outside 0..100", (long long)d->low_coh_thresh);
+  if (!(d->n_trial_wraps >= 0.0) || d->n_trial_wraps > 1.0e4)
+    return set_err(PS2_ERR_INVALID_ARG, "n_trial_wraps %g out of range", d->n_trial_wraps);
+  CK(cudaSetDevice(c->device));
+  int n_inc, nwi, nwj;
+  int rc = clap_geometry(d->n_i, d->n_j, d->clap_window, &n_inc, &nwi, &nwj);
+  if (rc) return rc;
+  c->loaded = false;
+  c->fp64 = d->precision == PS2_PRECISION_FP64;
+  c->N = d->n_ps;
+  c->M = static_cast<int>(d->n_ifg);
+  c->Mp = (c->M + 3) & ~3;
+  c->n_i = static_cast<int>(d->n_i);
+  c->n_j = static_cast<int>(d->n_j);
+  c->G = d->n_i * d->n_j;
+  c->n_win = static_cast<int>(d->clap_window);
+  c->n_inc = n_inc;
+  c->nwi = nwi;
+  c->nwj = nwj;
+  c->nchunk = (c->M + 31) / 32;
+  c->n_half = static_cast<int>(std::ceil(8.0 * d->n_trial_wraps));
+  c->bp_row_inv = d->bperp_row_invariant ? 1 : 0;
+  c->psquare = d->psquare ? 1 : 0;
+  c->low_coh_thresh = static_cast<int>(d->low_coh_thresh);
+  c->alpha = d->clap_alpha;
+  c->beta = d->clap_beta;
+  c->alpha_is_one = std::fabs(d->clap_alpha - 1.0) <= 2.220446049250313e-16 ? 1 : 0;
+  c->conv = d->gamma_change_convergence;
+  c->max_iter = d->gamma_max_iterations;
+  c->nr_max_nz_ix = d->nr_max_nz_ix;
+  const bool dev = d->pointers_on_device != 0;
+  const int64_t N = c->N, M = c->M, G = c->G;
+
+  // stable counting sort of rows by cell (host)
+  std::vector<int64_t> gl(N);
+  if (dev)
+    CK(cudaMemcpy(gl.data(), d->grid_lin, sizeof(int64_t) * N, cudaMemcpyDeviceToHost));
+  else
+    std::memcpy(gl.data(), d->grid_lin, sizeof(int64_t) * N);
+  std::vector<int32_t> start(G + 1, 0), perm(N), cell_of(N);
+  for (int64_t r = 0; r < N; ++r) {
+    if (gl[r] < 0 || gl[r] >= G)
+      return set_err(PS2_ERR_INVALID_ARG, "grid_lin[%lld] = %lld outside the %lldx%lld grid", (long long)r,
+                     (long long)gl[r], (long long)c->n_i, (long long)c->n_j);
+    start[gl[r] + 1] += 1;
+  }
+  for (int64_t g = 0; g < G; ++g) start[g + 1] += start[g];
+  {
+    std::vector<int32_t> fillp(start.begin(), start.end() - 1);
+    for (int64_t r = 0; r < N; ++r) {
+      const int32_t s = fillp[gl[r]]++;
+      perm[s] = static_cast<int32_t>(r);
+      cell_of[s] = static_cast<int32_t>(gl[r]);
+    }
+  }
+  const size_t R = rsz(c), Cz = csz(c);
+  CK(c->perm.alloc(sizeof(int32_t) * N));
+  CK(cudaMemcpyAsync(c->perm.p, perm.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, c->st));
+  CK(c->cell_start.alloc(sizeof(int32_t) * (G + 1)));
+  CK(cudaMemcpyAsync(c->cell_start.p, start.data(), sizeof(int32_t) * (G + 1), cudaMemcpyHostToDevice, c->st));
+  CK(c->cell_of.alloc(sizeof(int32_t) * N));
+  CK(cudaMemcpyAsync(c->cell_of.p, cell_of.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, c->st));
+  // row data, gathered into cell order on the device
+  {
+    DevBuf tmp;
+    rc = copy_in(c, tmp, d->ph_nm, sizeof(float) * 2 * N * M, dev);
+    if (rc) return rc;
+    CK(c->ph_nm.alloc(sizeof(float) * 2 * N * M));
+    CK(launch_gather_rows(tmp.p, c->ph_nm.p, c->perm.as<int32_t>(), N, sizeof(float) * 2 * M, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    tmp.release();
+  }
+  if (c->bp_row_inv) {
+    rc = copy_in(c, c->bp, d->bperp, sizeof(float) * M, dev);
+    if (rc) return rc;
+  } else {
+    DevBuf tmp;
+    rc = copy_in(c, tmp, d->bperp, sizeof(float) * N * M, dev);
+    if (rc) return rc;
+    CK(c->bp.alloc(sizeof(float) * N * M));
+    CK(launch_gather_rows(tmp.p, c->bp.p, c->perm.as<int32_t>(), N, sizeof(float) * M, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    tmp.release();
+  }
+  if (!c->psquare) {
+    DevBuf tmp;
+    rc = copy_in(c, tmp, d->amp, sizeof(float) * N * M, dev);
+    if (rc) return rc;
+    CK(c->amp.alloc(sizeof(float) * N * M));
+    CK(launch_gather_rows(tmp.p, c->amp.p, c->perm.as<int32_t>(), N, sizeof(float) * M, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    tmp.release();
+    CK(c->ph_res.alloc(R * N * M));
+  } else {
+    c->amp.release();
+    c->ph_res.release();
+  }
+  rc = copy_in(c, c->w0, d->weight0, sizeof(double) * N, dev);
+  if (rc) return rc;
+  rc = copy_in(c, c->low_pass, d->low_pass, sizeof(double) * 32 * 32, dev);
+  if (rc) return rc;
+  rc = copy_in(c, c->nr0, d->nr, sizeof(double) * PS2_COH_BINS, dev);
+  if (rc) return rc;
+  // loop state and work buffers
+  CK(c->K[0].alloc(R * N));
+  CK(c->K[1].alloc(R * N));
+  CK(c->w.alloc(R * N));
+  CK(c->coh.alloc(R * N));
+  CK(c->C.alloc(R * N));
+  CK(c->nopt.alloc(N));
+  CK(c->grid.alloc(Cz * G * c->Mp));
+  CK(c->filt.alloc(Cz * G * c->Mp));
+  const int64_t W = static_cast<int64_t>(nwi) * nwj;
+  CK(c->win.alloc(Cz * std::max<int64_t>(W, 1) * c->n_win * c->n_win * c->Mp));
+  if (W == 0) CK(cudaMemsetAsync(c->filt.p, 0, Cz * G * c->Mp, c->st));
+  std::vector<double> ws = window_weight_scaled(c->n_win, 32);
+  CK(c->wscaled.alloc(sizeof(double) * ws.size()));
+  CK(cudaMemcpyAsync(c->wscaled.p, ws.data(), sizeof(double) * ws.size(), cudaMemcpyHostToDevice, c->st));
+  CK(c->taps.alloc(sizeof(double) * 79));
+  CK(cudaMemcpyAsync(c->taps.p, kStage2Interp10Taps, sizeof(double) * 79, cudaMemcpyHostToDevice, c->st));
+  CK(c->lut.alloc(sizeof(double) * 1001));
+  CK(cudaMemsetAsync(c->lut.p, 0, sizeof(double) * 1001, c->st));
+  CK(c->nr_scaled.alloc(sizeof(double) * PS2_COH_BINS));
+  CK(c->state.alloc(sizeof(double) * 4));
+  CK(c->stats.alloc(sizeof(double) * 8));
+  CK(c->hist.alloc(sizeof(int32_t) * PS2_COH_BINS));
+  CK(c->n_invalid.alloc(sizeof(int32_t)));
+  c->topo_blocks = topofit_grid_blocks(c->sm_count, c->fp64);
+  CK(c->rms_partial.alloc(sizeof(double) * c->topo_blocks));
+  rc = reset_state(c);
+  if (rc) return rc;
+  c->loaded = true;
+  return PS2_OK;
+}
+
+int ps2_reset(ps2_ctx* c) {
+  if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "no patch loaded");
+  CK(cudaSetDevice(c->device));
+  return reset_state(c);
+}
+
+int ps2_iterate(ps2_ctx* c, int64_t n_iter, ps2_iter_stats* stats) {
+  if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "no patch loaded");
+  if (n_iter <= 0) return set_err(PS2_ERR_INVALID_ARG, "n_iter must be positive");
+  CK(cudaSetDevice(c->device));
+  int rc = ensure_events(c, static_cast<size_t>(5 * n_iter + 2));
+  if (rc) return rc;
+  std::vector<double> hs(static_cast<size_t>(8 * n_iter));
+  c->launches = 0;
+  cudaEvent_t span0 = c->evpool[5 * n_iter], span1 = c->evpool[5 * n_iter + 1];
+  CK(cudaEventRecord(span0, c->st));
+  for (int64_t k = 0; k < n_iter; ++k) {
+    rc = run_one_iteration(c, true, &c->evpool[5 * k]);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(&c->h_stats[0], c->stats.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    if (stats) {
+      CK(cudaStreamSynchronize(c->st));
+      std::memcpy(&hs[8 * k], c->h_stats, 8 * sizeof(double));
+    }
+  }
+  CK(cudaEventRecord(span1, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (!stats) std::memcpy(&hs[8 * (n_iter - 1)], c->h_stats, 8 * sizeof(double));
+  for (int i = 0; i < 4; ++i) c->kernel_ms[i] = 0.0;
+  float span_ms = 0.f;
+  CK(cudaEventElapsedTime(&span_ms, span0, span1));
+  c->last_ms = span_ms;
+  for (int64_t k = 0; k < n_iter; ++k) {
+    float ms;
+    for (int i = 0; i < 4; ++i) {
+      CK(cudaEventElapsedTime(&ms, c->evpool[5 * k + i], c->evpool[5 * k + i + 1]));
+      c->kernel_ms[i] += ms;
+    }
+    if (stats) fill_stats(&hs[8 * k], &stats[k]);
+  }
+  fill_stats(&hs[8 * (n_iter - 1)], &c->last);
+  return PS2_OK;
+}
+
+int ps2_run_to_convergence(ps2_ctx* c, ps2_iter_stats* last) {
+  if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "no patch loaded");
+  CK(cudaSetDevice(c->device));
+  const int64_t cap = std::max<int64_t>(c->max_iter, 1) + 1;
+  int rc = ensure_events(c, 5);
+  if (rc) return rc;
+  c->launches = 0;
+  c->last_ms = 0.0;
+  for (int i = 0; i < 4; ++i) c->kernel_ms[i] = 0.0;
+  for (int64_t k = 0; k < cap; ++k) {
+    rc = run_one_iteration(c, false, c->evpool.data());
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(c->h_stats, c->stats.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    float ms;
+    for (int i = 0; i < 4; ++i) {
+      CK(cudaEventElapsedTime(&ms, c->evpool[i], c->evpool[i + 1]));
+      c->kernel_ms[i] += ms;
+    }
+    CK(cudaEventElapsedTime(&ms, c->evpool[0], c->evpool[4]));
+    c->last_ms += ms;
+    fill_stats(c->h_stats, &c->last);
+    if (c->last.stop) break;
+  }
+  if (last) *last = c->last;
+  return PS2_OK;
+}
+
+int ps2_last_timing(const ps2_ctx* c, double* total_ms, double* per_kernel_ms) {
+  if (!c) return set_err(PS2_ERR_INVALID_ARG, "NULL context");
+  if (total_ms) *total_ms = c->last_ms;
+  if (per_kernel_ms)
+    for (int i = 0; i < 4; ++i) per_kernel_ms[i] = c->kernel_ms[i];
+  return PS2_OK;
+}
+
+int64_t ps2_last_launch_count(const ps2_ctx* c) { return c ? c->launches : -1; }
+
+int ps2_download(ps2_ctx* c, ps2_outputs* o) {
+  if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "no patch loaded");
+  if (!o) return set_err(PS2_ERR_INVALID_ARG, "NULL outputs");
+  CK(cudaSetDevice(c->device));
+  const int64_t N = c->N, M = c->M, G = c->G;
+  const size_t R = rsz(c), Cz = csz(c);
+  const int32_t* perm = c->perm.as<int32_t>();
+  const bool fp64 = c->fp64;
+  // per-PS vectors: scatter to the caller's order, widen to f64 on the host
+  auto fetch_vec = [&](const void* src, double* dst) -> int {
+    if (!dst) return PS2_OK;
+    CK(c->scratch.alloc(R * N));
+    CK(launch_scatter_rows(src, c->scratch.p, perm, N, R, c->st));
+    if (fp64) {
+      CK(cudaMemcpyAsync(dst, c->scratch.p, R * N, cudaMemcpyDeviceToHost, c->st));
+      CK(cudaStreamSynchronize(c->st));
+    } else {
+      std::vector<float> tmp(N);
+      CK(cudaMemcpyAsync(tmp.data(), c->scratch.p, R * N, cudaMemcpyDeviceToHost, c->st));
+      CK(cudaStreamSynchronize(c->st));
+      for (int64_t i = 0; i < N; ++i) dst[i] = static_cast<double>(tmp[i]);
+    }
+    return PS2_OK;
+  };
+  int rc;
+  if ((rc = fetch_vec(c->K[c->kcur].p, o->K_ps))) return rc;
+  if ((rc = fetch_vec(c->C.p, o->C_ps))) return rc;
+  if ((rc = fetch_vec(c->coh.p, o->coh_ps))) return rc;
+  if ((rc = fetch_vec(c->coh.p, o->coh_ps_save))) return rc;
+  if (o->N_opt) {
+    std::vector<uint8_t> sorted(N);
+    std::vector<int32_t> hperm(N);
+    CK(cudaMemcpyAsync(sorted.data(), c->nopt.p, N, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(hperm.data(), perm, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int64_t s = 0; s < N; ++s) o->N_opt[hperm[s]] = sorted[s] ? 1.0 : 0.0;
+  }
+  // residual phase and normalised patch phase: recomputed from the final
+  // state by the same topofit code (deterministic, bit-identical values)
+  const bool want_res = fp64 ? (o->ph_res_f64 || o->ph_res) : (o->ph_res != nullptr);
+  const bool want_patch = fp64 ? (o->ph_patch_f64 || o->ph_patch) : (o->ph_patch != nullptr);
+  if (c->iters_done > 0 && (want_res || want_patch)) {
+    DevBuf kk, cc, hh, res, pat;
+    CK(kk.alloc(R * N));
+    CK(cc.alloc(R * N));
+    CK(hh.alloc(R * N));
+    CK(res.alloc(R * N * M));
+    CK(pat.alloc(Cz * N * M));
+    TopoArgs t = topo_args(c, kk.p, cc.p, hh.p);
+    t.nopt = nullptr;
+    t.accumulate_stats = 0;
+    t.ph_res = res.p;
+    t.ph_patch = pat.p;
+    CK(launch_topofit(t, fp64, c->topo_blocks, c->st));
+    DevBuf out;
+    if (want_res) {
+      CK(out.alloc(R * N * M));
+      CK(launch_scatter_rows(res.p, out.p, perm, N, R * M, c->st));
+      if (fp64) {
+        if (o->ph_res_f64) CK(cudaMemcpyAsync(o->ph_res_f64, out.p, R * N * M, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        if (o->ph_res) {
+          std::vector<double> t2(N * M);
+          CK(cudaMemcpy(t2.data(), out.p, R * N * M, cudaMemcpyDeviceToHost));
+          for (int64_t i = 0; i < N * M; ++i) o->ph_res[i] = static_cast<float>(t2[i]);
+        }
+      } else {
+        CK(cudaMemcpyAsync(o->ph_res, out.p, R * N * M, cudaMemcpyDeviceToHost, c->st));
+      }
+    }
+    if (want_patch) {
+      CK(out.alloc(Cz * N * M));
+      CK(launch_scatter_rows(pat.p, out.p, perm, N, Cz * M, c->st));
+      if (fp64) {
+        if (o->ph_patch_f64) CK(cudaMemcpyAsync(o->ph_patch_f64, out.p, Cz * N * M, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        if (o->ph_patch) {
+          std::vector<double> t2(2 * N * M);
+          CK(cudaMemcpy(t2.data(), out.p, Cz * N * M, cudaMemcpyDeviceToHost));
+          for (int64_t i = 0; i < 2 * N * M; ++i) o->ph_patch[i] = static_cast<float>(t2[i]);
+        }
+      } else {
+        CK(cudaMemcpyAsync(o->ph_patch, out.p, Cz * N * M, cudaMemcpyDeviceToHost, c->st));
+      }
+    }
+    CK(cudaStreamSynchronize(c->st));
+  }
+  const bool want_w = fp64 ? (o->ph_weight_f64 || o->ph_weight) : (o->ph_weight != nullptr);
+  if (want_w && c->iters_done > 0) {
+    DevBuf out;
+    CK(out.alloc(Cz * N * M));
+    BinArgs a = bin_args(c, 0, c->K[1 - c->kcur].p);
+    CK(launch_ph_weight(a, N, fp64, perm, out.p, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (fp64) {
+      if (o->ph_weight_f64) CK(cudaMemcpy(o->ph_weight_f64, out.p, Cz * N * M, cudaMemcpyDeviceToHost));
+      if (o->ph_weight) {
+        std::vector<double> t2(2 * N * M);
+        CK(cudaMemcpy(t2.data(), out.p, Cz * N * M, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < 2 * N * M; ++i) o->ph_weight[i] = static_cast<float>(t2[i]);
+      }
+    } else {
+      CK(cudaMemcpy(o->ph_weight, out.p, Cz * N * M, cudaMemcpyDeviceToHost));
+    }
+  }
+  const bool want_g = fp64 ? (o->ph_grid_f64 || o->ph_grid) : (o->ph_grid != nullptr);
+  if (want_g) {
+    DevBuf out;
+    CK(out.alloc(Cz * G * M));
+    CK(launch_unpad_grid(c->grid.p, out.p, G, c->M, c->Mp, static_cast<int>(Cz), c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (fp64) {
+      if (o->ph_grid_f64) CK(cudaMemcpy(o->ph_grid_f64, out.p, Cz * G * M, cudaMemcpyDeviceToHost));
+      if (o->ph_grid) {
+        std::vector<double> t2(2 * G * M);
+        CK(cudaMemcpy(t2.data(), out.p, Cz * G * M, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < 2 * G * M; ++i) o->ph_grid[i] = static_cast<float>(t2[i]);
+      }
+    } else {
+      CK(cudaMemcpy(o->ph_grid, out.p, Cz * G * M, cudaMemcpyDeviceToHost));
+    }
+  }
+  if (o->Nr) CK(cudaMemcpy(o->Nr, c->nr_scaled.p, sizeof(double) * PS2_COH_BINS, cudaMemcpyDeviceToHost));
+  if (o->gamma_change_save || o->i_loop) {
+    double st[4];
+    CK(cudaMemcpy(st, c->state.p, sizeof(st), cudaMemcpyDeviceToHost));
+    if (o->gamma_change_save) *o->gamma_change_save = st[0];
+    if (o->i_loop) *o->i_loop = c->last.i_loop;
+  }
+  return PS2_OK;
+}
+
+// ------------------------------------------------------ stateless kernels --
+namespace {
+struct Scoped {
+  cudaStream_t st = nullptr;
+  int sm = 148;
+  ~Scoped() {
+    if (st) cudaStreamDestroy(st);
+  }
+};
+int scoped_init(Scoped& s) {
+  int dev;
+  CK(cudaGetDevice(&dev));
+  cudaDeviceProp p;
+  CK(cudaGetDeviceProperties(&p, dev));
+  s.sm = p.multiProcessorCount;
+  CK(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
+  return PS2_OK;
+}
+}  // namespace
+
+int ps2_grid_accumulate(const float* ph_weight, const int64_t* grid_lin, int64_t n_ps, int64_t n_ifg, int64_t n_i,
+                        int64_t n_j, float* out) {
+  if (!ph_weight || !grid_lin || !out || n_ps < 0 || n_ifg <= 0 || n_i <= 0 || n_j <= 0)
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_grid_accumulate: invalid arguments");
+  Scoped sc;
+  int rc = scoped_init(sc);
+  if (rc) return rc;
+  const int64_t G = n_i * n_j, M = n_ifg;
+  const int Mp = static_cast<int>((M + 3) & ~int64_t(3));
+  // rows outside the grid are skipped (accumulate_grid, native_stage2.rs:733-735)
+  std::vector<int32_t> start(G + 1, 0), perm;
+  perm.reserve(n_ps);
+  for (int64_t r = 0; r < n_ps; ++r)
+    if (grid_lin[r] >= 0 && grid_lin[r] < G) start[grid_lin[r] + 1] += 1;
+  for (int64_t g = 0; g < G; ++g) start[g + 1] += start[g];
+  const int64_t nv = start[G];
+  perm.resize(nv);
+  {
+    std::vector<int32_t> fp(start.begin(), start.end() - 1);
+    for (int64_t r = 0; r < n_ps; ++r)
+      if (grid_lin[r] >= 0 && grid_lin[r] < G) perm[fp[grid_lin[r]]++] = static_cast<int32_t>(r);
+  }
+  DevBuf src, sorted, dperm, dstart, grid, outb;
+  CK(src.alloc(sizeof(float) * 2 * std::max<int64_t>(n_ps, 1) * M));
+  if (n_ps) CK(cudaMemcpyAsync(src.p, ph_weight, sizeof(float) * 2 * n_ps * M, cudaMemcpyHostToDevice, sc.st));
+  CK(dperm.alloc(sizeof(int32_t) * std::max<int64_t>(nv, 1)));
+  if (nv) CK(cudaMemcpyAsync(dperm.p, perm.data(), sizeof(int32_t) * nv, cudaMemcpyHostToDevice, sc.st));
+  CK(sorted.alloc(sizeof(float) * 2 * std::max<int64_t>(nv, 1) * M));
+  CK(launch_gather_rows(src.p, sorted.p, dperm.as<int32_t>(), nv, sizeof(float) * 2 * M, sc.st));
+  CK(dstart.alloc(sizeof(int32_t) * (G + 1)));
+  CK(cudaMemcpyAsync(dstart.p, start.data(), sizeof(int32_t) * (G + 1), cudaMemcpyHostToDevice, sc.st));
+  CK(grid.alloc(sizeof(float) * 2 * G * Mp));
+  BinArgs a{};
+  a.ph_nm = sorted.p;
+  a.cell_start = dstart.as<int32_t>();
+  a.G = G;
+  a.M = static_cast<int>(M);
+  a.Mp = Mp;
+  a.nchunk = static_cast<int>((M + 31) / 32);
+  a.mode = 3;
+  a.grid = grid.p;
+  CK(launch_bin(a, false, sc.sm, sc.st));
+  CK(outb.alloc(sizeof(float) * 2 * G * M));
+  CK(launch_unpad_grid(grid.p, outb.p, G, static_cast<int>(M), Mp, 8, sc.st));
+  CK(cudaMemcpyAsync(out, outb.p, sizeof(float) * 2 * G * M, cudaMemcpyDeviceToHost, sc.st));
+  CK(cudaStreamSynchronize(sc.st));
+  return PS2_OK;
+}
+
+int ps2_topofit(const float* cpxphase, const float* bperp, int32_t row_inv, double n_trial_wraps, int64_t n,
+                int64_t m, double* K, double* C, double* coh, float* residual) {
+  if (!cpxphase || !bperp || !K || !C || !coh || n < 0 || m <= 0)
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_topofit: invalid arguments");
+  if (m > 256) return set_err(PS2_ERR_UNSUPPORTED, "m %lld > 256 is not supported", (long long)m);
+  if (!(n_trial_wraps >= 0.0) || n_trial_wraps > 1.0e4)
+    return set_err(PS2_ERR_INVALID_ARG, "n_trial_wraps %g out of range", n_trial_wraps);
+  if (n == 0) return PS2_OK;
+  Scoped sc;
+  int rc = scoped_init(sc);
+  if (rc) return rc;
+  DevBuf dc, db, dk, dcc, dh, dr;
+  CK(dc.alloc(sizeof(float) * 2 * n * m));
+  CK(cudaMemcpyAsync(dc.p, cpxphase, sizeof(float) * 2 * n * m, cudaMemcpyHostToDevice, sc.st));
+  const int64_t nb = row_inv ? m : n * m;
+  CK(db.alloc(sizeof(float) * nb));
+  CK(cudaMemcpyAsync(db.p, bperp, sizeof(float) * nb, cudaMemcpyHostToDevice, sc.st));
+  CK(dk.alloc(sizeof(float) * n));
+  CK(dcc.alloc(sizeof(float) * n));
+  CK(dh.alloc(sizeof(float) * n));
+  if (residual) CK(dr.alloc(sizeof(float) * 2 * n * m));
+  TopoArgs t{};
+  t.cpx = dc.p;
+  t.bp = db.as<float>();
+  t.bp_row_inv = row_inv ? 1 : 0;
+  t.N = n;
+  t.M = static_cast<int>(m);
+  t.Mp = static_cast<int>(m);
+  t.n_half = static_cast<int>(std::ceil(8.0 * n_trial_wraps));
+  t.zero_mode = 1;
+  t.K_out = dk.p;
+  t.C_out = dcc.p;
+  t.coh_io = dh.p;
+  t.residual = residual ? dr.p : nullptr;
+  t.accumulate_stats = 0;
+  CK(launch_topofit(t, false, topofit_grid_blocks(sc.sm, false), sc.st));
+  std::vector<float> hk(n), hc(n), hh(n);
+  CK(cudaMemcpyAsync(hk.data(), dk.p, sizeof(float) * n, cudaMemcpyDeviceToHost, sc.st));
+  CK(cudaMemcpyAsync(hc.data(), dcc.p, sizeof(float) * n, cudaMemcpyDeviceToHost, sc.st));
+  CK(cudaMemcpyAsync(hh.data(), dh.p, sizeof(float) * n, cudaMemcpyDeviceToHost, sc.st));
+  if (residual) CK(cudaMemcpyAsync(residual, dr.p, sizeof(float) * 2 * n * m, cudaMemcpyDeviceToHost, sc.st));
+  CK(cudaStreamSynchronize(sc.st));
+  for (int64_t i = 0; i < n; ++i) {
+    K[i] = hk[i];
+    C[i] = hc[i];
+    coh[i] = hh[i];
+  }
+  return PS2_OK;
+}
+
+int ps2_clap_filter_grid(const float* ph_grid, int64_t n_i, int64_t n_j, int64_t m, int64_t clap_window, double alpha,
+                         double beta, const double* low_pass, int64_t n_win_ex, float* out) {
+  if (!ph_grid || !out || !low_pass || n_i <= 0 || n_j <= 0 || m <= 0)
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_clap_filter_grid: invalid arguments");
+  if (n_win_ex != 32) return set_err(PS2_ERR_UNSUPPORTED, "CLAP FFT size %lld unsupported (32)", (long long)n_win_ex);
+  int n_inc, nwi, nwj;
+  int rc = clap_geometry(n_i, n_j, clap_window, &n_inc, &nwi, &nwj);
+  if (rc) return rc;
+  Scoped sc;
+  rc = scoped_init(sc);
+  if (rc) return rc;
+  const int64_t G = n_i * n_j;
+  const int Mp = static_cast<int>((m + 3) & ~int64_t(3));
+  DevBuf raw, grid, win, filt, lp, wsd, outb;
+  CK(raw.alloc(sizeof(float) * 2 * G * m));
+  CK(cudaMemcpyAsync(raw.p, ph_grid, sizeof(float) * 2 * G * m, cudaMemcpyHostToDevice, sc.st));
+  CK(grid.alloc(sizeof(float) * 2 * G * Mp));
+  CK(launch_pad_grid(raw.p, grid.p, G, static_cast<int>(m), Mp, 8, sc.st));
+  CK(filt.alloc(sizeof(float) * 2 * G * Mp));
+  const int64_t W = static_cast<int64_t>(nwi) * nwj;
+  CK(win.alloc(sizeof(float) * 2 * std::max<int64_t>(W, 1) * clap_window * clap_window * Mp));
+  CK(lp.alloc(sizeof(double) * 1024));
+  CK(cudaMemcpyAsync(lp.p, low_pass, sizeof(double) * 1024, cudaMemcpyHostToDevice, sc.st));
+  std::vector<double> ws = window_weight_scaled(static_cast<int>(clap_window), 32);
+  CK(wsd.alloc(sizeof(double) * ws.size()));
+  CK(cudaMemcpyAsync(wsd.p, ws.data(), sizeof(double) * ws.size(), cudaMemcpyHostToDevice, sc.st));
+  ClapArgs a{};
+  a.grid = grid.p;
+  a.n_i = static_cast<int>(n_i);
+  a.n_j = static_cast<int>(n_j);
+  a.M = static_cast<int>(m);
+  a.Mp = Mp;
+  a.n_win = static_cast<int>(clap_window);
+  a.nwi = nwi;
+  a.nwj = nwj;
+  a.alpha = alpha;
+  a.beta = beta;
+  a.alpha_is_one = std::fabs(alpha - 1.0) <= 2.220446049250313e-16 ? 1 : 0;
+  a.low_pass = lp.as<double>();
+  a.wscaled = wsd.as<double>();
+  gauss7(a.g7, nullptr);
+  a.win_out = win.p;
+  Twiddles32f tf;
+  Twiddles32d td;
+  twiddles(&tf, &td);
+  if (W > 0) {
+    CK(launch_clap(a, false, tf, td, sc.sm, sc.st));
+    OverlapArgs o{};
+    o.win_out = win.p;
+    o.filt = filt.p;
+    o.n_i = a.n_i;
+    o.n_j = a.n_j;
+    o.M = a.M;
+    o.Mp = Mp;
+    o.n_win = a.n_win;
+    o.n_inc = n_inc;
+    o.nwi = nwi;
+    o.nwj = nwj;
+    CK(launch_overlap(o, false, sc.st));
+  } else {
+    CK(cudaMemsetAsync(filt.p, 0, sizeof(float) * 2 * G * Mp, sc.st));
+  }
+  CK(outb.alloc(sizeof(float) * 2 * G * m));
+  CK(launch_unpad_grid(filt.p, outb.p, G, static_cast<int>(m), Mp, 8, sc.st));
+  CK(cudaMemcpyAsync(out, outb.p, sizeof(float) * 2 * G * m, cudaMemcpyDeviceToHost, sc.st));
+  CK(cudaStreamSynchronize(sc.st));
+  return PS2_OK;
+}
+
+int ps2_random_coherence_histogram(const double* bperp_nm, int64_t n_ifg, double n_trial_wraps, int64_t n_rand,
+                                   int32_t small_baseline, const int64_t* ifgday_ix, int64_t n_image, double* nr_out,
+                                   double* nr_max_nz_ix) {
+  if (!bperp_nm || !nr_out || !nr_max_nz_ix || n_ifg <= 0 || n_ifg > 256 || n_rand <= 0)
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_random_coherence_histogram: invalid arguments");
+  if (!(n_trial_wraps >= 0.0) || n_trial_wraps > 1.0e4)
+    return set_err(PS2_ERR_INVALID_ARG, "n_trial_wraps %g out of range", n_trial_wraps);
+  std::vector<int64_t> ia(n_ifg, 0), ib(n_ifg, 0);
+  int64_t cols = n_ifg;
+  if (small_baseline) {
+    if (!ifgday_ix || n_image <= 0) return set_err(PS2_ERR_INVALID_ARG, "small baselines need ifgday_ix and n_image");
+    for (int64_t k = 0; k < n_ifg; ++k) {
+      ia[k] = ifgday_ix[2 * k] - 1;
+      ib[k] = ifgday_ix[2 * k + 1] - 1;
+      if (ia[k] < 0 || ib[k] < 0 || ia[k] >= n_image || ib[k] >= n_image)
+        return set_err(PS2_ERR_INVALID_ARG, "ps1.ifgday_ix must contain positive one-based image ids");
+    }
+    cols = n_image;
+  }
+  // random phases, column-major [cols][n_rand] (MATLAB draws the whole matrix first)
+  std::vector<double> rnd(static_cast<size_t>(n_rand) * cols);
+  {
+    V5Uniform rng(2005);
+    const double two_pi = 2.0 * M_PI;
+    for (auto& v : rnd) v = rng.next() * two_pi;
+  }
+  Scoped sc;
+  int rc = scoped_init(sc);
+  if (rc) return rc;
+  DevBuf dr, db, dia, dib, dh;
+  CK(dr.alloc(sizeof(double) * rnd.size()));
+  CK(cudaMemcpyAsync(dr.p, rnd.data(), sizeof(double) * rnd.size(), cudaMemcpyHostToDevice, sc.st));
+  CK(db.alloc(sizeof(double) * n_ifg));
+  CK(cudaMemcpyAsync(db.p, bperp_nm, sizeof(double) * n_ifg, cudaMemcpyHostToDevice, sc.st));
+  CK(dia.alloc(sizeof(int64_t) * n_ifg));
+  CK(dib.alloc(sizeof(int64_t) * n_ifg));
+  CK(cudaMemcpyAsync(dia.p, ia.data(), sizeof(int64_t) * n_ifg, cudaMemcpyHostToDevice, sc.st));
+  CK(cudaMemcpyAsync(dib.p, ib.data(), sizeof(int64_t) * n_ifg, cudaMemcpyHostToDevice, sc.st));
+  CK(dh.alloc(sizeof(int32_t) * PS2_COH_BINS));
+  CK(cudaMemsetAsync(dh.p, 0, sizeof(int32_t) * PS2_COH_BINS, sc.st));
+  double cutoff0, dbin;
+  coh_bin_rule(&cutoff0, &dbin);
+  CK(launch_random_hist(dr.as<double>(), n_rand, db.as<double>(), static_cast<int>(n_ifg), dia.as<int64_t>(),
+                        dib.as<int64_t>(), small_baseline ? 1 : 0, static_cast<int>(std::ceil(8.0 * n_trial_wraps)),
+                        cutoff0, dbin, dh.as<int32_t>(), sc.sm, sc.st));
+  int32_t h[PS2_COH_BINS];
+  CK(cudaMemcpyAsync(h, dh.p, sizeof(h), cudaMemcpyDeviceToHost, sc.st));
+  CK(cudaStreamSynchronize(sc.st));
+  double mx = 1.0;
+  for (int i = 0; i < PS2_COH_BINS; ++i) nr_out[i] = static_cast<double>(h[i]);
+  for (int i = PS2_COH_BINS - 1; i >= 0; --i)
+    if (nr_out[i] > 0.0) {
+      mx = static_cast<double>(i + 1);
+      break;
+    }
+  *nr_max_nz_ix = mx;
+  return PS2_OK;
+}
+
+}  // extern "C"

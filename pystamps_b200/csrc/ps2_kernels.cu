@@ -1,0 +1,1350 @@
+// Stage-2 gamma-estimation kernels for B200 (sm_100a).
+//
+// One iteration of the reference loop (crates/pystamps-core/src/native_stage2.rs:261-406)
+// is five launches on one stream:
+//   k_bin       fill_phase_weight + accumulate_grid (:629-657, :722-740), fused,
+//               as a sort-by-cell sequential segmented reduction (no float atomics)
+//   k_clap      clap_filter_one_ifg per (window, ifg) (:823-916): 32x32 FFT in
+//               registers + shared memory, |H| smoothing, median, filter, IFFT
+//   k_overlap   the pyramid-weighted overlap-add (:904-915) as a gather in the
+//               reference's window order (deterministic)
+//   k_topofit   extract_patch_phase + fit_stage2_rows + topofit_row + refine_candidate
+//               (:1186-1303): one warp per PS, trial sweep by phasor recurrence
+//   k_finalize  rms_difference, stop rule, P-square weighting table (:307-381, :1538-1783)
+#include <math.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "ps2_device.cuh"
+#include "ps2_kernels.cuh"
+
+namespace ps2 {
+
+template <typename R>
+struct CT;
+template <>
+struct CT<float> {
+  using C = float2;
+  using Tw = Twiddles32f;
+  using U = uint32_t;
+};
+template <>
+struct CT<double> {
+  using C = double2;
+  using Tw = Twiddles32d;
+  using U = unsigned long long;
+};
+
+__device__ __forceinline__ void sincos_r(float x, float* s, float* c) { sincosf(x, s, c); }
+__device__ __forceinline__ void sincos_r(double x, double* s, double* c) { sincos(x, s, c); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float hypot_r(float a, float b) { return hypotf(a, b); }
+__device__ __forceinline__ double hypot_r(double a, double b) { return hypot(a, b); }
+__device__ __forceinline__ float atan2_r(float y, float x) { return atan2f(y, x); }
+__device__ __forceinline__ double atan2_r(double y, double x) { return atan2(y, x); }
+__device__ __forceinline__ float2 mk(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 mk(double a, double b) { return make_double2(a, b); }
+
+// ============================================================= binning ====
+template <typename R>
+__global__ void __launch_bounds__(256) k_bin(BinArgs a) {
+  using C = typename CT<R>::C;
+  const float2* __restrict__ ph = static_cast<const float2*>(a.ph_nm);
+  const R* __restrict__ K = static_cast<const R*>(a.K);
+  R* __restrict__ W = static_cast<R*>(a.w);
+  const R* __restrict__ coh = static_cast<const R*>(a.coh);
+  C* __restrict__ grid = static_cast<C*>(a.grid);
+  const float* __restrict__ bp = a.bp;
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  const int64_t ntask = a.G * a.nchunk;
+  const int64_t M = a.M;
+  for (int64_t task = gw; task < ntask; task += nw) {
+    const int64_t cell = task / a.nchunk;
+    const int chunk = static_cast<int>(task - cell * a.nchunk);
+    const int c = chunk * 32 + lane;
+    const bool active = c < a.M;
+    const int s0 = a.cell_start[cell], s1 = a.cell_start[cell + 1];
+    R ax = R(0), ay = R(0);
+#pragma unroll 4
+    for (int s = s0; s < s1; ++s) {
+      R w = R(1);
+      if (a.mode == 3) {
+      } else if (a.mode == 1) {
+        // psquare_weighting lookup (native_stage2.rs:1674-1682)
+        const double v = __dmul_rn(static_cast<double>(coh[s]), 1000.0);
+        double r = v >= 0.0 ? floor(__dadd_rn(v, 0.5)) : ceil(__dsub_rn(v, 0.5));
+        r = fmin(fmax(r, 0.0), static_cast<double>(a.lut_len - 1));
+        const int ix = isnan(r) ? 0 : static_cast<int>(r);
+        const double t = 1.0 - a.lut[ix];
+        w = static_cast<R>(t * t);
+        if (chunk == 0 && lane == 0) W[s] = w;
+      } else {
+        w = W[s];
+      }
+      if (active && a.mode == 3) {
+        // accumulate_grid alone: ph_nm holds ph_weight, no ramp and no weight
+        const float2 v = ph[static_cast<int64_t>(s) * M + c];
+        ax = add_rn(ax, static_cast<R>(v.x));
+        ay = add_rn(ay, static_cast<R>(v.y));
+      } else if (active) {
+        const R k = K[s];
+        const R b = a.bp_row_inv ? static_cast<R>(bp[c]) : static_cast<R>(bp[static_cast<int64_t>(s) * M + c]);
+        const R phs = -(b * k);
+        R sn, cs;
+        sincos_r(phs, &sn, &cs);
+        const float2 v = ph[static_cast<int64_t>(s) * M + c];
+        const C r = cmul_rn(mk(static_cast<R>(v.x), static_cast<R>(v.y)), mk(cs, sn));
+        ax = add_rn(ax, mul_rn(r.x, w));
+        ay = add_rn(ay, mul_rn(r.y, w));
+      }
+    }
+    if (c < a.Mp) grid[cell * a.Mp + c] = active ? mk(ax, ay) : mk(R(0), R(0));
+  }
+}
+
+cudaError_t launch_bin(const BinArgs& a, bool fp64, int sm_count, cudaStream_t st) {
+  const int64_t warps = a.G * a.nchunk;
+  int64_t blocks = (warps + 7) / 8;
+  const int64_t cap = static_cast<int64_t>(sm_count) * 16;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  if (fp64)
+    k_bin<double><<<static_cast<unsigned>(blocks), 256, 0, st>>>(a);
+  else
+    k_bin<float><<<static_cast<unsigned>(blocks), 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+// ====================================================================== FFT
+// Radix-2 decimation-in-time FFT of 32 points held in registers (textbook
+// Cooley-Tukey). Forward uses e^{-2 pi i k/32}; inverse the conjugate and no
+// scaling (the 1/1024 is folded into the overlap-add weight, like rustfft's
+// unnormalised inverse followed by inv_scale in the reference).
+template <typename R, bool INV>
+__device__ __forceinline__ void fft32(typename CT<R>::C (&x)[32], const typename CT<R>::Tw& tw) {
+  using C = typename CT<R>::C;
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    const int r = ((i & 1) << 4) | ((i & 2) << 2) | (i & 4) | ((i & 8) >> 2) | ((i & 16) >> 4);
+    if (r > i) {
+      C t = x[i];
+      x[i] = x[r];
+      x[r] = t;
+    }
+  }
+#pragma unroll
+  for (int half = 1; half < 32; half <<= 1) {
+    const int step = 16 / half;
+#pragma unroll
+    for (int s = 0; s < 32; s += 2 * half) {
+#pragma unroll
+      for (int k = 0; k < half; ++k) {
+        const int ti = k * step;
+        const C u = x[s + k];
+        const C v = x[s + k + half];
+        C t;
+        if (ti == 0) {
+          t = v;
+        } else if (ti == 8) {
+          t = INV ? mk(-v.y, v.x) : mk(v.y, -v.x);
+        } else {
+          C w = tw.w[ti];
+          if (INV) w.y = -w.y;
+          t = cmul(v, w);
+        }
+        x[s + k] = mk(u.x + t.x, u.y + t.y);
+        x[s + k + half] = mk(u.x - t.x, u.y - t.y);
+      }
+    }
+  }
+}
+
+// ================================================================== CLAP ==
+template <typename R>
+struct ClapTile {
+  R re[32][33];
+  R im[32][33];
+  R hs[32][33];
+};
+
+__device__ __forceinline__ uint32_t to_bits(float v) { return __float_as_uint(v); }
+__device__ __forceinline__ unsigned long long to_bits(double v) {
+  return static_cast<unsigned long long>(__double_as_longlong(v));
+}
+__device__ __forceinline__ float from_bits(uint32_t u) { return __uint_as_float(u); }
+__device__ __forceinline__ double from_bits(unsigned long long u) {
+  return __longlong_as_double(static_cast<long long>(u));
+}
+__device__ __forceinline__ uint32_t warp_min_u(uint32_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+__device__ __forceinline__ uint32_t warp_max_u(uint32_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+__device__ __forceinline__ unsigned long long warp_min_u(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+__device__ __forceinline__ unsigned long long warp_max_u(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+
+// Median of the 1,024 non-negative values held 32 per lane (median(),
+// native_stage2.rs:1173-1184: mean of the 512th and 513th smallest). Exact
+// order statistic by bisection on the IEEE bit pattern, which orders
+// non-negative floats like their values.
+template <typename R>
+__device__ __forceinline__ R warp_median1024(const R (&o)[32]) {
+  using U = typename CT<R>::U;
+  U lo = to_bits(o[0]), hi = lo;
+#pragma unroll
+  for (int i = 1; i < 32; ++i) {
+    const U u = to_bits(o[i]);
+    lo = min(lo, u);
+    hi = max(hi, u);
+  }
+  lo = warp_min_u(lo);
+  hi = warp_max_u(hi);
+  const int kth = 511;
+  while (lo < hi) {
+    const U mid = lo + ((hi - lo) >> 1);
+    int cnt = 0;
+#pragma unroll
+    for (int i = 0; i < 32; ++i) cnt += (to_bits(o[i]) <= mid) ? 1 : 0;
+    cnt = warp_sum(cnt);
+    if (cnt >= kth + 1)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  int cle = 0;
+  U nxt = ~U(0);
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    const U u = to_bits(o[i]);
+    cle += (u <= lo) ? 1 : 0;
+    if (u > lo) nxt = min(nxt, u);
+  }
+  cle = warp_sum(cle);
+  nxt = warp_min_u(nxt);
+  const R v0 = from_bits(lo);
+  const R v1 = (cle >= kth + 2) ? v0 : from_bits(nxt);
+  return (v0 + v1) * R(0.5);
+}
+
+// One window of one interferogram, computed by one warp in its tile.
+// On entry the tile holds the 24x24 window zero-padded to 32x32; on exit rows
+// and columns < 24 hold the filtered values times the pyramid weight / 1024.
+template <typename R>
+__device__ __forceinline__ void clap_window_warp(ClapTile<R>& T, const int lane, const ClapArgs& a,
+                                                 const typename CT<R>::Tw& tw, const R* lp, const R* wt,
+                                                 const R (&g7)[7], const int rs, const int cs) {
+  using C = typename CT<R>::C;
+  C x[32];
+  // forward FFT along rows (lane = row; rows >= n_win are zero)
+  if (lane < a.n_win) {
+#pragma unroll
+    for (int k = 0; k < 32; ++k) x[k] = mk(T.re[lane][k], T.im[lane][k]);
+    fft32<R, false>(x, tw);
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+      T.re[lane][k] = x[k].x;
+      T.im[lane][k] = x[k].y;
+    }
+  }
+  __syncwarp();
+  // forward FFT along columns (lane = column), |H|
+#pragma unroll
+  for (int k = 0; k < 32; ++k) x[k] = mk(T.re[k][lane], T.im[k][lane]);
+  fft32<R, false>(x, tw);
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    T.re[k][lane] = x[k].x;
+    T.im[k][lane] = x[k].y;
+    T.hs[k][lane] = sqrt(x[k].x * x[k].x + x[k].y * x[k].y);
+  }
+  __syncwarp();
+  // 7x7 separable Gaussian 'same' convolution of fftshift(|H|), then
+  // ifftshift (native_stage2.rs:1097-1166). In unshifted coordinates this is a
+  // circular convolution cut at the Nyquist seam: neighbour k+d is used iff
+  // 0 <= ((k+16) mod 32) + d < 32.
+  R t[32];
+  const int sj = (lane + 16) & 31;
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    R acc = R(0);
+#pragma unroll
+    for (int d = -3; d <= 3; ++d) {
+      if (sj + d >= 0 && sj + d < 32) acc += T.hs[k][(lane + d) & 31] * g7[d + 3];
+    }
+    t[k] = acc;
+  }
+  R o[32];
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    const int sk = (k + 16) & 31;
+    R acc = R(0);
+#pragma unroll
+    for (int d = -3; d <= 3; ++d) {
+      if (sk + d >= 0 && sk + d < 32) acc += t[(k + d) & 31] * g7[d + 3];
+    }
+    o[k] = acc;
+  }
+  const R med = warp_median1024<R>(o);
+  // H <- max((H/med)^alpha - 1, 0); spectrum *= H*beta + low_pass; inverse
+  // FFT along columns in registers.
+  const R beta = static_cast<R>(a.beta);
+  const R alpha = static_cast<R>(a.alpha);
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    R v = o[k];
+    if (med != R(0)) v = v / med;
+    v = a.alpha_is_one ? v - R(1) : pow(v, alpha) - R(1);
+    if (v < R(0)) v = R(0);
+    const R gk = v * beta + lp[k * 32 + lane];
+    x[k] = mk(T.re[k][lane] * gk, T.im[k][lane] * gk);
+  }
+  fft32<R, true>(x, tw);
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    T.re[k][lane] = x[k].x;
+    T.im[k][lane] = x[k].y;
+  }
+  __syncwarp();
+  // inverse FFT along rows; keep the n_win x n_win corner, weighted
+  if (lane < a.n_win) {
+#pragma unroll
+    for (int k = 0; k < 32; ++k) x[k] = mk(T.re[lane][k], T.im[lane][k]);
+    fft32<R, true>(x, tw);
+    const bool row_zero = lane < rs;
+#pragma unroll
+    for (int l = 0; l < 32; ++l) {
+      if (l < a.n_win) {
+        const R wv = (row_zero || l < cs) ? R(0) : wt[(lane - rs) * a.n_win + (l - cs)];
+        T.re[lane][l] = x[l].x * wv;
+        T.im[lane][l] = x[l].y * wv;
+      }
+    }
+  }
+  __syncwarp();
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_clap(ClapArgs a, typename CT<R>::Tw tw) {
+  using C = typename CT<R>::C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ClapTile<R>* tiles = reinterpret_cast<ClapTile<R>*>(smem_raw);
+  R* lp = reinterpret_cast<R*>(tiles + 4);
+  R* wt = lp + 1024;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nw = a.n_win, nw2 = nw * nw;
+  for (int i = tid; i < 1024; i += 128) lp[i] = static_cast<R>(a.low_pass[i]);
+  for (int i = tid; i < nw2; i += 128) wt[i] = static_cast<R>(a.wscaled[i]);
+  R g7[7];
+#pragma unroll
+  for (int i = 0; i < 7; ++i) g7[i] = static_cast<R>(a.g7[i]);
+  const int n_inc = nw / 4 > 1 ? nw / 4 : 1;
+  const int ngroups = a.Mp / 4;
+  const int64_t ntask = static_cast<int64_t>(a.nwi) * a.nwj * ngroups;
+  const C* __restrict__ grid = static_cast<const C*>(a.grid);
+  C* __restrict__ out = static_cast<C*>(a.win_out);
+  ClapTile<R>& T = tiles[warp];
+  for (int64_t task = blockIdx.x; task < ntask; task += gridDim.x) {
+    const int64_t wi = task / ngroups;
+    const int g = static_cast<int>(task - wi * ngroups);
+    const int ix1 = static_cast<int>(wi / a.nwj), ix2 = static_cast<int>(wi - static_cast<int64_t>(ix1) * a.nwj);
+    // clap_windows (native_stage2.rs:957-995)
+    int i1 = ix1 * n_inc, rs = 0;
+    if (i1 + nw > a.n_i) {
+      rs = i1 + nw - a.n_i;
+      i1 = a.n_i - nw;
+    }
+    int j1 = ix2 * n_inc, cs = 0;
+    if (j1 + nw > a.n_j) {
+      cs = j1 + nw - a.n_j;
+      j1 = a.n_j - nw;
+    }
+    __syncthreads();
+    // zero the padding of the four tiles, load the windows (NaN -> 0)
+    for (int idx = tid; idx < 4 * 32 * 32; idx += 128) {
+      const int q = idx >> 10, e = idx & 1023, r = e >> 5, cc = e & 31;
+      if (r >= nw || cc >= nw) {
+        tiles[q].re[r][cc] = R(0);
+        tiles[q].im[r][cc] = R(0);
+      }
+    }
+    for (int idx = tid; idx < nw2 * 4; idx += 128) {
+      const int pix = idx >> 2, q = idx & 3;
+      const int li = pix / nw, lj = pix - li * nw;
+      const int c = 4 * g + q;
+      C v = mk(R(0), R(0));
+      if (c < a.M) {
+        v = grid[(static_cast<int64_t>(i1 + li) * a.n_j + (j1 + lj)) * a.Mp + c];
+        if (isnan(v.x) || isnan(v.y)) v = mk(R(0), R(0));
+      }
+      tiles[q].re[li][lj] = v.x;
+      tiles[q].im[li][lj] = v.y;
+    }
+    __syncthreads();
+    if (4 * g + warp < a.M) clap_window_warp<R>(T, lane, a, tw, lp, wt, g7, rs, cs);
+    __syncthreads();
+    for (int idx = tid; idx < nw2 * 4; idx += 128) {
+      const int pix = idx >> 2, q = idx & 3;
+      const int li = pix / nw, lj = pix - li * nw;
+      out[(wi * nw2 + pix) * a.Mp + 4 * g + q] = mk(tiles[q].re[li][lj], tiles[q].im[li][lj]);
+    }
+  }
+}
+
+template <typename R>
+static size_t clap_smem_bytes() {
+  return 4 * sizeof(ClapTile<R>) + (1024 + 1024) * sizeof(R);
+}
+
+cudaError_t launch_clap(const ClapArgs& a, bool fp64, const Twiddles32f& tf, const Twiddles32d& td, int sm_count,
+                        cudaStream_t st) {
+  const int64_t ntask = static_cast<int64_t>(a.nwi) * a.nwj * (a.Mp / 4);
+  if (ntask <= 0) return cudaSuccess;
+  if (fp64) {
+    const size_t sm = clap_smem_bytes<double>();
+    cudaError_t e = cudaFuncSetAttribute(k_clap<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clap<double>, 128, sm);
+    int64_t blocks = std::min<int64_t>(ntask, static_cast<int64_t>(sm_count) * (per_sm > 0 ? per_sm : 1));
+    k_clap<double><<<static_cast<unsigned>(blocks), 128, sm, st>>>(a, td);
+  } else {
+    const size_t sm = clap_smem_bytes<float>();
+    cudaError_t e = cudaFuncSetAttribute(k_clap<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clap<float>, 128, sm);
+    int64_t blocks = std::min<int64_t>(ntask, static_cast<int64_t>(sm_count) * (per_sm > 0 ? per_sm : 1));
+    k_clap<float><<<static_cast<unsigned>(blocks), 128, sm, st>>>(a, tf);
+  }
+  return cudaGetLastError();
+}
+
+// Overlap-add as a gather: cell (i, j) sums the windows that cover it, in the
+// reference's raster window order, in f64 (the reference accumulates in f64).
+template <typename R>
+__global__ void __launch_bounds__(256) k_overlap(OverlapArgs a) {
+  using C = typename CT<R>::C;
+  const C* __restrict__ win = static_cast<const C*>(a.win_out);
+  C* __restrict__ filt = static_cast<C*>(a.filt);
+  const int64_t total = static_cast<int64_t>(a.n_i) * a.n_j * a.Mp;
+  const int nw = a.n_win, nw2 = nw * nw;
+  for (int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t cell = idx / a.Mp;
+    const int c = static_cast<int>(idx - cell * a.Mp);
+    const int i = static_cast<int>(cell / a.n_j), j = static_cast<int>(cell - static_cast<int64_t>(i) * a.n_j);
+    double sx = 0.0, sy = 0.0;
+    if (c < a.M && a.nwi > 0 && a.nwj > 0) {
+      const int a1 = max(0, i / a.n_inc - 4), b1 = min(a.nwi - 1, i / a.n_inc + 1);
+      const int a2 = max(0, j / a.n_inc - 4), b2 = min(a.nwj - 1, j / a.n_inc + 1);
+      for (int ix1 = a1; ix1 <= b1; ++ix1) {
+        const int i1 = min(ix1 * a.n_inc, a.n_i - nw);
+        const int li = i - i1;
+        if (li < 0 || li >= nw) continue;
+        for (int ix2 = a2; ix2 <= b2; ++ix2) {
+          const int j1 = min(ix2 * a.n_inc, a.n_j - nw);
+          const int lj = j - j1;
+          if (lj < 0 || lj >= nw) continue;
+          const C v = win[((static_cast<int64_t>(ix1) * a.nwj + ix2) * nw2 + li * nw + lj) * a.Mp + c];
+          sx += static_cast<double>(v.x);
+          sy += static_cast<double>(v.y);
+        }
+      }
+    }
+    filt[idx] = mk(static_cast<R>(sx), static_cast<R>(sy));
+  }
+}
+
+cudaError_t launch_overlap(const OverlapArgs& a, bool fp64, cudaStream_t st) {
+  const int64_t total = static_cast<int64_t>(a.n_i) * a.n_j * a.Mp;
+  int64_t blocks = (total + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks < 1) blocks = 1;
+  if (fp64)
+    k_overlap<double><<<static_cast<unsigned>(blocks), 256, 0, st>>>(a);
+  else
+    k_overlap<float><<<static_cast<unsigned>(blocks), 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+// =============================================================== topofit ==
+// Lane l ends with the warp-wide sum of slot (l mod W) of v[]: full xor
+// reductions for the lane bits >= log2(W), then a transposing reduction
+// (each step halves the slots a lane keeps and exchanges the other half).
+template <int W>
+__device__ __forceinline__ float2 transpose_reduce(float2 (&v)[W], const int lane) {
+#pragma unroll
+  for (int o = 16; o >= W; o >>= 1) {
+#pragma unroll
+    for (int i = 0; i < W; ++i) {
+      v[i].x += __shfl_xor_sync(kFull, v[i].x, o);
+      v[i].y += __shfl_xor_sync(kFull, v[i].y, o);
+    }
+  }
+#pragma unroll
+  for (int o = W / 2; o >= 1; o >>= 1) {
+    const bool upper = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < o; ++i) {
+      const float2 lo = v[i], hi = v[i + o];
+      float2 send = upper ? lo : hi;
+      const float2 keep = upper ? hi : lo;
+      send.x = __shfl_xor_sync(kFull, send.x, o);
+      send.y = __shfl_xor_sync(kFull, send.y, o);
+      v[i] = make_float2(keep.x + send.x, keep.y + send.y);
+    }
+  }
+  return v[0];
+}
+
+// W consecutive trial multipliers m0 .. m0+W-1: S_m = sum_c z_c e^{-j th_c m}.
+// The phasor u = z e^{-j th m} advances by one complex multiply per trial and
+// is re-anchored with an exact sincos every 16 trials.
+template <int W, int MAXC>
+__device__ __forceinline__ void trial_block(const float2 (&z)[MAXC], const float (&th)[MAXC], const float2 (&rot)[MAXC],
+                                            const int m0, const int t0, const int T, const int lane, float& best_sq,
+                                            int& best_t) {
+  float2 S[W];
+#pragma unroll
+  for (int k = 0; k < W; ++k) S[k] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int q = 0; q < MAXC; ++q) {
+    float sn, cs;
+    sincosf(th[q] * static_cast<float>(m0), &sn, &cs);
+    float2 u = cmul(z[q], make_float2(cs, -sn));
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      if (k > 0 && (k & 15) == 0) {
+        sincosf(th[q] * static_cast<float>(m0 + k), &sn, &cs);
+        u = cmul(z[q], make_float2(cs, -sn));
+      }
+      S[k].x += u.x;
+      S[k].y += u.y;
+      if (k + 1 < W) u = cmul(u, rot[q]);
+    }
+  }
+  const float2 tot = transpose_reduce<W>(S, lane);
+  const int t = t0 + (lane & (W - 1));
+  if (t < T) {
+    const float sq = tot.x * tot.x + tot.y * tot.y;
+    if (sq > best_sq) {
+      best_sq = sq;
+      best_t = t;
+    }
+  }
+}
+
+constexpr float kQuarterPiF = 3.14159265358979323846f / 4.0f;  // Rust std::f32::consts::PI / 4.0
+
+template <int MAXC>
+__global__ void __launch_bounds__(256, 2) k_topofit_f32(TopoArgs a) {
+  __shared__ int sh_hist[kCohBins];
+  __shared__ double sh_rms[8];
+  __shared__ int sh_inv[8];
+  const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
+  for (int i = tid; i < kCohBins; i += blockDim.x) sh_hist[i] = 0;
+  __syncthreads();
+  const float2* __restrict__ ph_nm = static_cast<const float2*>(a.ph_nm);
+  const float2* __restrict__ filt = static_cast<const float2*>(a.filt);
+  const float2* __restrict__ cpx = static_cast<const float2*>(a.cpx);
+  float* __restrict__ K_out = static_cast<float*>(a.K_out);
+  float* __restrict__ C_out = static_cast<float*>(a.C_out);
+  float* __restrict__ coh_io = static_cast<float*>(a.coh_io);
+  float2* __restrict__ resid = static_cast<float2*>(a.residual);
+  float* __restrict__ ph_res = static_cast<float*>(a.ph_res);
+  float2* __restrict__ ph_patch = static_cast<float2*>(a.ph_patch);
+  const int64_t M = a.M;
+  const int T = 2 * a.n_half + 1;
+  double rms_acc = 0.0;
+  int inv_acc = 0;
+  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + tid) >> 5;
+  const int64_t nwarps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t s = gw; s < a.N; s += nwarps) {
+    float2 z[MAXC];
+    float bpv[MAXC];
+    bool zero = false, nonzero = false;
+    const int64_t cell = cpx ? 0 : a.cell_of[s];
+#pragma unroll
+    for (int q = 0; q < MAXC; ++q) {
+      const int c = lane + 32 * q;
+      z[q] = make_float2(0.f, 0.f);
+      bpv[q] = 0.f;
+      if (c < a.M) {
+        float2 v;
+        if (cpx) {
+          v = cpx[s * M + c];
+        } else {
+          // extract_patch_phase + normalize_complex_unit_magnitude (:1186-1205)
+          float2 f = filt[cell * a.Mp + c];
+          const float mag = hypotf(f.x, f.y);
+          if (mag != 0.f) f = make_float2(f.x / mag, f.y / mag);
+          if (ph_patch) ph_patch[s * M + c] = f;
+          v = cmul_rn(conjf2(f), ph_nm[s * M + c]);  // psdph (:687-689)
+        }
+        z[q] = v;
+        bpv[q] = a.bp_row_inv ? a.bp[c] : a.bp[s * M + c];
+        if (v.x == 0.f && v.y == 0.f)
+          zero = true;
+        else
+          nonzero = true;
+      }
+    }
+    const bool any_zero = __any_sync(kFull, zero);
+    const bool any_nonzero = __any_sync(kFull, nonzero);
+    const bool invalid = a.zero_mode == 0 ? any_zero : !any_nonzero;
+    float Kv, Cv, cohv;
+    if (invalid) {
+      // fit_stage2_rows invalid row (:676-697) / topofit_row empty row (:1216-1222)
+      Kv = __int_as_float(0x7fffffff);
+      Cv = a.zero_mode == 0 ? 0.f : Kv;
+      cohv = a.zero_mode == 0 ? 0.f : Kv;
+#pragma unroll
+      for (int q = 0; q < MAXC; ++q) {
+        const int c = lane + 32 * q;
+        if (c < a.M) {
+          if (resid) resid[s * M + c] = make_float2(0.f, 0.f);
+          if (ph_res) ph_res[s * M + c] = 0.f;
+        }
+      }
+      inv_acc += 1;
+    } else {
+      // topofit_row (:1207-1257) over the non-zero columns
+      float mn = __int_as_float(0x7f800000), mx = -mn;
+#pragma unroll
+      for (int q = 0; q < MAXC; ++q) {
+        if (lane + 32 * q < a.M && (z[q].x != 0.f || z[q].y != 0.f)) {
+          mn = fminf(mn, bpv[q]);
+          mx = fmaxf(mx, bpv[q]);
+        }
+      }
+      mn = warp_min(mn);
+      mx = warp_max(mx);
+      float range = mx - mn;
+      if (range == 0.f) range = 1.f;
+      float th[MAXC];
+      float2 rot[MAXC];
+#pragma unroll
+      for (int q = 0; q < MAXC; ++q) {
+        th[q] = (bpv[q] / range) * kQuarterPiF;
+        float sn, cs;
+        sincosf(th[q], &sn, &cs);
+        rot[q] = make_float2(cs, -sn);
+      }
+      float best_sq = -1.f;
+      int best_t = 0;
+      int t0 = 0;
+      for (; T - t0 >= 32; t0 += 32) trial_block<32, MAXC>(z, th, rot, t0 - a.n_half, t0, T, lane, best_sq, best_t);
+      if (T - t0 >= 16) {
+        trial_block<16, MAXC>(z, th, rot, t0 - a.n_half, t0, T, lane, best_sq, best_t);
+        t0 += 16;
+      }
+      if (T - t0 >= 8) {
+        trial_block<8, MAXC>(z, th, rot, t0 - a.n_half, t0, T, lane, best_sq, best_t);
+        t0 += 8;
+      }
+      if (T - t0 >= 4) {
+        trial_block<4, MAXC>(z, th, rot, t0 - a.n_half, t0, T, lane, best_sq, best_t);
+        t0 += 4;
+      }
+      if (T - t0 >= 2) {
+        trial_block<2, MAXC>(z, th, rot, t0 - a.n_half, t0, T, lane, best_sq, best_t);
+        t0 += 2;
+      }
+      if (T - t0 >= 1) {
+        trial_block<1, MAXC>(z, th, rot, t0 - a.n_half, t0, T, lane, best_sq, best_t);
+        t0 += 1;
+      }
+      // first maximum over the warp (argmax_first_f32, :1526-1536)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const float osq = __shfl_xor_sync(kFull, best_sq, o);
+        const int ot = __shfl_xor_sync(kFull, best_t, o);
+        if (osq > best_sq || (osq == best_sq && ot < best_t)) {
+          best_sq = osq;
+          best_t = ot;
+        }
+      }
+      // refine_candidate (:1259-1303); FP64 normal equations
+      const float k0 = kQuarterPiF / range * static_cast<float>(best_t - a.n_half);
+      float2 res[MAXC];
+      float ox = 0.f, oy = 0.f;
+#pragma unroll
+      for (int q = 0; q < MAXC; ++q) {
+        float sn, cs;
+        sincosf(k0 * bpv[q], &sn, &cs);
+        res[q] = cmul_rn(z[q], make_float2(cs, -sn));
+        ox += res[q].x;
+        oy += res[q].y;
+      }
+      ox = warp_sum(ox);
+      oy = warp_sum(oy);
+      const float2 oc = make_float2(ox, -oy);
+      double mopt = 0.0, dl = 0.0;
+#pragma unroll
+      for (int q = 0; q < MAXC; ++q) {
+        const double wgt = static_cast<double>(hypotf(z[q].x, z[q].y));
+        const double wb = __dmul_rn(wgt, static_cast<double>(bpv[q]));
+        dl = __dadd_rn(dl, __dmul_rn(wb, wb));
+        const float2 r = cmul_rn(res[q], oc);
+        const double ang = static_cast<double>(atan2f(r.y, r.x));
+        mopt = __dadd_rn(mopt, __dmul_rn(wb, __dmul_rn(wgt, ang)));
+      }
+      mopt = warp_sum(mopt);
+      dl = warp_sum(dl);
+      if (dl == 0.0) dl = 1.0;
+      const float K1 = static_cast<float>(static_cast<double>(k0) + mopt / dl);
+      float mx2 = 0.f, my2 = 0.f, den2 = 0.f;
+#pragma unroll
+      for (int q = 0; q < MAXC; ++q) {
+        float sn, cs;
+        sincosf(K1 * bpv[q], &sn, &cs);
+        const float2 r = cmul_rn(z[q], make_float2(cs, -sn));
+        mx2 += r.x;
+        my2 += r.y;
+        den2 += hypotf(r.x, r.y);
+        const int c = lane + 32 * q;
+        if (c < a.M) {
+          if (resid) resid[s * M + c] = r;
+          if (ph_res) ph_res[s * M + c] = atan2f(r.y, r.x);
+        }
+      }
+      mx2 = warp_sum(mx2);
+      my2 = warp_sum(my2);
+      den2 = warp_sum(den2);
+      if (den2 == 0.f) den2 = 1.f;
+      Kv = K1;
+      Cv = atan2f(my2, mx2);
+      cohv = hypotf(mx2, my2) / den2;
+    }
+    if (lane == 0) {
+      if (a.accumulate_stats) {
+        const double d = static_cast<double>(cohv) - static_cast<double>(coh_io[s]);
+        rms_acc += d * d;
+        const int b = coh_bin(static_cast<double>(cohv), a.cutoff0, a.dbin);
+        if (b >= 0) atomicAdd(&sh_hist[b], 1);
+      }
+      K_out[s] = Kv;
+      C_out[s] = Cv;
+      coh_io[s] = cohv;
+      if (a.nopt) a.nopt[s] = invalid ? 0 : 1;
+    }
+  }
+  if (!a.accumulate_stats) return;
+  if (lane == 0) {
+    sh_rms[wib] = rms_acc;
+    sh_inv[wib] = inv_acc;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+    int iv = 0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
+      t += sh_rms[w];
+      iv += sh_inv[w];
+    }
+    a.rms_partial[blockIdx.x] = t;
+    if (iv) atomicAdd(a.n_invalid, iv);
+  }
+  for (int i = tid; i < kCohBins; i += blockDim.x)
+    if (sh_hist[i]) atomicAdd(&a.hist[i], sh_hist[i]);
+}
+
+// Plain FP64 topofit: direct sincos for every (trial, column), lanes over
+// trials for the sweep and over columns for the refinement. This is the
+// comparison path; it shares only the data layout with the FP32 kernel.
+__global__ void __launch_bounds__(256) k_topofit_f64(TopoArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
+  double2* zs = reinterpret_cast<double2*>(smem_raw) + static_cast<int64_t>(wib) * a.M;
+  double* ths = reinterpret_cast<double*>(reinterpret_cast<double2*>(smem_raw) + 8 * a.M) + static_cast<int64_t>(wib) * a.M;
+  __shared__ int sh_hist[kCohBins];
+  __shared__ double sh_rms[8];
+  __shared__ int sh_inv[8];
+  for (int i = tid; i < kCohBins; i += blockDim.x) sh_hist[i] = 0;
+  __syncthreads();
+  const float2* __restrict__ ph_nm = static_cast<const float2*>(a.ph_nm);
+  const double2* __restrict__ filt = static_cast<const double2*>(a.filt);
+  double* K_out = static_cast<double*>(a.K_out);
+  double* C_out = static_cast<double*>(a.C_out);
+  double* coh_io = static_cast<double*>(a.coh_io);
+  double2* resid = static_cast<double2*>(a.residual);
+  double* ph_res = static_cast<double*>(a.ph_res);
+  double2* ph_patch = static_cast<double2*>(a.ph_patch);
+  const int64_t M = a.M;
+  const int T = 2 * a.n_half + 1;
+  const double qpi = 3.14159265358979323846 / 4.0;
+  double rms_acc = 0.0;
+  int inv_acc = 0;
+  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + tid) >> 5;
+  const int64_t nwarps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t s = gw; s < a.N; s += nwarps) {
+    const int64_t cell = a.cell_of[s];
+    bool zero = false;
+    double mn = INFINITY, mx = -INFINITY;
+    for (int c = lane; c < a.M; c += 32) {
+      double2 f = filt[cell * a.Mp + c];
+      const double mag = hypot(f.x, f.y);
+      if (mag != 0.0) f = make_double2(f.x / mag, f.y / mag);
+      if (ph_patch) ph_patch[s * M + c] = f;
+      const float2 p = ph_nm[s * M + c];
+      const double2 v = cmul_rn(conjd2(f), make_double2(p.x, p.y));
+      zs[c] = v;
+      if (v.x == 0.0 && v.y == 0.0) zero = true;
+      const double b = a.bp_row_inv ? static_cast<double>(a.bp[c]) : static_cast<double>(a.bp[s * M + c]);
+      ths[c] = b;
+      mn = fmin(mn, b);
+      mx = fmax(mx, b);
+    }
+    const bool invalid = __any_sync(kFull, zero);
+    double Kv, Cv, cohv;
+    if (invalid) {
+      Kv = __longlong_as_double(0x7ff8000000000000LL);
+      Cv = 0.0;
+      cohv = 0.0;
+      for (int c = lane; c < a.M; c += 32) {
+        if (resid) resid[s * M + c] = make_double2(0.0, 0.0);
+        if (ph_res) ph_res[s * M + c] = 0.0;
+      }
+      inv_acc += 1;
+    } else {
+      mn = warp_min(mn);
+      mx = warp_max(mx);
+      double range = mx - mn;
+      if (range == 0.0) range = 1.0;
+      __syncwarp();
+      for (int c = lane; c < a.M; c += 32) ths[c] = (ths[c] / range) * qpi;  // keeps bp in registers below
+      __syncwarp();
+      double best = -1.0;
+      int bt = 0;
+      for (int t = lane; t < T; t += 32) {
+        const double m = static_cast<double>(t - a.n_half);
+        double sx = 0.0, sy = 0.0;
+        for (int c = 0; c < a.M; ++c) {
+          double sn, cs;
+          sincos(ths[c] * m, &sn, &cs);
+          const double2 zz = zs[c];
+          sx += zz.x * cs + zz.y * sn;
+          sy += zz.y * cs - zz.x * sn;
+        }
+        const double sq = sx * sx + sy * sy;
+        if (sq > best) {
+          best = sq;
+          bt = t;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(kFull, best, o);
+        const int ot = __shfl_xor_sync(kFull, bt, o);
+        if (ob > best || (ob == best && ot < bt)) {
+          best = ob;
+          bt = ot;
+        }
+      }
+      const double k0 = qpi / range * static_cast<double>(bt - a.n_half);
+      double ox = 0.0, oy = 0.0;
+      for (int c = lane; c < a.M; c += 32) {
+        const double b = a.bp_row_inv ? static_cast<double>(a.bp[c]) : static_cast<double>(a.bp[s * M + c]);
+        double sn, cs;
+        sincos(k0 * b, &sn, &cs);
+        const double2 r = cmul_rn(zs[c], make_double2(cs, -sn));
+        ox += r.x;
+        oy += r.y;
+      }
+      ox = warp_sum(ox);
+      oy = warp_sum(oy);
+      double mopt = 0.0, dl = 0.0;
+      for (int c = lane; c < a.M; c += 32) {
+        const double b = a.bp_row_inv ? static_cast<double>(a.bp[c]) : static_cast<double>(a.bp[s * M + c]);
+        double sn, cs;
+        sincos(k0 * b, &sn, &cs);
+        const double2 r = cmul_rn(zs[c], make_double2(cs, -sn));
+        const double wgt = hypot(zs[c].x, zs[c].y);
+        const double wb = wgt * b;
+        dl += wb * wb;
+        const double2 q = cmul_rn(r, make_double2(ox, -oy));
+        mopt += wb * (wgt * atan2(q.y, q.x));
+      }
+      mopt = warp_sum(mopt);
+      dl = warp_sum(dl);
+      if (dl == 0.0) dl = 1.0;
+      const double K1 = k0 + mopt / dl;
+      double mx2 = 0.0, my2 = 0.0, den2 = 0.0;
+      for (int c = lane; c < a.M; c += 32) {
+        const double b = a.bp_row_inv ? static_cast<double>(a.bp[c]) : static_cast<double>(a.bp[s * M + c]);
+        double sn, cs;
+        sincos(K1 * b, &sn, &cs);
+        const double2 r = cmul_rn(zs[c], make_double2(cs, -sn));
+        mx2 += r.x;
+        my2 += r.y;
+        den2 += hypot(r.x, r.y);
+        if (resid) resid[s * M + c] = r;
+        if (ph_res) ph_res[s * M + c] = atan2(r.y, r.x);
+      }
+      mx2 = warp_sum(mx2);
+      my2 = warp_sum(my2);
+      den2 = warp_sum(den2);
+      if (den2 == 0.0) den2 = 1.0;
+      Kv = K1;
+      Cv = atan2(my2, mx2);
+      cohv = hypot(mx2, my2) / den2;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      if (a.accumulate_stats) {
+        const double d = cohv - coh_io[s];
+        rms_acc += d * d;
+        const int b = coh_bin(cohv, a.cutoff0, a.dbin);
+        if (b >= 0) atomicAdd(&sh_hist[b], 1);
+      }
+      K_out[s] = Kv;
+      C_out[s] = Cv;
+      coh_io[s] = cohv;
+      if (a.nopt) a.nopt[s] = invalid ? 0 : 1;
+    }
+  }
+  if (!a.accumulate_stats) return;
+  if (lane == 0) {
+    sh_rms[wib] = rms_acc;
+    sh_inv[wib] = inv_acc;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+    int iv = 0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
+      t += sh_rms[w];
+      iv += sh_inv[w];
+    }
+    a.rms_partial[blockIdx.x] = t;
+    if (iv) atomicAdd(a.n_invalid, iv);
+  }
+  for (int i = tid; i < kCohBins; i += blockDim.x)
+    if (sh_hist[i]) atomicAdd(&a.hist[i], sh_hist[i]);
+}
+
+int topofit_grid_blocks(int sm_count, bool fp64) { return sm_count * (fp64 ? 4 : 2); }
+
+cudaError_t launch_topofit(const TopoArgs& a, bool fp64, int grid_blocks, cudaStream_t st) {
+  if (a.N <= 0) return cudaSuccess;
+  int64_t need = (a.N + 7) / 8;
+  const int blocks = static_cast<int>(need < grid_blocks ? need : grid_blocks);
+  if (fp64) {
+    const size_t sm = static_cast<size_t>(8) * a.M * (sizeof(double2) + sizeof(double));
+    cudaError_t e = cudaFuncSetAttribute(k_topofit_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_topofit_f64<<<blocks, 256, sm, st>>>(a);
+    return cudaGetLastError();
+  }
+  const int maxc = (a.M + 31) / 32;
+  switch (maxc) {
+    case 1: k_topofit_f32<1><<<blocks, 256, 0, st>>>(a); break;
+    case 2: k_topofit_f32<2><<<blocks, 256, 0, st>>>(a); break;
+    case 3: k_topofit_f32<3><<<blocks, 256, 0, st>>>(a); break;
+    case 4: k_topofit_f32<4><<<blocks, 256, 0, st>>>(a); break;
+    case 5: k_topofit_f32<5><<<blocks, 256, 0, st>>>(a); break;
+    case 6: k_topofit_f32<6><<<blocks, 256, 0, st>>>(a); break;
+    case 7: k_topofit_f32<7><<<blocks, 256, 0, st>>>(a); break;
+    case 8: k_topofit_f32<8><<<blocks, 256, 0, st>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+// ============================================================= finalize ===
+// rms_difference + stop rule (:307-313, :2045-2057); when continuing, the
+// P-square update (:364-381, :1642-1683) producing the prand_hi table that the
+// next k_bin turns into weights. Sums use explicit _rn arithmetic and the
+// reference's order so the table matches the reference given equal inputs.
+__global__ void __launch_bounds__(256) k_finalize(FinalizeArgs a) {
+  __shared__ double sh[256];
+  __shared__ double na[kCohBins], prand[kCohBins], interp_in[kCohBins + 1];
+  __shared__ double scale_s;
+  __shared__ int go_on;
+  const int tid = threadIdx.x;
+  double s = 0.0;
+  for (int i = tid; i < a.n_partial; i += 256) s += a.rms_partial[i];
+  sh[tid] = s;
+  if (tid < kCohBins) na[tid] = static_cast<double>(a.hist[tid]);
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (tid < w) sh[tid] += sh[tid + w];
+    __syncthreads();
+  }
+  if (tid == 0) {
+    const double rms = sqrt(sh[0] / static_cast<double>(a.N > 0 ? a.N : 1));
+    const double gcs = a.state[0];
+    const double delta = rms - gcs;
+    const int64_t i_loop = static_cast<int64_t>(a.state[1]);
+    const int64_t cap = a.gamma_max_iterations > 1 ? a.gamma_max_iterations : 1;
+    const bool stop = fabs(delta) < a.gamma_change_convergence || i_loop >= cap;
+    a.state[0] = rms;
+    a.state[1] = static_cast<double>(i_loop + 1);
+    a.state[2] = rms;
+    a.state[3] = delta;
+    a.stats_out[0] = static_cast<double>(i_loop);
+    a.stats_out[1] = rms;
+    a.stats_out[2] = delta;
+    a.stats_out[3] = stop ? 1.0 : 0.0;
+    a.stats_out[4] = static_cast<double>(*a.n_invalid);
+    go_on = ((!stop || a.force_continue) && a.psquare) ? 1 : 0;
+    if (go_on) {
+      // Nr rescaled so its low-coherence mass matches Na's (sequential sums)
+      double den = 0.0;
+      for (int i = 0; i < a.low_coh_thresh; ++i) den = __dadd_rn(den, a.nr_scaled[i]);
+      double sc = 1.0;
+      if (den > 0.0) {
+        double num = 0.0;
+        for (int i = 0; i < a.low_coh_thresh; ++i) num = __dadd_rn(num, na[i]);
+        sc = num / den;
+      }
+      scale_s = sc;
+      interp_in[0] = 1.0;
+    }
+  }
+  __syncthreads();
+  if (!go_on) return;
+  if (tid < kCohBins) {
+    const double nrv = __dmul_rn(a.nr_scaled[tid], scale_s);
+    a.nr_scaled[tid] = nrv;
+    const double d = na[tid] == 0.0 ? 1.0 : na[tid];
+    double p = fmin(nrv / d, 1.0);
+    if (tid < a.low_coh_thresh) p = 1.0;
+    if (tid >= static_cast<int>(a.nr_max_nz_ix)) p = 0.0;
+    prand[tid] = p;
+  }
+  __syncthreads();
+  // lfilter(gausswin, [1]*7 ++ prand), shifted by 7, / sum(gausswin)
+  if (tid < kCohBins) {
+    const int ix = tid + 7;
+    double acc = 0.0;
+    for (int k = 0; k < 7; ++k) {
+      const int j = ix - k;
+      const double v = j < 7 ? 1.0 : prand[j - 7];
+      acc = __dadd_rn(acc, __dmul_rn(a.g7w[k], v));
+    }
+    interp_in[1 + tid] = acc / a.g7sum;
+  }
+  __syncthreads();
+  // matlab_interp(.., 10) with the 79-tap FIR, delay 39, tail trimmed to 1001
+  for (int i = tid; i < 1001; i += 256) {
+    const int n = i + 39;
+    double acc = 0.0;
+    for (int k = 0; k < 79; ++k) {
+      const int p = n - k;
+      if (p < 0) continue;
+      const double v = (p % 10 == 0 && p / 10 < 101) ? interp_in[p / 10] : 0.0;
+      acc = __dadd_rn(acc, __dmul_rn(a.taps79[k], v));
+    }
+    a.lut[i] = __dmul_rn(acc, 10.0);
+  }
+}
+
+cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t st) {
+  k_finalize<<<1, 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+// ========================================================= SNR weighting ==
+// snr_weighting (:1875-1897) from the residual phase written by the last
+// topofit: w = g / sqrt(0.5 (mean amp^2 - g^2)), g = mean(amp cos(ph_res)).
+template <typename R>
+__global__ void __launch_bounds__(256) k_snr_weight(const R* ph_res, const float* amp, int64_t N, int M, R* w_out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t s = gw; s < N; s += nw) {
+    double g = 0.0, a2 = 0.0;
+    for (int c = lane; c < M; c += 32) {
+      const double am = static_cast<double>(amp[s * M + c]);
+      g += am * cos(static_cast<double>(ph_res[s * M + c]));
+      a2 += am * am;
+    }
+    g = warp_sum(g);
+    a2 = warp_sum(a2);
+    if (lane == 0) {
+      const double mm = static_cast<double>(M > 0 ? M : 1);
+      g /= mm;
+      a2 /= mm;
+      const double sig = sqrt(0.5 * (a2 - g * g));
+      w_out[s] = static_cast<R>(sig != 0.0 ? g / sig : 0.0);
+    }
+  }
+}
+
+cudaError_t launch_snr_weight(const TopoArgs& t, const float* amp, void* w_out, bool fp64, int sm_count,
+                              cudaStream_t st) {
+  const int blocks = sm_count * 8;
+  if (fp64)
+    k_snr_weight<double><<<blocks, 256, 0, st>>>(static_cast<const double*>(t.ph_res), amp, t.N, t.M,
+                                                 static_cast<double*>(w_out));
+  else
+    k_snr_weight<float><<<blocks, 256, 0, st>>>(static_cast<const float*>(t.ph_res), amp, t.N, t.M,
+                                                static_cast<float*>(w_out));
+  return cudaGetLastError();
+}
+
+// ============================================== random-phase histogram ====
+// random_coherence_histogram / topofit_phase_row_coh (:1310-1512) in FP64:
+// one warp per random row, lanes over trials for the sweep (each lane sums its
+// trial over the columns in the reference's order), lanes over columns for the
+// refinement with the sums taken in column order by lane 0.
+__global__ void __launch_bounds__(256) k_random_hist(const double* __restrict__ rnd, int64_t n_rand,
+                                                     const double* __restrict__ bp, int m,
+                                                     const int64_t* __restrict__ ia, const int64_t* __restrict__ ib,
+                                                     int small_baseline, int n_half, double cutoff0, double dbin,
+                                                     int32_t* hist) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
+  double* ph = reinterpret_cast<double*>(smem_raw) + static_cast<int64_t>(wib) * 3 * m;
+  double* t1 = ph + m;
+  double* t2 = t1 + m;
+  __shared__ int sh_hist[kCohBins];
+  for (int i = tid; i < kCohBins; i += blockDim.x) sh_hist[i] = 0;
+  __syncthreads();
+  const int T = 2 * n_half + 1;
+  double mn = INFINITY, mx = -INFINITY;
+  for (int c = 0; c < m; ++c) {
+    mn = fmin(mn, bp[c]);
+    mx = fmax(mx, bp[c]);
+  }
+  double range = mx - mn;
+  if (range == 0.0) range = 1.0;
+  const double qpi = 3.14159265358979323846 / 4.0;
+  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + tid) >> 5;
+  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t row = gw; row < n_rand; row += nw) {
+    __syncwarp();
+    for (int c = lane; c < m; c += 32)
+      ph[c] = small_baseline ? rnd[row + ib[c] * n_rand] - rnd[row + ia[c] * n_rand] : rnd[row + c * n_rand];
+    __syncwarp();
+    double best = -1.0;
+    int bt = 0;
+    for (int t = lane; t < T; t += 32) {
+      const double trial = static_cast<double>(t - n_half);
+      double sre = 0.0, sim = 0.0;
+      for (int c = 0; c < m; ++c) {
+        const double p = __dsub_rn(ph[c], __dmul_rn(__dmul_rn(bp[c] / range, qpi), trial));
+        double sn, cs;
+        sincos(p, &sn, &cs);
+        sre = __dadd_rn(sre, cs);
+        sim = __dadd_rn(sim, sn);
+      }
+      const double v = hypot(sre, sim) / static_cast<double>(m);
+      if (v > best) {
+        best = v;
+        bt = t;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(kFull, best, o);
+      const int ot = __shfl_xor_sync(kFull, bt, o);
+      if (ob > best || (ob == best && ot < bt)) {
+        best = ob;
+        bt = ot;
+      }
+    }
+    const double k0 = qpi / range * static_cast<double>(bt - n_half);
+    for (int c = lane; c < m; c += 32) {
+      double sn, cs;
+      sincos(__dsub_rn(ph[c], __dmul_rn(k0, bp[c])), &sn, &cs);
+      t1[c] = cs;
+      t2[c] = sn;
+    }
+    __syncwarp();
+    double ore = 0.0, oim = 0.0;
+    for (int c = 0; c < m; ++c) {
+      ore = __dadd_rn(ore, t1[c]);
+      oim = __dadd_rn(oim, t2[c]);
+    }
+    __syncwarp();
+    for (int c = lane; c < m; c += 32) {
+      const double cs = t1[c], sn = t2[c];
+      const double pre = __dsub_rn(__dmul_rn(cs, ore), __dmul_rn(sn, -oim));
+      const double pim = __dadd_rn(__dmul_rn(cs, -oim), __dmul_rn(sn, ore));
+      t1[c] = __dmul_rn(bp[c], atan2(pim, pre));
+      t2[c] = __dmul_rn(bp[c], bp[c]);
+    }
+    __syncwarp();
+    double mopt = 0.0, den = 0.0;
+    for (int c = 0; c < m; ++c) {
+      den = __dadd_rn(den, t2[c]);
+      mopt = __dadd_rn(mopt, t1[c]);
+    }
+    if (den == 0.0) den = 1.0;
+    const double k = k0 + mopt / den;
+    __syncwarp();
+    for (int c = lane; c < m; c += 32) {
+      double sn, cs;
+      sincos(__dsub_rn(ph[c], __dmul_rn(k, bp[c])), &sn, &cs);
+      t1[c] = cs;
+      t2[c] = sn;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      double sre = 0.0, sim = 0.0;
+      for (int c = 0; c < m; ++c) {
+        sre = __dadd_rn(sre, t1[c]);
+        sim = __dadd_rn(sim, t2[c]);
+      }
+      const double coh = hypot(sre, sim) / static_cast<double>(m > 1 ? m : 1);
+      const int b = coh_bin(coh, cutoff0, dbin);
+      if (b >= 0) atomicAdd(&sh_hist[b], 1);
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < kCohBins; i += blockDim.x)
+    if (sh_hist[i]) atomicAdd(&hist[i], sh_hist[i]);
+}
+
+cudaError_t launch_random_hist(const double* rnd, int64_t n_rand, const double* bp, int m, const int64_t* ia,
+                               const int64_t* ib, int small_baseline, int n_half, double cutoff0, double dbin,
+                               int32_t* hist, int sm_count, cudaStream_t st) {
+  const size_t sm = static_cast<size_t>(8) * 3 * m * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(k_random_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  int64_t blocks = (n_rand + 7) / 8;
+  if (blocks > static_cast<int64_t>(sm_count) * 8) blocks = static_cast<int64_t>(sm_count) * 8;
+  if (blocks < 1) blocks = 1;
+  k_random_hist<<<static_cast<unsigned>(blocks), 256, sm, st>>>(rnd, n_rand, bp, m, ia, ib, small_baseline, n_half,
+                                                                cutoff0, dbin, hist);
+  return cudaGetLastError();
+}
+
+// ============================================================== layout ====
+// Row gathers/scatters in 4-byte words (row_bytes is a multiple of 4).
+__global__ void k_gather_rows(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
+                              const int32_t* __restrict__ perm, int64_t n, int64_t words, int scatter) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t s = gw; s < n; s += nw) {
+    const int64_t r = perm[s];
+    const uint32_t* a = scatter ? src + s * words : src + r * words;
+    uint32_t* b = scatter ? dst + r * words : dst + s * words;
+    for (int64_t k = lane; k < words; k += 32) b[k] = a[k];
+  }
+}
+
+static cudaError_t gather_impl(const void* src, void* dst, const int32_t* perm, int64_t n, int64_t row_bytes,
+                               int scatter, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  if (row_bytes % 4) return cudaErrorInvalidValue;
+  int64_t blocks = (n + 7) / 8;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_gather_rows<<<static_cast<unsigned>(blocks), 256, 0, st>>>(static_cast<const uint32_t*>(src),
+                                                               static_cast<uint32_t*>(dst), perm, n, row_bytes / 4,
+                                                               scatter);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_rows(const void* src, void* dst, const int32_t* perm, int64_t n, int64_t row_bytes,
+                               cudaStream_t st) {
+  return gather_impl(src, dst, perm, n, row_bytes, 0, st);
+}
+cudaError_t launch_scatter_rows(const void* src, void* dst, const int32_t* perm, int64_t n, int64_t row_bytes,
+                                cudaStream_t st) {
+  return gather_impl(src, dst, perm, n, row_bytes, 1, st);
+}
+
+__global__ void k_repad(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int64_t G, int M, int Mp, int eb,
+                        int to_padded) {
+  const int64_t total = G * static_cast<int64_t>(to_padded ? Mp : M) * eb;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t e = i / eb, byte = i - e * eb;
+    if (to_padded) {
+      const int64_t g = e / Mp, c = e - g * Mp;
+      dst[i] = c < M ? src[(g * M + c) * eb + byte] : 0;
+    } else {
+      const int64_t g = e / M, c = e - g * M;
+      dst[i] = src[(g * Mp + c) * eb + byte];
+    }
+  }
+}
+
+cudaError_t launch_unpad_grid(const void* src, void* dst, int64_t G, int M, int Mp, int eb, cudaStream_t st) {
+  k_repad<<<148 * 8, 256, 0, st>>>(static_cast<const uint8_t*>(src), static_cast<uint8_t*>(dst), G, M, Mp, eb, 0);
+  return cudaGetLastError();
+}
+cudaError_t launch_pad_grid(const void* src, void* dst, int64_t G, int M, int Mp, int eb, cudaStream_t st) {
+  k_repad<<<148 * 8, 256, 0, st>>>(static_cast<const uint8_t*>(src), static_cast<uint8_t*>(dst), G, M, Mp, eb, 1);
+  return cudaGetLastError();
+}
+
+template <typename R>
+__global__ void k_init_state(const double* __restrict__ w0, const int32_t* __restrict__ perm, int64_t N, R* K, R* w,
+                             R* coh) {
+  for (int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; s < N;
+       s += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    K[s] = R(0);
+    w[s] = static_cast<R>(w0[perm[s]]);
+    coh[s] = R(0);
+  }
+}
+
+cudaError_t launch_init_state(const double* w0, const int32_t* perm, int64_t N, void* K, void* w, void* coh,
+                              bool fp64, cudaStream_t st) {
+  if (fp64)
+    k_init_state<double><<<148 * 4, 256, 0, st>>>(w0, perm, N, static_cast<double*>(K), static_cast<double*>(w),
+                                                  static_cast<double*>(coh));
+  else
+    k_init_state<float><<<148 * 4, 256, 0, st>>>(w0, perm, N, static_cast<float*>(K), static_cast<float*>(w),
+                                                 static_cast<float*>(coh));
+  return cudaGetLastError();
+}
+
+// ph_weight of the last iteration (fill_phase_weight with the K and w that
+// iteration used), written in the caller's row order.
+template <typename R>
+__global__ void k_ph_weight(BinArgs a, const int32_t* __restrict__ perm, int64_t N,
+                            typename CT<R>::C* __restrict__ out) {
+  using C = typename CT<R>::C;
+  const float2* ph = static_cast<const float2*>(a.ph_nm);
+  const R* K = static_cast<const R*>(a.K);
+  const R* W = static_cast<const R*>(a.w);
+  const int64_t total = N * a.M;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t s = i / a.M;
+    const int c = static_cast<int>(i - s * a.M);
+    const R b = a.bp_row_inv ? static_cast<R>(a.bp[c]) : static_cast<R>(a.bp[i]);
+    const R phs = -(b * K[s]);
+    R sn, cs;
+    sincos_r(phs, &sn, &cs);
+    const float2 v = ph[i];
+    const C r = cmul_rn(mk(static_cast<R>(v.x), static_cast<R>(v.y)), mk(cs, sn));
+    out[static_cast<int64_t>(perm[s]) * a.M + c] = mk(mul_rn(r.x, W[s]), mul_rn(r.y, W[s]));
+  }
+}
+
+cudaError_t launch_ph_weight(const BinArgs& a, int64_t N, bool fp64, const int32_t* perm, void* out_orig,
+                             cudaStream_t st) {
+  if (fp64)
+    k_ph_weight<double><<<148 * 8, 256, 0, st>>>(a, perm, N, static_cast<double2*>(out_orig));
+  else
+    k_ph_weight<float><<<148 * 8, 256, 0, st>>>(a, perm, N, static_cast<float2*>(out_orig));
+  return cudaGetLastError();
+}
+
+}  // namespace ps2

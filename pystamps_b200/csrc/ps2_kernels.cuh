@@ -1,0 +1,132 @@
+// Kernel argument blocks and launchers for the stage-2 loop.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ps2 {
+
+// e^{-2 pi i k / 32}, k = 0..15, computed on the host in double precision.
+struct Twiddles32f {
+  float2 w[16];
+};
+struct Twiddles32d {
+  double2 w[16];
+};
+
+// --------------------------------------------------------------- binning --
+// fill_phase_weight + accumulate_grid (native_stage2.rs:629-657, 722-740):
+// grid[cell, c] = sum over the cell's rows s (ascending original row order)
+// of ph_nm[s, c] * e^{-j bp K_s} * w_s, summed sequentially.
+struct BinArgs {
+  const void* ph_nm;     // complex [N, M] (cell-sorted rows)
+  const float* bp;       // f32 [N, M] sorted, or [M]
+  int bp_row_inv;
+  const int32_t* cell_start;  // [G + 1]
+  int64_t G;
+  int M, Mp, nchunk;
+  const void* K;         // real [N] (sorted)
+  void* w;               // real [N] (sorted): read (mode 0) or written (mode 1)
+  const void* coh;       // real [N] previous coherence (mode 1)
+  const double* lut;     // P-square prand_hi table (mode 1)
+  int lut_len;
+  int mode;              // 0: w given; 1: w = (1 - lut[round(1000 coh)])^2
+  void* grid;            // complex [G, Mp]
+};
+
+// ------------------------------------------------------------------ CLAP --
+struct ClapArgs {
+  const void* grid;   // complex [G, Mp]
+  int n_i, n_j, M, Mp;
+  int n_win;          // 24
+  int nwi, nwj;       // window counts per axis
+  int alpha_is_one;
+  double alpha, beta;
+  const double* low_pass;  // [32*32] natural FFT order (device)
+  const double* wscaled;   // [n_win*n_win] pyramid weight / 1024 (device)
+  double g7[7];            // 7-tap Gaussian of the |H| smoothing
+  void* win_out;           // complex [W, n_win*n_win, Mp]
+};
+
+struct OverlapArgs {
+  const void* win_out;  // complex [W, n_win*n_win, Mp]
+  void* filt;           // complex [G, Mp]
+  int n_i, n_j, M, Mp, n_win, n_inc, nwi, nwj;
+};
+
+// --------------------------------------------------------------- topofit --
+struct TopoArgs {
+  const void* ph_nm;      // complex [N, M] sorted (loop mode)
+  const void* filt;       // complex [G, Mp] filtered grid (loop mode)
+  const int32_t* cell_of; // [N] (loop mode)
+  const void* cpx;        // complex [N, M] (registry mode, replaces ph_nm/filt)
+  const float* bp;        // f32 [N, M] or [M]
+  int bp_row_inv;
+  int64_t N;
+  int M, Mp;
+  int n_half;             // ceil(8 * n_trial_wraps)
+  int zero_mode;          // 0: a zero element invalidates the row; 1: zero columns skipped
+  void* K_out;            // real [N]
+  void* C_out;            // real [N]
+  void* coh_io;           // real [N]: previous coherence in, new coherence out
+  uint8_t* nopt;          // [N]
+  double* rms_partial;    // [gridDim.x]
+  int32_t* hist;          // [100]
+  int32_t* n_invalid;     // [1]
+  double cutoff0, dbin;
+  // optional outputs (written only when non-null)
+  void* residual;         // complex [N, M]
+  void* ph_res;           // real [N, M]
+  void* ph_patch;         // complex [N, M]
+  int accumulate_stats;   // 1: rms partials / histogram / invalid count
+};
+
+// -------------------------------------------------------------- finalize --
+struct FinalizeArgs {
+  const double* rms_partial;
+  int n_partial;
+  int64_t N;
+  const int32_t* hist;       // Na
+  double* nr_scaled;         // [100] in/out
+  double nr_max_nz_ix;
+  int low_coh_thresh;
+  int psquare;
+  double gamma_change_convergence;
+  int64_t gamma_max_iterations;
+  double g7w[7];             // gausswin(7, 2.5) for the prand smoothing
+  double g7sum;
+  const double* taps79;      // interp(x, 10) FIR
+  double* lut;               // [1001] out
+  double* state;             // [4]: gamma_change_save, i_loop, last rms, last delta
+  double* stats_out;         // [6] per-iteration record
+  int32_t* n_invalid;
+  int force_continue;        // iterate past the stop rule (timing runs)
+};
+
+// ---------------------------------------------------------- launchers -----
+cudaError_t launch_bin(const BinArgs& a, bool fp64, int sm_count, cudaStream_t st);
+cudaError_t launch_clap(const ClapArgs& a, bool fp64, const Twiddles32f& tf, const Twiddles32d& td, int sm_count,
+                        cudaStream_t st);
+cudaError_t launch_overlap(const OverlapArgs& a, bool fp64, cudaStream_t st);
+cudaError_t launch_topofit(const TopoArgs& a, bool fp64, int grid_blocks, cudaStream_t st);
+int topofit_grid_blocks(int sm_count, bool fp64);
+cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t st);
+cudaError_t launch_snr_weight(const TopoArgs& t, const float* amp, void* w_out, bool fp64, int sm_count,
+                              cudaStream_t st);
+cudaError_t launch_random_hist(const double* rnd, int64_t n_rand, const double* bp, int m, const int64_t* ia,
+                               const int64_t* ib, int small_baseline, int n_half, double cutoff0, double dbin,
+                               int32_t* hist, int sm_count, cudaStream_t st);
+
+// layout helpers
+cudaError_t launch_gather_rows(const void* src, void* dst, const int32_t* perm, int64_t n, int64_t row_bytes,
+                               cudaStream_t st);
+cudaError_t launch_scatter_rows(const void* src, void* dst, const int32_t* perm, int64_t n, int64_t row_bytes,
+                                cudaStream_t st);
+cudaError_t launch_unpad_grid(const void* src, void* dst, int64_t G, int M, int Mp, int elem_bytes, cudaStream_t st);
+cudaError_t launch_pad_grid(const void* src, void* dst, int64_t G, int M, int Mp, int elem_bytes, cudaStream_t st);
+cudaError_t launch_init_state(const double* w0, const int32_t* perm, int64_t N, void* K, void* w, void* coh,
+                              bool fp64, cudaStream_t st);
+cudaError_t launch_ph_weight(const BinArgs& a, int64_t N, bool fp64, const int32_t* perm, void* out_orig,
+                             cudaStream_t st);
+
+}  // namespace ps2

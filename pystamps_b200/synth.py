@@ -133,18 +133,20 @@ def make_patch(
 
     ph = np.empty((n_ps, n_ifg + 1), dtype=np.complex64)
     ph[:, 0] = 1.0
-    chunk = max(1, min(n_ps, (1 << 24) // max(n_ifg, 1)))
+    chunk = max(1, min(n_ps, (1 << 22) // max(n_ifg, 1)))
+    k32 = k_ps.astype(np.float32)
     for s in range(0, n_ps, chunk):
         e = min(n_ps, s + chunk)
-        defo = fields[:, ix[s:e], iy[s:e]].T.astype(np.float64) * (4.0 * math.pi / LAMBDA)
-        topo = k_ps[s:e, None] * bperp_mat[s:e]
-        noise = np.where(
-            stable[s:e, None],
-            rng.normal(0.0, 0.3, (e - s, n_ifg)),
-            rng.uniform(-math.pi, math.pi, (e - s, n_ifg)),
-        )
-        phase = defo + topo + noise
-        ph[s:e, 1:] = np.exp(1j * phase).astype(np.complex64)
+        phase = fields[:, ix[s:e], iy[s:e]].T * np.float32(4.0 * math.pi / LAMBDA)
+        phase += k32[s:e, None] * bperp_mat[s:e].astype(np.float32)
+        st = stable[s:e]
+        noise = rng.uniform(-math.pi, math.pi, (e - s, n_ifg)).astype(np.float32)
+        n_st = int(st.sum())
+        if n_st:
+            noise[st] = rng.normal(0.0, 0.3, (n_st, n_ifg)).astype(np.float32)
+        phase += noise
+        ph[s:e, 1:].real = np.cos(phase)
+        ph[s:e, 1:].imag = np.sin(phase)
     d_a = rng.uniform(0.2, 0.6, n_ps)
 
     parms = {
