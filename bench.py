@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="E", help="A, B, D or E (default E, the full-scale patch)")
+    ap.add_argument("--n-ps", type=int, default=0, help="override the PS count (profiling a smaller case)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -110,10 +111,14 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- workload -----
-def make_workload(name: str, rank: int):
+def make_workload(name: str, rank: int, n_ps: int = 0):
     from pystamps_b200 import synth
 
     w = synth.ALIASES.get(name) or synth.WORKLOADS[name]
+    if n_ps:
+        import dataclasses
+
+        w = dataclasses.replace(w, name=f"{w.name}-at-{n_ps}-ps", n_ps=n_ps)
     patch = synth.make_workload(w, patch_id=rank)
     return w, patch
 
@@ -172,7 +177,7 @@ def run_reference(args, rank: int, world: int):
         return
     from pystamps_b200 import stage2 as S
 
-    w, patch = make_workload(args.workload, 0)
+    w, patch = make_workload(args.workload, 0, args.n_ps)
     prep = S.prepare_patch(patch, nr=np.ones(100), nr_max_nz_ix=100.0)
     vals = []
     for i in range(args.warmup + args.steps):
@@ -206,7 +211,7 @@ def run_ours(args, rank: int, world: int, dist):
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
-    w, patch = make_workload(args.workload, rank)
+    w, patch = make_workload(args.workload, rank, args.n_ps)
     t0 = time.perf_counter()
     prep = S.prepare_patch(patch)
     t_prep = time.perf_counter() - t0

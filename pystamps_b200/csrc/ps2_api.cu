@@ -340,6 +340,7 @@ int run_one_iteration(ps2_ctx* c, bool force_continue, cudaEvent_t* ev) {
   }
   CK(cudaMemsetAsync(c->hist.p, 0, sizeof(int32_t) * PS2_COH_BINS, c->st));
   CK(cudaMemsetAsync(c->n_invalid.p, 0, sizeof(int32_t), c->st));
+  CK(cudaMemsetAsync(c->rms_partial.p, 0, sizeof(double) * c->topo_blocks, c->st));
   const int mode = (c->iters_done > 0 && c->psquare) ? 1 : 0;
   CK(launch_bin(bin_args(c, mode, c->K[cur].p), fp64, c->sm_count, c->st));
   ++launched;
@@ -355,7 +356,7 @@ int run_one_iteration(ps2_ctx* c, bool force_continue, cudaEvent_t* ev) {
   if (ev) CK(cudaEventRecord(ev[3], c->st));
   FinalizeArgs f{};
   f.rms_partial = c->rms_partial.as<double>();
-  f.n_partial = static_cast<int>(std::min<int64_t>(c->topo_blocks, (c->N + 7) / 8));
+  f.n_partial = c->topo_blocks;  // unlaunched blocks' partials stay zero
   f.N = c->N;
   f.hist = c->hist.as<int32_t>();
   f.nr_scaled = c->nr_scaled.as<double>();

@@ -15,6 +15,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "ps2_device.cuh"
 #include "ps2_kernels.cuh"
@@ -487,82 +488,213 @@ cudaError_t launch_overlap(const OverlapArgs& a, bool fp64, cudaStream_t st) {
 }
 
 // =============================================================== topofit ==
-// Lane l ends with the warp-wide sum of slot (l mod W) of v[]: full xor
-// reductions for the lane bits >= log2(W), then a transposing reduction
-// (each step halves the slots a lane keeps and exchanges the other half).
-template <int W>
-__device__ __forceinline__ float2 transpose_reduce(float2 (&v)[W], const int lane) {
-#pragma unroll
-  for (int o = 16; o >= W; o >>= 1) {
-#pragma unroll
-    for (int i = 0; i < W; ++i) {
-      v[i].x += __shfl_xor_sync(kFull, v[i].x, o);
-      v[i].y += __shfl_xor_sync(kFull, v[i].y, o);
-    }
-  }
-#pragma unroll
-  for (int o = W / 2; o >= 1; o >>= 1) {
-    const bool upper = (lane & o) != 0;
-#pragma unroll
-    for (int i = 0; i < o; ++i) {
-      const float2 lo = v[i], hi = v[i + o];
-      float2 send = upper ? lo : hi;
-      const float2 keep = upper ? hi : lo;
-      send.x = __shfl_xor_sync(kFull, send.x, o);
-      send.y = __shfl_xor_sync(kFull, send.y, o);
-      v[i] = make_float2(keep.x + send.x, keep.y + send.y);
-    }
-  }
-  return v[0];
-}
-
-// W consecutive trial multipliers m0 .. m0+W-1: S_m = sum_c z_c e^{-j th_c m}.
-// The phasor u = z e^{-j th m} advances by one complex multiply per trial and
-// is re-anchored with an exact sincos every 16 trials.
-template <int W, int MAXC>
-__device__ __forceinline__ void trial_block(const float2 (&z)[MAXC], const float (&th)[MAXC], const float2 (&rot)[MAXC],
-                                            const int m0, const int t0, const int T, const int lane, float& best_sq,
-                                            int& best_t) {
-  float2 S[W];
-#pragma unroll
-  for (int k = 0; k < W; ++k) S[k] = make_float2(0.f, 0.f);
-#pragma unroll
-  for (int q = 0; q < MAXC; ++q) {
-    float sn, cs;
-    sincosf(th[q] * static_cast<float>(m0), &sn, &cs);
-    float2 u = cmul(z[q], make_float2(cs, -sn));
-#pragma unroll
-    for (int k = 0; k < W; ++k) {
-      if (k > 0 && (k & 15) == 0) {
-        sincosf(th[q] * static_cast<float>(m0 + k), &sn, &cs);
-        u = cmul(z[q], make_float2(cs, -sn));
-      }
-      S[k].x += u.x;
-      S[k].y += u.y;
-      if (k + 1 < W) u = cmul(u, rot[q]);
-    }
-  }
-  const float2 tot = transpose_reduce<W>(S, lane);
-  const int t = t0 + (lane & (W - 1));
-  if (t < T) {
-    const float sq = tot.x * tot.x + tot.y * tot.y;
-    if (sq > best_sq) {
-      best_sq = sq;
-      best_t = t;
-    }
-  }
-}
+// One group of L lanes per PS (L = 4, 8, 16 or 32, chosen from the number of
+// interferograms so a lane owns about 5-10 columns); a warp holds 32/L PS.
+// Column data (psdph z_c, theta_c = bp_c/range*pi/4, e^{-j theta_c}, bp_c)
+// live in shared memory. The trial sweep evaluates
+//   S_m = sum_c z_c e^{-j theta_c m}
+// for 32 consecutive m at a time: the phasor u = z e^{-j theta m} advances by
+// one complex multiply per trial and is re-anchored with a directly computed
+// e^{-j theta m} every 16 trials; the group then reduces its 32 partial sums
+// with a transposing butterfly, each lane ending with 32/L of the trials.
 
 constexpr float kQuarterPiF = 3.14159265358979323846f / 4.0f;  // Rust std::f32::consts::PI / 4.0
 
-template <int MAXC>
-__global__ void __launch_bounds__(256, 2) k_topofit_f32(TopoArgs a) {
+// e^{-j x} for the re-anchoring points, |x| < ~1e3: Cody-Waite argument
+// reduction by pi/2 with a two-constant split of pi/2 (Cody & Waite, "Software
+// Manual for the Elementary Functions", 1980), then the hardware sin/cos
+// approximations on |r| <= pi/4 and the quadrant rotation.
+__device__ __forceinline__ float2 cis_neg_anchor(float x) {
+  const float k = rintf(x * 0.636619772367581343f);
+  float r = fmaf(-k, 1.57079637050628662109375f, x);
+  r = fmaf(-k, -4.37113900018624283e-8f, r);
+  const float sr = __sinf(r), cr = __cosf(r);
+  const int q = static_cast<int>(k) & 3;
+  const float sx0 = (q & 1) ? cr : sr;
+  const float cx0 = (q & 1) ? sr : cr;
+  const float sx = (q & 2) ? -sx0 : sx0;
+  const float cx = ((q + 1) & 2) ? -cx0 : cx0;
+  return make_float2(cx, -sx);
+}
+
+template <int L>
+__device__ __forceinline__ float group_sum(float v) {
+#pragma unroll
+  for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+template <int L>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+template <int L>
+__device__ __forceinline__ float group_min(float v) {
+#pragma unroll
+  for (int o = L / 2; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+template <int L>
+__device__ __forceinline__ float group_max(float v) {
+#pragma unroll
+  for (int o = L / 2; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+
+// Sum over the L lanes of a group of each of the W slots of v. Halving steps
+// (lanes whose offset bit is set keep the upper half) while more than one slot
+// remains, plain xor reductions after that. Returns the number of slots the
+// lane holds (max(W/L, 1)) in v[0..]; they are slots base .. base+count-1.
+template <int W, int L>
+__device__ __forceinline__ int group_transpose_reduce(float2 (&v)[W], const int gl, int& base) {
+  int cnt = W;
+  base = 0;
+#pragma unroll
+  for (int o = L / 2; o >= 1; o >>= 1) {
+    if (cnt > 1) {
+      const int h = cnt / 2;
+      const bool upper = (gl & o) != 0;
+#pragma unroll
+      for (int i = 0; i < W / 2; ++i) {
+        if (i < h) {
+          const float2 lo = v[i], hi = v[i + h];
+          float2 send = upper ? lo : hi;
+          const float2 keep = upper ? hi : lo;
+          send.x = __shfl_xor_sync(kFull, send.x, o);
+          send.y = __shfl_xor_sync(kFull, send.y, o);
+          v[i] = make_float2(keep.x + send.x, keep.y + send.y);
+        }
+      }
+      if (upper) base += h;
+      cnt = h;
+    } else {
+      v[0].x += __shfl_xor_sync(kFull, v[0].x, o);
+      v[0].y += __shfl_xor_sync(kFull, v[0].y, o);
+    }
+  }
+  return cnt;
+}
+
+template <int W>
+__device__ __forceinline__ void accumulate_column(float2 (&S)[W], const float2 z, const float2 rot, const float th,
+                                                  const int m0) {
+  float2 u = cmul(z, cis_neg_anchor(th * static_cast<float>(m0)));
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    if (k > 0 && (k & 15) == 0) u = cmul(z, cis_neg_anchor(th * static_cast<float>(m0 + k)));
+    S[k].x += u.x;
+    S[k].y += u.y;
+    if (k + 1 < W) u = cmul(u, rot);
+  }
+}
+
+template <int W>
+__device__ __forceinline__ void accumulate_two_columns(float2 (&S)[W], const float2 z0, const float2 r0,
+                                                       const float t0, const float2 z1, const float2 r1,
+                                                       const float t1, const int m0) {
+  float2 u0 = cmul(z0, cis_neg_anchor(t0 * static_cast<float>(m0)));
+  float2 u1 = cmul(z1, cis_neg_anchor(t1 * static_cast<float>(m0)));
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    if (k > 0 && (k & 15) == 0) {
+      u0 = cmul(z0, cis_neg_anchor(t0 * static_cast<float>(m0 + k)));
+      u1 = cmul(z1, cis_neg_anchor(t1 * static_cast<float>(m0 + k)));
+    }
+    S[k].x += u0.x + u1.x;
+    S[k].y += u0.y + u1.y;
+    if (k + 1 < W) {
+      u0 = cmul(u0, r0);
+      u1 = cmul(u1, r1);
+    }
+  }
+}
+
+template <int W>
+__device__ __forceinline__ void accumulate_four_columns(float2 (&S)[W], const float2 (&z)[4], const float2 (&r)[4],
+                                                        const float (&t)[4], const int m0) {
+  float2 u[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) u[i] = cmul(z[i], cis_neg_anchor(t[i] * static_cast<float>(m0)));
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    if (k > 0 && (k & 15) == 0) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) u[i] = cmul(z[i], cis_neg_anchor(t[i] * static_cast<float>(m0 + k)));
+    }
+    S[k].x += (u[0].x + u[1].x) + (u[2].x + u[3].x);
+    S[k].y += (u[0].y + u[1].y) + (u[2].y + u[3].y);
+    if (k + 1 < W) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) u[i] = cmul(u[i], r[i]);
+    }
+  }
+}
+
+struct ColumnSmem {
+  float *zx, *zy, *rx, *ry, *th;
+};
+
+template <int W, int L>
+__device__ __forceinline__ void sweep_block(const ColumnSmem& cs, const int ncl, const int gl, const int m0,
+                                            const int t0, const int T, float& best_sq, int& best_t) {
+  float2 S[W];
+#pragma unroll
+  for (int k = 0; k < W; ++k) S[k] = make_float2(0.f, 0.f);
+  int k = 0;
+  for (; k + 3 < ncl; k += 4) {
+    float2 z[4], r[4];
+    float t[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int c = gl + L * (k + i);
+      z[i] = make_float2(cs.zx[c], cs.zy[c]);
+      r[i] = make_float2(cs.rx[c], cs.ry[c]);
+      t[i] = cs.th[c];
+    }
+    accumulate_four_columns<W>(S, z, r, t, m0);
+  }
+  for (; k + 1 < ncl; k += 2) {
+    const int c0 = gl + L * k, c1 = c0 + L;
+    accumulate_two_columns<W>(S, make_float2(cs.zx[c0], cs.zy[c0]), make_float2(cs.rx[c0], cs.ry[c0]), cs.th[c0],
+                              make_float2(cs.zx[c1], cs.zy[c1]), make_float2(cs.rx[c1], cs.ry[c1]), cs.th[c1], m0);
+  }
+  if (k < ncl) {
+    const int c0 = gl + L * k;
+    accumulate_column<W>(S, make_float2(cs.zx[c0], cs.zy[c0]), make_float2(cs.rx[c0], cs.ry[c0]), cs.th[c0], m0);
+  }
+  int base;
+  const int cnt = group_transpose_reduce<W, L>(S, gl, base);
+#pragma unroll
+  for (int j = 0; j < (W / L > 1 ? W / L : 1); ++j) {
+    if (j < cnt) {
+      const int t = t0 + base + j;
+      if (t < T) {
+        const float sq = S[j].x * S[j].x + S[j].y * S[j].y;
+        if (sq > best_sq) {
+          best_sq = sq;
+          best_t = t;
+        }
+      }
+    }
+  }
+}
+
+template <int L>
+__global__ void __launch_bounds__(128) k_topofit_f32(TopoArgs a, int mpad) {
+  constexpr int G = 32 / L;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int sh_hist[kCohBins];
-  __shared__ double sh_rms[8];
-  __shared__ int sh_inv[8];
+  __shared__ double sh_rms[4];
+  __shared__ int sh_inv[4];
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
+  const int g = lane / L, gl = lane % L;
   for (int i = tid; i < kCohBins; i += blockDim.x) sh_hist[i] = 0;
   __syncthreads();
+  // per-PS slot stride = L (mod 32) floats so the groups of a warp hit different banks
+  const int stride = ((5 * mpad + 31) / 32) * 32 + (L % 32);
+  float* base_ptr = reinterpret_cast<float*>(smem_raw) + static_cast<int64_t>(wib * G + g) * stride;
+  ColumnSmem cs{base_ptr, base_ptr + mpad, base_ptr + 2 * mpad, base_ptr + 3 * mpad, base_ptr + 4 * mpad};
   const float2* __restrict__ ph_nm = static_cast<const float2*>(a.ph_nm);
   const float2* __restrict__ filt = static_cast<const float2*>(a.filt);
   const float2* __restrict__ cpx = static_cast<const float2*>(a.cpx);
@@ -573,23 +705,23 @@ __global__ void __launch_bounds__(256, 2) k_topofit_f32(TopoArgs a) {
   float* __restrict__ ph_res = static_cast<float*>(a.ph_res);
   float2* __restrict__ ph_patch = static_cast<float2*>(a.ph_patch);
   const int64_t M = a.M;
+  const int ncl = mpad / L;
   const int T = 2 * a.n_half + 1;
+  const unsigned gmask = (L == 32) ? kFull : (((1u << L) - 1u) << (g * L));
   double rms_acc = 0.0;
   int inv_acc = 0;
-  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + tid) >> 5;
-  const int64_t nwarps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
-  for (int64_t s = gw; s < a.N; s += nwarps) {
-    float2 z[MAXC];
-    float bpv[MAXC];
+  const int64_t step = static_cast<int64_t>(gridDim.x) * 4 * G;
+  for (int64_t s0 = (static_cast<int64_t>(blockIdx.x) * 4 + wib) * G; s0 < a.N; s0 += step) {
+    const int64_t s = s0 + g;
+    const bool active = s < a.N;
+    const int64_t cell = (active && !cpx) ? a.cell_of[s] : 0;
     bool zero = false, nonzero = false;
-    const int64_t cell = cpx ? 0 : a.cell_of[s];
-#pragma unroll
-    for (int q = 0; q < MAXC; ++q) {
-      const int c = lane + 32 * q;
-      z[q] = make_float2(0.f, 0.f);
-      bpv[q] = 0.f;
-      if (c < a.M) {
-        float2 v;
+    float mn = __int_as_float(0x7f800000), mx = -mn;
+    for (int k = 0; k < ncl; ++k) {
+      const int c = gl + L * k;
+      float2 v = make_float2(0.f, 0.f);
+      float b = 0.f;
+      if (active && c < a.M) {
         if (cpx) {
           v = cpx[s * M + c];
         } else {
@@ -600,142 +732,127 @@ __global__ void __launch_bounds__(256, 2) k_topofit_f32(TopoArgs a) {
           if (ph_patch) ph_patch[s * M + c] = f;
           v = cmul_rn(conjf2(f), ph_nm[s * M + c]);  // psdph (:687-689)
         }
-        z[q] = v;
-        bpv[q] = a.bp_row_inv ? a.bp[c] : a.bp[s * M + c];
-        if (v.x == 0.f && v.y == 0.f)
+        b = a.bp_row_inv ? a.bp[c] : a.bp[s * M + c];
+        if (v.x == 0.f && v.y == 0.f) {
           zero = true;
-        else
+        } else {
           nonzero = true;
+          mn = fminf(mn, b);
+          mx = fmaxf(mx, b);
+        }
+      }
+      cs.zx[c] = v.x;
+      cs.zy[c] = v.y;
+      cs.th[c] = b;  // bp for now; theta once the range is known
+    }
+    const bool any_zero = (__ballot_sync(kFull, zero) & gmask) != 0u;
+    const bool any_nonzero = (__ballot_sync(kFull, nonzero) & gmask) != 0u;
+    const bool invalid = !active || (a.zero_mode == 0 ? any_zero : !any_nonzero);
+    mn = group_min<L>(mn);
+    mx = group_max<L>(mx);
+    float range = mx - mn;
+    if (!(range != 0.f) || invalid) range = 1.f;
+    for (int k = 0; k < ncl; ++k) {
+      const int c = gl + L * k;
+      const float t = (cs.th[c] / range) * kQuarterPiF;
+      float sn, cn;
+      sincosf(t, &sn, &cn);
+      cs.th[c] = t;
+      cs.rx[c] = cn;
+      cs.ry[c] = -sn;
+    }
+    __syncwarp();
+    // trial sweep over m = -n .. n (all groups run it; invalid ones discard it)
+    float best_sq = -1.f;
+    int best_t = 0;
+    int t0 = 0;
+    for (; T - t0 >= 16; t0 += 16) sweep_block<16, L>(cs, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
+    if (T - t0 >= 8) {
+      sweep_block<8, L>(cs, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
+      t0 += 8;
+    }
+    if (T - t0 >= 4) {
+      sweep_block<4, L>(cs, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
+      t0 += 4;
+    }
+    if (T - t0 >= 2) {
+      sweep_block<2, L>(cs, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
+      t0 += 2;
+    }
+    if (T - t0 >= 1) {
+      sweep_block<1, L>(cs, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
+      t0 += 1;
+    }
+    // first maximum over the group (argmax_first_f32, :1526-1536)
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) {
+      const float osq = __shfl_xor_sync(kFull, best_sq, o);
+      const int ot = __shfl_xor_sync(kFull, best_t, o);
+      if (osq > best_sq || (osq == best_sq && ot < best_t)) {
+        best_sq = osq;
+        best_t = ot;
       }
     }
-    const bool any_zero = __any_sync(kFull, zero);
-    const bool any_nonzero = __any_sync(kFull, nonzero);
-    const bool invalid = a.zero_mode == 0 ? any_zero : !any_nonzero;
-    float Kv, Cv, cohv;
-    if (invalid) {
-      // fit_stage2_rows invalid row (:676-697) / topofit_row empty row (:1216-1222)
-      Kv = __int_as_float(0x7fffffff);
-      Cv = a.zero_mode == 0 ? 0.f : Kv;
-      cohv = a.zero_mode == 0 ? 0.f : Kv;
-#pragma unroll
-      for (int q = 0; q < MAXC; ++q) {
-        const int c = lane + 32 * q;
-        if (c < a.M) {
-          if (resid) resid[s * M + c] = make_float2(0.f, 0.f);
-          if (ph_res) ph_res[s * M + c] = 0.f;
-        }
-      }
-      inv_acc += 1;
-    } else {
-      // topofit_row (:1207-1257) over the non-zero columns
-      float mn = __int_as_float(0x7f800000), mx = -mn;
-#pragma unroll
-      for (int q = 0; q < MAXC; ++q) {
-        if (lane + 32 * q < a.M && (z[q].x != 0.f || z[q].y != 0.f)) {
-          mn = fminf(mn, bpv[q]);
-          mx = fmaxf(mx, bpv[q]);
-        }
-      }
-      mn = warp_min(mn);
-      mx = warp_max(mx);
-      float range = mx - mn;
-      if (range == 0.f) range = 1.f;
-      float th[MAXC];
-      float2 rot[MAXC];
-#pragma unroll
-      for (int q = 0; q < MAXC; ++q) {
-        th[q] = (bpv[q] / range) * kQuarterPiF;
-        float sn, cs;
-        sincosf(th[q], &sn, &cs);
-        rot[q] = make_float2(cs, -sn);
-      }
-      float best_sq = -1.f;
-      int best_t = 0;
-      int t0 = 0;
-      for (; T - t0 >= 32; t0 += 32) trial_block<32, MAXC>(z, th, rot, t0 - a.n_half, t0, T, lane, best_sq, best_t);
-      if (T - t0 >= 16) {
-        trial_block<16, MAXC>(z, th, rot, t0 - a.n_half, t0, T, lane, best_sq, best_t);
-        t0 += 16;
-      }
-      if (T - t0 >= 8) {
-        trial_block<8, MAXC>(z, th, rot, t0 - a.n_half, t0, T, lane, best_sq, best_t);
-        t0 += 8;
-      }
-      if (T - t0 >= 4) {
-        trial_block<4, MAXC>(z, th, rot, t0 - a.n_half, t0, T, lane, best_sq, best_t);
-        t0 += 4;
-      }
-      if (T - t0 >= 2) {
-        trial_block<2, MAXC>(z, th, rot, t0 - a.n_half, t0, T, lane, best_sq, best_t);
-        t0 += 2;
-      }
-      if (T - t0 >= 1) {
-        trial_block<1, MAXC>(z, th, rot, t0 - a.n_half, t0, T, lane, best_sq, best_t);
-        t0 += 1;
-      }
-      // first maximum over the warp (argmax_first_f32, :1526-1536)
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const float osq = __shfl_xor_sync(kFull, best_sq, o);
-        const int ot = __shfl_xor_sync(kFull, best_t, o);
-        if (osq > best_sq || (osq == best_sq && ot < best_t)) {
-          best_sq = osq;
-          best_t = ot;
-        }
-      }
-      // refine_candidate (:1259-1303); FP64 normal equations
-      const float k0 = kQuarterPiF / range * static_cast<float>(best_t - a.n_half);
-      float2 res[MAXC];
-      float ox = 0.f, oy = 0.f;
-#pragma unroll
-      for (int q = 0; q < MAXC; ++q) {
-        float sn, cs;
-        sincosf(k0 * bpv[q], &sn, &cs);
-        res[q] = cmul_rn(z[q], make_float2(cs, -sn));
-        ox += res[q].x;
-        oy += res[q].y;
-      }
-      ox = warp_sum(ox);
-      oy = warp_sum(oy);
-      const float2 oc = make_float2(ox, -oy);
-      double mopt = 0.0, dl = 0.0;
-#pragma unroll
-      for (int q = 0; q < MAXC; ++q) {
-        const double wgt = static_cast<double>(hypotf(z[q].x, z[q].y));
-        const double wb = __dmul_rn(wgt, static_cast<double>(bpv[q]));
-        dl = __dadd_rn(dl, __dmul_rn(wb, wb));
-        const float2 r = cmul_rn(res[q], oc);
-        const double ang = static_cast<double>(atan2f(r.y, r.x));
-        mopt = __dadd_rn(mopt, __dmul_rn(wb, __dmul_rn(wgt, ang)));
-      }
-      mopt = warp_sum(mopt);
-      dl = warp_sum(dl);
-      if (dl == 0.0) dl = 1.0;
-      const float K1 = static_cast<float>(static_cast<double>(k0) + mopt / dl);
-      float mx2 = 0.f, my2 = 0.f, den2 = 0.f;
-#pragma unroll
-      for (int q = 0; q < MAXC; ++q) {
-        float sn, cs;
-        sincosf(K1 * bpv[q], &sn, &cs);
-        const float2 r = cmul_rn(z[q], make_float2(cs, -sn));
-        mx2 += r.x;
-        my2 += r.y;
-        den2 += hypotf(r.x, r.y);
-        const int c = lane + 32 * q;
-        if (c < a.M) {
-          if (resid) resid[s * M + c] = r;
-          if (ph_res) ph_res[s * M + c] = atan2f(r.y, r.x);
-        }
-      }
-      mx2 = warp_sum(mx2);
-      my2 = warp_sum(my2);
-      den2 = warp_sum(den2);
-      if (den2 == 0.f) den2 = 1.f;
-      Kv = K1;
-      Cv = atan2f(my2, mx2);
-      cohv = hypotf(mx2, my2) / den2;
+    // refine_candidate (:1259-1303) with FP64 normal-equation sums; the
+    // column store now holds bp (th slots) and z e^{-j k0 bp} (rotation slots)
+    const float k0 = kQuarterPiF / range * static_cast<float>(best_t - a.n_half);
+    float ox = 0.f, oy = 0.f;
+    for (int k = 0; k < ncl; ++k) {
+      const int c = gl + L * k;
+      const float b = (active && c < a.M) ? (a.bp_row_inv ? a.bp[c] : a.bp[s * M + c]) : 0.f;
+      cs.th[c] = b;
+      const float2 r = cmul_rn(make_float2(cs.zx[c], cs.zy[c]), cis_neg_anchor(k0 * b));
+      cs.rx[c] = r.x;
+      cs.ry[c] = r.y;
+      ox += r.x;
+      oy += r.y;
     }
-    if (lane == 0) {
+    ox = group_sum<L>(ox);
+    oy = group_sum<L>(oy);
+    const float2 oc = make_float2(ox, -oy);
+    double mopt = 0.0, dl = 0.0;
+    for (int k = 0; k < ncl; ++k) {
+      const int c = gl + L * k;
+      const double wgt = static_cast<double>(hypotf(cs.zx[c], cs.zy[c]));
+      const double wb = __dmul_rn(wgt, static_cast<double>(cs.th[c]));
+      dl = __dadd_rn(dl, __dmul_rn(wb, wb));
+      const float2 q = cmul_rn(make_float2(cs.rx[c], cs.ry[c]), oc);
+      mopt = __dadd_rn(mopt, __dmul_rn(wb, __dmul_rn(wgt, static_cast<double>(atan2f(q.y, q.x)))));
+    }
+    mopt = group_sum<L>(mopt);
+    dl = group_sum<L>(dl);
+    if (dl == 0.0) dl = 1.0;
+    const float K1 = static_cast<float>(static_cast<double>(k0) + mopt / dl);
+    float mx2 = 0.f, my2 = 0.f, den2 = 0.f;
+    for (int k = 0; k < ncl; ++k) {
+      const int c = gl + L * k;
+      const float2 r = cmul_rn(make_float2(cs.zx[c], cs.zy[c]), cis_neg_anchor(K1 * cs.th[c]));
+      mx2 += r.x;
+      my2 += r.y;
+      den2 += hypotf(r.x, r.y);
+      if (active && c < a.M) {
+        if (resid) resid[s * M + c] = invalid ? make_float2(0.f, 0.f) : r;
+        if (ph_res) ph_res[s * M + c] = invalid ? 0.f : atan2f(r.y, r.x);
+      }
+    }
+    mx2 = group_sum<L>(mx2);
+    my2 = group_sum<L>(my2);
+    den2 = group_sum<L>(den2);
+    if (den2 == 0.f) den2 = 1.f;
+    __syncwarp();
+    if (gl == 0 && active) {
+      float Kv, Cv, cohv;
+      if (invalid) {
+        // fit_stage2_rows invalid row (:676-697) / topofit_row empty row (:1216-1222)
+        Kv = __int_as_float(0x7fffffff);
+        Cv = a.zero_mode == 0 ? 0.f : Kv;
+        cohv = a.zero_mode == 0 ? 0.f : Kv;
+        inv_acc += 1;
+      } else {
+        Kv = K1;
+        Cv = atan2f(my2, mx2);
+        cohv = hypotf(mx2, my2) / den2;
+      }
       if (a.accumulate_stats) {
         const double d = static_cast<double>(cohv) - static_cast<double>(coh_io[s]);
         rms_acc += d * d;
@@ -749,19 +866,16 @@ __global__ void __launch_bounds__(256, 2) k_topofit_f32(TopoArgs a) {
     }
   }
   if (!a.accumulate_stats) return;
+  rms_acc = warp_sum(rms_acc);
+  inv_acc = warp_sum(inv_acc);
   if (lane == 0) {
     sh_rms[wib] = rms_acc;
     sh_inv[wib] = inv_acc;
   }
   __syncthreads();
   if (tid == 0) {
-    double t = 0.0;
-    int iv = 0;
-    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
-      t += sh_rms[w];
-      iv += sh_inv[w];
-    }
-    a.rms_partial[blockIdx.x] = t;
+    a.rms_partial[blockIdx.x] = sh_rms[0] + sh_rms[1] + sh_rms[2] + sh_rms[3];
+    const int iv = sh_inv[0] + sh_inv[1] + sh_inv[2] + sh_inv[3];
     if (iv) atomicAdd(a.n_invalid, iv);
   }
   for (int i = tid; i < kCohBins; i += blockDim.x)
@@ -942,32 +1056,58 @@ __global__ void __launch_bounds__(256) k_topofit_f64(TopoArgs a) {
     if (sh_hist[i]) atomicAdd(&a.hist[i], sh_hist[i]);
 }
 
-int topofit_grid_blocks(int sm_count, bool fp64) { return sm_count * (fp64 ? 4 : 2); }
+int topofit_grid_blocks(int sm_count, bool fp64) { return sm_count * 16; }
+
+int topofit_lanes(int M) {
+  static const int forced = [] {
+    const char* e = getenv("PS2_TOPOFIT_LANES");
+    return e ? atoi(e) : 0;
+  }();
+  if (forced == 4 || forced == 8 || forced == 16 || forced == 32) return forced;
+  int L = 4;
+  while (L < 32 && L * 24 < M) L *= 2;
+  return L;
+}
+
+template <int L>
+static cudaError_t launch_topofit_l(const TopoArgs& a, int grid_cap, cudaStream_t st) {
+  const int mpad = ((a.M + L - 1) / L) * L;
+  const int stride = ((5 * mpad + 31) / 32) * 32 + (L % 32);
+  const size_t sm = static_cast<size_t>(4 * (32 / L)) * stride * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(k_topofit_f32<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_topofit_f32<L>, 128, sm);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t per_block = 4 * (32 / L);
+  int64_t blocks = (a.N + per_block - 1) / per_block;
+  const int64_t cap = std::min<int64_t>(grid_cap, static_cast<int64_t>(sms) * std::max(per_sm, 1));
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  k_topofit_f32<L><<<static_cast<unsigned>(blocks), 128, sm, st>>>(a, mpad);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_topofit(const TopoArgs& a, bool fp64, int grid_blocks, cudaStream_t st) {
   if (a.N <= 0) return cudaSuccess;
-  int64_t need = (a.N + 7) / 8;
-  const int blocks = static_cast<int>(need < grid_blocks ? need : grid_blocks);
   if (fp64) {
+    int64_t need = (a.N + 7) / 8;
+    const int blocks = static_cast<int>(std::min<int64_t>(need, grid_blocks));
     const size_t sm = static_cast<size_t>(8) * a.M * (sizeof(double2) + sizeof(double));
     cudaError_t e = cudaFuncSetAttribute(k_topofit_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     k_topofit_f64<<<blocks, 256, sm, st>>>(a);
     return cudaGetLastError();
   }
-  const int maxc = (a.M + 31) / 32;
-  switch (maxc) {
-    case 1: k_topofit_f32<1><<<blocks, 256, 0, st>>>(a); break;
-    case 2: k_topofit_f32<2><<<blocks, 256, 0, st>>>(a); break;
-    case 3: k_topofit_f32<3><<<blocks, 256, 0, st>>>(a); break;
-    case 4: k_topofit_f32<4><<<blocks, 256, 0, st>>>(a); break;
-    case 5: k_topofit_f32<5><<<blocks, 256, 0, st>>>(a); break;
-    case 6: k_topofit_f32<6><<<blocks, 256, 0, st>>>(a); break;
-    case 7: k_topofit_f32<7><<<blocks, 256, 0, st>>>(a); break;
-    case 8: k_topofit_f32<8><<<blocks, 256, 0, st>>>(a); break;
-    default: return cudaErrorInvalidValue;
+  switch (topofit_lanes(a.M)) {
+    case 4: return launch_topofit_l<4>(a, grid_blocks, st);
+    case 8: return launch_topofit_l<8>(a, grid_blocks, st);
+    case 16: return launch_topofit_l<16>(a, grid_blocks, st);
+    default: return launch_topofit_l<32>(a, grid_blocks, st);
   }
-  return cudaGetLastError();
 }
 
 // ============================================================= finalize ===
