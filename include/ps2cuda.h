@@ -150,6 +150,27 @@ int ps2_random_coherence_histogram(const double* bperp_nm, int64_t n_ifg, double
                                    int32_t small_baseline, const int64_t* ifgday_ix, int64_t n_image,
                                    double* nr_out /* [PS2_COH_BINS] */, double* nr_max_nz_ix);
 
+/* CLAP filter for callers that cannot allocate GPU memory: code running under
+ * a memory budget owned by another allocator (a framework's caching pool, a
+ * Rust or JVM host that hands in pre-allocated buffers), or code that must not
+ * call cudaMalloc/cudaFree because they synchronise the device. Same result as
+ * ps2_clap_filter_grid, but d_ph_grid and d_out are DEVICE pointers owned by
+ * the caller, the work is queued on `stream` (a cudaStream_t, NULL = legacy
+ * default stream) and the call returns without waiting. It allocates nothing:
+ * its scratch is a fixed 32 MiB array inside the library, which every GPU that
+ * loads the library holds until the process exits. Sizes whose scratch
+ * (16*G*Mp + 8*W*clap_window^2*Mp bytes + about 13 KiB, G = n_i*n_j, Mp = m rounded
+ * up to 4, W = CLAP windows) exceed 32 MiB are rejected with
+ * PS2_ERR_UNSUPPORTED. Every call shares that one array: calls whose GPU work
+ * overlaps (other streams, other host threads) race on it and must be
+ * serialised by the caller. The first call on a device resolves the array's
+ * device address (cudaGetSymbolAddress) with that device current; make that
+ * first call before any stream capture. low_pass is a host pointer
+ * [32*32]. This entry point has no counterpart in the reference. */
+int ps2_clap_filter_grid_noalloc(const float* d_ph_grid, int64_t n_i, int64_t n_j, int64_t m, int64_t clap_window,
+                                 double alpha, double beta, const double* low_pass, int64_t n_win_ex, float* d_out,
+                                 void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -1060,6 +1061,114 @@ int ps2_random_coherence_histogram(const double* bperp_nm, int64_t n_ifg, double
       break;
     }
   *nr_max_nz_ix = mx;
+  return PS2_OK;
+}
+
+
+// ------------------------------------------- CLAP without device allocation --
+// Scratch for ps2_clap_filter_grid_noalloc: a fixed 32 MiB array in the module
+// (every GPU that loads the library holds it until the process exits). Host
+// code never uses the symbol itself as an address: ps2_clap_noalloc_scratch()
+// resolves the device address once per device with cudaGetSymbolAddress.
+namespace {
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[128] = {nullptr};
+
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) return set_err(PS2_ERR_UNSUPPORTED, "device ordinal %d unsupported", dev);
+  std::lock_guard<std::mutex> g(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return PS2_OK;
+}
+}  // namespace
+
+int ps2_clap_filter_grid_noalloc(const float* d_ph_grid, int64_t n_i, int64_t n_j, int64_t m, int64_t clap_window,
+                                 double alpha, double beta, const double* low_pass, int64_t n_win_ex, float* d_out,
+                                 void* stream) {
+  if (!d_ph_grid || !d_out || !low_pass || n_i <= 0 || n_j <= 0 || m <= 0)
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_clap_filter_grid_noalloc: invalid arguments");
+  if (n_win_ex != 32) return set_err(PS2_ERR_UNSUPPORTED, "CLAP FFT size %lld unsupported (32)", (long long)n_win_ex);
+  int n_inc, nwi, nwj;
+  int rc = clap_geometry(n_i, n_j, clap_window, &n_inc, &nwi, &nwj);
+  if (rc) return rc;
+  const int64_t G = n_i * n_j;
+  const int Mp = static_cast<int>((m + 3) & ~int64_t(3));
+  const int64_t W = static_cast<int64_t>(nwi) * nwj;
+  const size_t cz = 2 * sizeof(float);
+  auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+  const size_t b_grid = up(cz * G * Mp), b_filt = up(cz * G * Mp);
+  const size_t b_win = up(cz * static_cast<size_t>(W) * clap_window * clap_window * Mp);
+  const size_t b_lp = up(sizeof(double) * 1024), b_ws = up(sizeof(double) * clap_window * clap_window);
+  const size_t need = b_grid + b_filt + b_win + b_lp + b_ws;
+  if (need > kNoAllocScratchBytes)
+    return set_err(PS2_ERR_UNSUPPORTED,
+                   "ps2_clap_filter_grid_noalloc: a %lldx%lld grid with %lld interferograms needs %zu bytes of "
+                   "scratch, more than the fixed %zu; use ps2_clap_filter_grid",
+                   (long long)n_i, (long long)n_j, (long long)m, need, kNoAllocScratchBytes);
+  unsigned char* base = nullptr;
+  rc = noalloc_scratch(reinterpret_cast<void**>(&base));
+  if (rc) return rc;
+  void* grid = base;
+  void* filt = base + b_grid;
+  void* win = base + b_grid + b_filt;
+  double* lp = reinterpret_cast<double*>(base + b_grid + b_filt + b_win);
+  double* wsd = reinterpret_cast<double*>(base + b_grid + b_filt + b_win + b_lp);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int dev = 0, sms = 148;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  std::vector<double> ws = window_weight_scaled(static_cast<int>(clap_window), 32);
+  CK(cudaMemcpyAsync(lp, low_pass, sizeof(double) * 1024, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(wsd, ws.data(), sizeof(double) * ws.size(), cudaMemcpyHostToDevice, st));
+  // the padded copy rewrites every element, so nothing stale survives from an earlier call
+  CK(launch_pad_grid(d_ph_grid, grid, G, static_cast<int>(m), Mp, 8, st));
+  if (W > 0) {
+    ClapArgs a{};
+    a.grid = grid;
+    a.n_i = static_cast<int>(n_i);
+    a.n_j = static_cast<int>(n_j);
+    a.M = static_cast<int>(m);
+    a.Mp = Mp;
+    a.n_win = static_cast<int>(clap_window);
+    a.nwi = nwi;
+    a.nwj = nwj;
+    a.alpha = alpha;
+    a.beta = beta;
+    a.alpha_is_one = std::fabs(alpha - 1.0) <= 2.220446049250313e-16 ? 1 : 0;
+    a.low_pass = lp;
+    a.wscaled = wsd;
+    gauss7(a.g7, nullptr);
+    a.win_out = win;
+    Twiddles32f tf;
+    Twiddles32d td;
+    twiddles(&tf, &td);
+    CK(launch_clap(a, false, tf, td, sms, st));
+    OverlapArgs o{};
+    o.win_out = win;
+    o.filt = filt;
+    o.n_i = a.n_i;
+    o.n_j = a.n_j;
+    o.M = a.M;
+    o.Mp = Mp;
+    o.n_win = a.n_win;
+    o.n_inc = n_inc;
+    o.nwi = nwi;
+    o.nwj = nwj;
+    CK(launch_overlap(o, false, st));
+  } else {
+    CK(cudaMemsetAsync(filt, 0, cz * G * Mp, st));
+  }
+  CK(launch_unpad_grid(filt, d_out, G, static_cast<int>(m), Mp, 8, st));
   return PS2_OK;
 }
 
