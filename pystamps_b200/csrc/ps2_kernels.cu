@@ -172,6 +172,7 @@ struct ClapTile {
   R re[32][33];
   R im[32][33];
   R hs[32][33];
+  R pad[8];  // consecutive tiles start 8 banks apart (the 4-ifg loads hit 4 tiles at once)
 };
 
 __device__ __forceinline__ uint32_t to_bits(float v) { return __float_as_uint(v); }
@@ -246,36 +247,70 @@ __device__ __forceinline__ R warp_median1024(const R (&o)[32]) {
   return (v0 + v1) * R(0.5);
 }
 
-// One window of one interferogram, computed by one warp in its tile.
-// On entry the tile holds the 24x24 window zero-padded to 32x32; on exit rows
-// and columns < 24 hold the filtered values times the pyramid weight / 1024.
+// One 32-point FFT per lane over a row (rows = true, lane = row) or a column
+// (lane = column) of the tile, in place. Not inlined: the window code calls it
+// four times and one copy keeps the kernel inside the instruction cache.
+// tw holds e^{-2 pi i k/32} (forward) or its conjugate (inverse), k < 16.
 template <typename R>
-__device__ __forceinline__ void clap_window_warp(ClapTile<R>& T, const int lane, const ClapArgs& a,
-                                                 const typename CT<R>::Tw& tw, const R* lp, const R* wt,
-                                                 const R (&g7)[7], const int rs, const int cs) {
+__device__ __noinline__ void fft_pass(R (*re)[33], R (*im)[33], const typename CT<R>::C* tw, const int lane,
+                                      const bool rows) {
   using C = typename CT<R>::C;
   C x[32];
-  // forward FFT along rows (lane = row; rows >= n_win are zero)
-  if (lane < a.n_win) {
 #pragma unroll
-    for (int k = 0; k < 32; ++k) x[k] = mk(T.re[lane][k], T.im[lane][k]);
-    fft32<R, false>(x, tw);
+  for (int k = 0; k < 32; ++k) x[k] = rows ? mk(re[lane][k], im[lane][k]) : mk(re[k][lane], im[k][lane]);
 #pragma unroll
-    for (int k = 0; k < 32; ++k) {
-      T.re[lane][k] = x[k].x;
-      T.im[lane][k] = x[k].y;
+  for (int i = 0; i < 32; ++i) {
+    const int r = ((i & 1) << 4) | ((i & 2) << 2) | (i & 4) | ((i & 8) >> 2) | ((i & 16) >> 4);
+    if (r > i) {
+      C t = x[i];
+      x[i] = x[r];
+      x[r] = t;
     }
   }
-  __syncwarp();
-  // forward FFT along columns (lane = column), |H|
 #pragma unroll
-  for (int k = 0; k < 32; ++k) x[k] = mk(T.re[k][lane], T.im[k][lane]);
-  fft32<R, false>(x, tw);
+  for (int half = 1; half < 32; half <<= 1) {
+    const int step = 16 / half;
+#pragma unroll
+    for (int s = 0; s < 32; s += 2 * half) {
+#pragma unroll
+      for (int k = 0; k < half; ++k) {
+        const int ti = k * step;
+        const C u = x[s + k];
+        const C v = x[s + k + half];
+        const C t = ti == 0 ? v : cmul(v, tw[ti]);
+        x[s + k] = mk(u.x + t.x, u.y + t.y);
+        x[s + k + half] = mk(u.x - t.x, u.y - t.y);
+      }
+    }
+  }
 #pragma unroll
   for (int k = 0; k < 32; ++k) {
-    T.re[k][lane] = x[k].x;
-    T.im[k][lane] = x[k].y;
-    T.hs[k][lane] = sqrt(x[k].x * x[k].x + x[k].y * x[k].y);
+    if (rows) {
+      re[lane][k] = x[k].x;
+      im[lane][k] = x[k].y;
+    } else {
+      re[k][lane] = x[k].x;
+      im[k][lane] = x[k].y;
+    }
+  }
+}
+
+// One window of one interferogram, computed by one warp in its tile.
+// On entry the tile holds the 24x24 window zero-padded to 32x32; on exit rows
+// and columns < n_win hold the filtered values times the pyramid weight / 1024.
+template <typename R>
+__device__ __forceinline__ void clap_window_warp(ClapTile<R>& T, const int lane, const ClapArgs& a,
+                                                 const typename CT<R>::C* twf, const typename CT<R>::C* twi,
+                                                 const R* lp, const R* wt, const R (&g7)[7], const int rs,
+                                                 const int cs) {
+  // forward FFT along rows (rows >= n_win are zero and stay zero), then columns
+  if (lane < a.n_win) fft_pass<R>(T.re, T.im, twf, lane, true);
+  __syncwarp();
+  fft_pass<R>(T.re, T.im, twf, lane, false);
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    const R xr = T.re[k][lane], xi = T.im[k][lane];
+    T.hs[k][lane] = sqrt(xr * xr + xi * xi);
   }
   __syncwarp();
   // 7x7 separable Gaussian 'same' convolution of fftshift(|H|), then
@@ -305,39 +340,29 @@ __device__ __forceinline__ void clap_window_warp(ClapTile<R>& T, const int lane,
     o[k] = acc;
   }
   const R med = warp_median1024<R>(o);
-  // H <- max((H/med)^alpha - 1, 0); spectrum *= H*beta + low_pass; inverse
-  // FFT along columns in registers.
+  // H <- max((H/med)^alpha - 1, 0); spectrum *= H*beta + low_pass
   const R beta = static_cast<R>(a.beta);
   const R alpha = static_cast<R>(a.alpha);
+  const R inv_med = med != R(0) ? R(1) / med : R(1);
 #pragma unroll
   for (int k = 0; k < 32; ++k) {
-    R v = o[k];
-    if (med != R(0)) v = v / med;
+    R v = o[k] * inv_med;
     v = a.alpha_is_one ? v - R(1) : pow(v, alpha) - R(1);
     if (v < R(0)) v = R(0);
     const R gk = v * beta + lp[k * 32 + lane];
-    x[k] = mk(T.re[k][lane] * gk, T.im[k][lane] * gk);
+    T.re[k][lane] *= gk;
+    T.im[k][lane] *= gk;
   }
-  fft32<R, true>(x, tw);
-#pragma unroll
-  for (int k = 0; k < 32; ++k) {
-    T.re[k][lane] = x[k].x;
-    T.im[k][lane] = x[k].y;
-  }
+  // inverse FFT along columns, then rows; keep the n_win x n_win corner, weighted
+  fft_pass<R>(T.re, T.im, twi, lane, false);
   __syncwarp();
-  // inverse FFT along rows; keep the n_win x n_win corner, weighted
   if (lane < a.n_win) {
-#pragma unroll
-    for (int k = 0; k < 32; ++k) x[k] = mk(T.re[lane][k], T.im[lane][k]);
-    fft32<R, true>(x, tw);
+    fft_pass<R>(T.re, T.im, twi, lane, true);
     const bool row_zero = lane < rs;
-#pragma unroll
-    for (int l = 0; l < 32; ++l) {
-      if (l < a.n_win) {
-        const R wv = (row_zero || l < cs) ? R(0) : wt[(lane - rs) * a.n_win + (l - cs)];
-        T.re[lane][l] = x[l].x * wv;
-        T.im[lane][l] = x[l].y * wv;
-      }
+    for (int l = 0; l < a.n_win; ++l) {
+      const R wv = (row_zero || l < cs) ? R(0) : wt[(lane - rs) * a.n_win + (l - cs)];
+      T.re[lane][l] *= wv;
+      T.im[lane][l] *= wv;
     }
   }
   __syncwarp();
@@ -350,10 +375,16 @@ __global__ void __launch_bounds__(128) k_clap(ClapArgs a, typename CT<R>::Tw tw)
   ClapTile<R>* tiles = reinterpret_cast<ClapTile<R>*>(smem_raw);
   R* lp = reinterpret_cast<R*>(tiles + 4);
   R* wt = lp + 1024;
+  C* twf = reinterpret_cast<C*>(wt + 1024);
+  C* twi = twf + 16;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nw = a.n_win, nw2 = nw * nw;
   for (int i = tid; i < 1024; i += 128) lp[i] = static_cast<R>(a.low_pass[i]);
   for (int i = tid; i < nw2; i += 128) wt[i] = static_cast<R>(a.wscaled[i]);
+  if (tid < 16) {
+    twf[tid] = tw.w[tid];
+    twi[tid] = mk(tw.w[tid].x, -tw.w[tid].y);
+  }
   R g7[7];
 #pragma unroll
   for (int i = 0; i < 7; ++i) g7[i] = static_cast<R>(a.g7[i]);
@@ -400,7 +431,7 @@ __global__ void __launch_bounds__(128) k_clap(ClapArgs a, typename CT<R>::Tw tw)
       tiles[q].im[li][lj] = v.y;
     }
     __syncthreads();
-    if (4 * g + warp < a.M) clap_window_warp<R>(T, lane, a, tw, lp, wt, g7, rs, cs);
+    if (4 * g + warp < a.M) clap_window_warp<R>(T, lane, a, twf, twi, lp, wt, g7, rs, cs);
     __syncthreads();
     for (int idx = tid; idx < nw2 * 4; idx += 128) {
       const int pix = idx >> 2, q = idx & 3;
@@ -412,7 +443,7 @@ __global__ void __launch_bounds__(128) k_clap(ClapArgs a, typename CT<R>::Tw tw)
 
 template <typename R>
 static size_t clap_smem_bytes() {
-  return 4 * sizeof(ClapTile<R>) + (1024 + 1024) * sizeof(R);
+  return 4 * sizeof(ClapTile<R>) + (1024 + 1024) * sizeof(R) + 32 * 2 * sizeof(R);
 }
 
 cudaError_t launch_clap(const ClapArgs& a, bool fp64, const Twiddles32f& tf, const Twiddles32d& td, int sm_count,
@@ -579,6 +610,7 @@ __device__ __forceinline__ int group_transpose_reduce(float2 (&v)[W], const int 
 template <int W>
 __device__ __forceinline__ void accumulate_column(float2 (&S)[W], const float2 z, const float2 rot, const float th,
                                                   const int m0) {
+  // th here is bp * (pi/4)/range; the anchor angle is th * m
   float2 u = cmul(z, cis_neg_anchor(th * static_cast<float>(m0)));
 #pragma unroll
   for (int k = 0; k < W; ++k) {
@@ -631,13 +663,16 @@ __device__ __forceinline__ void accumulate_four_columns(float2 (&S)[W], const fl
   }
 }
 
+// Per-PS column store: z (psdph), e^{-j theta} (the per-trial rotation, theta =
+// bp/range*pi/4 as the reference rounds it) and bp. Anchor angles are formed as
+// bp * ((pi/4)/range) * m.
 struct ColumnSmem {
-  float *zx, *zy, *rx, *ry, *th;
+  float *zx, *zy, *rx, *ry, *bp;
 };
 
 template <int W, int L>
-__device__ __forceinline__ void sweep_block(const ColumnSmem& cs, const int ncl, const int gl, const int m0,
-                                            const int t0, const int T, float& best_sq, int& best_t) {
+__device__ __forceinline__ void sweep_block(const ColumnSmem& cs, const float qr, const int ncl, const int gl,
+                                            const int m0, const int t0, const int T, float& best_sq, int& best_t) {
   float2 S[W];
 #pragma unroll
   for (int k = 0; k < W; ++k) S[k] = make_float2(0.f, 0.f);
@@ -650,18 +685,20 @@ __device__ __forceinline__ void sweep_block(const ColumnSmem& cs, const int ncl,
       const int c = gl + L * (k + i);
       z[i] = make_float2(cs.zx[c], cs.zy[c]);
       r[i] = make_float2(cs.rx[c], cs.ry[c]);
-      t[i] = cs.th[c];
+      t[i] = cs.bp[c] * qr;
     }
     accumulate_four_columns<W>(S, z, r, t, m0);
   }
   for (; k + 1 < ncl; k += 2) {
     const int c0 = gl + L * k, c1 = c0 + L;
-    accumulate_two_columns<W>(S, make_float2(cs.zx[c0], cs.zy[c0]), make_float2(cs.rx[c0], cs.ry[c0]), cs.th[c0],
-                              make_float2(cs.zx[c1], cs.zy[c1]), make_float2(cs.rx[c1], cs.ry[c1]), cs.th[c1], m0);
+    accumulate_two_columns<W>(S, make_float2(cs.zx[c0], cs.zy[c0]), make_float2(cs.rx[c0], cs.ry[c0]),
+                              cs.bp[c0] * qr, make_float2(cs.zx[c1], cs.zy[c1]), make_float2(cs.rx[c1], cs.ry[c1]),
+                              cs.bp[c1] * qr, m0);
   }
   if (k < ncl) {
     const int c0 = gl + L * k;
-    accumulate_column<W>(S, make_float2(cs.zx[c0], cs.zy[c0]), make_float2(cs.rx[c0], cs.ry[c0]), cs.th[c0], m0);
+    accumulate_column<W>(S, make_float2(cs.zx[c0], cs.zy[c0]), make_float2(cs.rx[c0], cs.ry[c0]), cs.bp[c0] * qr,
+                         m0);
   }
   int base;
   const int cnt = group_transpose_reduce<W, L>(S, gl, base);
@@ -717,33 +754,54 @@ __global__ void __launch_bounds__(128) k_topofit_f32(TopoArgs a, int mpad) {
     const int64_t cell = (active && !cpx) ? a.cell_of[s] : 0;
     bool zero = false, nonzero = false;
     float mn = __int_as_float(0x7f800000), mx = -mn;
-    for (int k = 0; k < ncl; ++k) {
-      const int c = gl + L * k;
-      float2 v = make_float2(0.f, 0.f);
-      float b = 0.f;
-      if (active && c < a.M) {
-        if (cpx) {
-          v = cpx[s * M + c];
-        } else {
-          // extract_patch_phase + normalize_complex_unit_magnitude (:1186-1205)
-          float2 f = filt[cell * a.Mp + c];
-          const float mag = hypotf(f.x, f.y);
-          if (mag != 0.f) f = make_float2(f.x / mag, f.y / mag);
-          if (ph_patch) ph_patch[s * M + c] = f;
-          v = cmul_rn(conjf2(f), ph_nm[s * M + c]);  // psdph (:687-689)
-        }
-        b = a.bp_row_inv ? a.bp[c] : a.bp[s * M + c];
-        if (v.x == 0.f && v.y == 0.f) {
-          zero = true;
-        } else {
-          nonzero = true;
-          mn = fminf(mn, b);
-          mx = fmaxf(mx, b);
+    // four columns per round with their global loads issued first
+    for (int k0c = 0; k0c < ncl; k0c += 4) {
+      float2 fv[4], pv[4];
+      float bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int c = gl + L * (k0c + i);
+        fv[i] = make_float2(0.f, 0.f);
+        pv[i] = make_float2(0.f, 0.f);
+        bv[i] = 0.f;
+        if (active && k0c + i < ncl && c < a.M) {
+          if (cpx) {
+            pv[i] = cpx[s * M + c];
+          } else {
+            fv[i] = filt[cell * a.Mp + c];
+            pv[i] = ph_nm[s * M + c];
+          }
+          bv[i] = a.bp_row_inv ? a.bp[c] : a.bp[s * M + c];
         }
       }
-      cs.zx[c] = v.x;
-      cs.zy[c] = v.y;
-      cs.th[c] = b;  // bp for now; theta once the range is known
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int c = gl + L * (k0c + i);
+        if (k0c + i >= ncl) break;
+        float2 v = make_float2(0.f, 0.f);
+        if (active && c < a.M) {
+          if (cpx) {
+            v = pv[i];
+          } else {
+            // extract_patch_phase + normalize_complex_unit_magnitude (:1186-1205)
+            float2 f = fv[i];
+            const float mag = hypotf(f.x, f.y);
+            if (mag != 0.f) f = make_float2(f.x / mag, f.y / mag);
+            if (ph_patch) ph_patch[s * M + c] = f;
+            v = cmul_rn(conjf2(f), pv[i]);  // psdph (:687-689)
+          }
+          if (v.x == 0.f && v.y == 0.f) {
+            zero = true;
+          } else {
+            nonzero = true;
+            mn = fminf(mn, bv[i]);
+            mx = fmaxf(mx, bv[i]);
+          }
+        }
+        cs.zx[c] = v.x;
+        cs.zy[c] = v.y;
+        cs.bp[c] = bv[i];
+      }
     }
     const bool any_zero = (__ballot_sync(kFull, zero) & gmask) != 0u;
     const bool any_nonzero = (__ballot_sync(kFull, nonzero) & gmask) != 0u;
@@ -754,33 +812,33 @@ __global__ void __launch_bounds__(128) k_topofit_f32(TopoArgs a, int mpad) {
     if (!(range != 0.f) || invalid) range = 1.f;
     for (int k = 0; k < ncl; ++k) {
       const int c = gl + L * k;
-      const float t = (cs.th[c] / range) * kQuarterPiF;
+      const float t = (cs.bp[c] / range) * kQuarterPiF;
       float sn, cn;
       sincosf(t, &sn, &cn);
-      cs.th[c] = t;
       cs.rx[c] = cn;
       cs.ry[c] = -sn;
     }
+    const float qr = kQuarterPiF / range;
     __syncwarp();
     // trial sweep over m = -n .. n (all groups run it; invalid ones discard it)
     float best_sq = -1.f;
     int best_t = 0;
     int t0 = 0;
-    for (; T - t0 >= 16; t0 += 16) sweep_block<16, L>(cs, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
+    for (; T - t0 >= 16; t0 += 16) sweep_block<16, L>(cs, qr, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
     if (T - t0 >= 8) {
-      sweep_block<8, L>(cs, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
+      sweep_block<8, L>(cs, qr, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
       t0 += 8;
     }
     if (T - t0 >= 4) {
-      sweep_block<4, L>(cs, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
+      sweep_block<4, L>(cs, qr, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
       t0 += 4;
     }
     if (T - t0 >= 2) {
-      sweep_block<2, L>(cs, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
+      sweep_block<2, L>(cs, qr, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
       t0 += 2;
     }
     if (T - t0 >= 1) {
-      sweep_block<1, L>(cs, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
+      sweep_block<1, L>(cs, qr, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
       t0 += 1;
     }
     // first maximum over the group (argmax_first_f32, :1526-1536)
@@ -794,14 +852,12 @@ __global__ void __launch_bounds__(128) k_topofit_f32(TopoArgs a, int mpad) {
       }
     }
     // refine_candidate (:1259-1303) with FP64 normal-equation sums; the
-    // column store now holds bp (th slots) and z e^{-j k0 bp} (rotation slots)
+    // rotation slots of the column store now hold z e^{-j k0 bp}
     const float k0 = kQuarterPiF / range * static_cast<float>(best_t - a.n_half);
     float ox = 0.f, oy = 0.f;
     for (int k = 0; k < ncl; ++k) {
       const int c = gl + L * k;
-      const float b = (active && c < a.M) ? (a.bp_row_inv ? a.bp[c] : a.bp[s * M + c]) : 0.f;
-      cs.th[c] = b;
-      const float2 r = cmul_rn(make_float2(cs.zx[c], cs.zy[c]), cis_neg_anchor(k0 * b));
+      const float2 r = cmul_rn(make_float2(cs.zx[c], cs.zy[c]), cis_neg_anchor(k0 * cs.bp[c]));
       cs.rx[c] = r.x;
       cs.ry[c] = r.y;
       ox += r.x;
@@ -814,7 +870,7 @@ __global__ void __launch_bounds__(128) k_topofit_f32(TopoArgs a, int mpad) {
     for (int k = 0; k < ncl; ++k) {
       const int c = gl + L * k;
       const double wgt = static_cast<double>(hypotf(cs.zx[c], cs.zy[c]));
-      const double wb = __dmul_rn(wgt, static_cast<double>(cs.th[c]));
+      const double wb = __dmul_rn(wgt, static_cast<double>(cs.bp[c]));
       dl = __dadd_rn(dl, __dmul_rn(wb, wb));
       const float2 q = cmul_rn(make_float2(cs.rx[c], cs.ry[c]), oc);
       mopt = __dadd_rn(mopt, __dmul_rn(wb, __dmul_rn(wgt, static_cast<double>(atan2f(q.y, q.x)))));
@@ -826,7 +882,7 @@ __global__ void __launch_bounds__(128) k_topofit_f32(TopoArgs a, int mpad) {
     float mx2 = 0.f, my2 = 0.f, den2 = 0.f;
     for (int k = 0; k < ncl; ++k) {
       const int c = gl + L * k;
-      const float2 r = cmul_rn(make_float2(cs.zx[c], cs.zy[c]), cis_neg_anchor(K1 * cs.th[c]));
+      const float2 r = cmul_rn(make_float2(cs.zx[c], cs.zy[c]), cis_neg_anchor(K1 * cs.bp[c]));
       mx2 += r.x;
       my2 += r.y;
       den2 += hypotf(r.x, r.y);
