@@ -118,7 +118,11 @@ int ps2_load_patch(ps2_ctx* ctx, const ps2_patch_desc* desc);
  * timing); stats may be NULL or hold n_iter entries. */
 int ps2_iterate(ps2_ctx* ctx, int64_t n_iter, ps2_iter_stats* stats);
 /* Runs iterations until the reference's stop rule holds
- * (|delta gamma_change| < gamma_change_convergence or i_loop >= max). */
+ * (|delta gamma_change| < gamma_change_convergence or i_loop >= max). The
+ * first iteration runs as individual launches; the rest run as one CUDA graph
+ * launch (a WHILE conditional node whose body is one iteration), built on the
+ * first call after ps2_load_patch. PS2_NO_GRAPH=1 in the environment selects
+ * individual launches throughout. */
 int ps2_run_to_convergence(ps2_ctx* ctx, ps2_iter_stats* last);
 /* Resets the loop state of the loaded patch to iteration 1 (K=0, w=weight0). */
 int ps2_reset(ps2_ctx* ctx);

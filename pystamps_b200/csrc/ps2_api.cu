@@ -21,6 +21,7 @@
 #include <mutex>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -201,7 +202,11 @@ struct ps2_ctx {
   Twiddles32d twd;
   DevBuf ph_nm, bp, amp, perm, cell_start, cell_of, w0, K[2], w, coh, C, nopt, grid, win, filt, low_pass, wscaled,
       taps, lut, nr0, nr_scaled, state, stats, hist, n_invalid, rms_partial, ph_res, scratch;
-  int kcur = 0;
+  cudaGraph_t loop_graph = nullptr;
+  cudaGraphExec_t loop_exec = nullptr;
+  bool graph_failed = false;
+  bool last_run_graph = false;
+  int64_t graph_body_launches = 0;
   int topo_blocks = 0;
   int64_t iters_done = 0;  // since load/reset
   double* h_stats = nullptr;  // pinned [8]
@@ -328,12 +333,14 @@ int copy_in(ps2_ctx* c, DevBuf& dst, const void* src, size_t bytes, bool on_devi
   return PS2_OK;
 }
 
-int run_one_iteration(ps2_ctx* c, bool force_continue, cudaEvent_t* ev) {
+// Queues one gamma iteration on the context's stream. `later` selects the form
+// of iterations 2.. (P-square weights from the previous table, or the SNR
+// weight kernel); `capturing` queues into a graph without touching counters.
+int enqueue_iteration(ps2_ctx* c, bool later, bool force_continue, cudaEvent_t* ev, int64_t* launched_out) {
   const bool fp64 = c->fp64;
-  const int cur = c->kcur;
   int64_t launched = 0;
   if (ev) CK(cudaEventRecord(ev[0], c->st));
-  if (!c->psquare && c->iters_done > 0) {
+  if (!c->psquare && later) {
     TopoArgs t = topo_args(c, nullptr, nullptr, nullptr);
     t.ph_res = c->ph_res.p;
     CK(launch_snr_weight(t, c->amp.as<float>(), c->w.p, fp64, c->sm_count, c->st));
@@ -342,15 +349,18 @@ int run_one_iteration(ps2_ctx* c, bool force_continue, cudaEvent_t* ev) {
   CK(cudaMemsetAsync(c->hist.p, 0, sizeof(int32_t) * PS2_COH_BINS, c->st));
   CK(cudaMemsetAsync(c->n_invalid.p, 0, sizeof(int32_t), c->st));
   CK(cudaMemsetAsync(c->rms_partial.p, 0, sizeof(double) * c->topo_blocks, c->st));
-  const int mode = (c->iters_done > 0 && c->psquare) ? 1 : 0;
-  CK(launch_bin(bin_args(c, mode, c->K[cur].p), fp64, c->sm_count, c->st));
+  const int mode = (later && c->psquare) ? 1 : 0;
+  CK(launch_bin(bin_args(c, mode, c->K[0].p), fp64, c->sm_count, c->st));
   ++launched;
   if (ev) CK(cudaEventRecord(ev[1], c->st));
   CK(launch_clap(clap_args(c, c->grid.p, c->win.p), fp64, c->twf, c->twd, c->sm_count, c->st));
   CK(launch_overlap(overlap_args(c, c->win.p, c->filt.p), fp64, c->st));
   launched += 2;
   if (ev) CK(cudaEventRecord(ev[2], c->st));
-  TopoArgs t = topo_args(c, c->K[1 - cur].p, c->C.p, c->coh.p);
+  // K[1] keeps the K this iteration binned with (pm1's ph_weight needs it);
+  // topofit then rewrites K[0] in place
+  CK(cudaMemcpyAsync(c->K[1].p, c->K[0].p, rsz(c) * c->N, cudaMemcpyDeviceToDevice, c->st));
+  TopoArgs t = topo_args(c, c->K[0].p, c->C.p, c->coh.p);
   if (!c->psquare) t.ph_res = c->ph_res.p;
   CK(launch_topofit(t, fp64, c->topo_blocks, c->st));
   ++launched;
@@ -377,9 +387,54 @@ int run_one_iteration(ps2_ctx* c, bool force_continue, cudaEvent_t* ev) {
   CK(launch_finalize(f, c->st));
   ++launched;
   if (ev) CK(cudaEventRecord(ev[4], c->st));
-  c->kcur = 1 - cur;
+  if (launched_out) *launched_out = launched;
+  return PS2_OK;
+}
+
+int run_one_iteration(ps2_ctx* c, bool force_continue, cudaEvent_t* ev) {
+  int64_t launched = 0;
+  int rc = enqueue_iteration(c, c->iters_done > 0, force_continue, ev, &launched);
+  if (rc) return rc;
   c->iters_done += 1;
   c->launches += launched;
+  return PS2_OK;
+}
+
+void drop_loop_graph(ps2_ctx* c) {
+  if (c->loop_exec) cudaGraphExecDestroy(c->loop_exec);
+  if (c->loop_graph) cudaGraphDestroy(c->loop_graph);
+  c->loop_exec = nullptr;
+  c->loop_graph = nullptr;
+}
+
+// The loop from iteration 2 on as one graph: a WHILE conditional node whose
+// body is one iteration followed by k_loop_continue, which clears the
+// condition when finalize raised the stop flag (native_stage2.rs:312-314).
+int build_loop_graph(ps2_ctx* c, int64_t* body_launches) {
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  c->loop_graph = g;
+  cudaGraphConditionalHandle h;
+  CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams p{};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, g, nullptr, 0, &p));
+  cudaGraph_t body = p.conditional.phGraph_out[0];
+  CK(cudaStreamBeginCaptureToGraph(c->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  int64_t launched = 0;
+  int rc = enqueue_iteration(c, true, false, nullptr, &launched);
+  cudaError_t e2 = rc ? cudaSuccess : launch_loop_continue(h, c->stats.as<double>(), c->st);
+  cudaGraph_t captured = nullptr;
+  cudaError_t e3 = cudaStreamEndCapture(c->st, &captured);
+  if (rc) return rc;
+  CK(e2);
+  CK(e3);
+  CK(cudaGraphInstantiate(&c->loop_exec, g, 0));
+  *body_launches = launched + 1;
   return PS2_OK;
 }
 
@@ -398,7 +453,6 @@ int reset_state(ps2_ctx* c) {
   double st0[4] = {0.0, 1.0, 0.0, 0.0};
   CK(cudaMemcpyAsync(c->state.p, st0, sizeof(st0), cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
-  c->kcur = 0;
   c->iters_done = 0;
   c->last = ps2_iter_stats{};
   return PS2_OK;
@@ -449,6 +503,7 @@ void ps2_destroy(ps2_ctx* c) {
                     &c->taps, &c->lut, &c->nr0, &c->nr_scaled, &c->state, &c->stats, &c->hist, &c->n_invalid,
                     &c->rms_partial, &c->ph_res, &c->scratch};
   for (DevBuf* b : bufs) b->release();
+  drop_loop_graph(c);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
   if (c->h_stats) cudaFreeHost(c->h_stats);
   if (c->st) cudaStreamDestroy(c->st);
@@ -476,6 +531,8 @@ int ps2_load_patch(ps2_ctx* c, const ps2_patch_desc* d) {
   int rc = clap_geometry(d->n_i, d->n_j, d->clap_window, &n_inc, &nwi, &nwj);
   if (rc) return rc;
   c->loaded = false;
+  drop_loop_graph(c);
+  c->graph_failed = false;
   c->fp64 = d->precision == PS2_PRECISION_FP64;
   c->N = d->n_ps;
   c->M = static_cast<int>(d->n_ifg);
@@ -651,12 +708,41 @@ int ps2_run_to_convergence(ps2_ctx* c, ps2_iter_stats* last) {
   if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "no patch loaded");
   CK(cudaSetDevice(c->device));
   const int64_t cap = std::max<int64_t>(c->max_iter, 1) + 1;
-  int rc = ensure_events(c, 5);
+  int rc = ensure_events(c, 7);
   if (rc) return rc;
   c->launches = 0;
   c->last_ms = 0.0;
+  c->last_run_graph = false;
   for (int i = 0; i < 4; ++i) c->kernel_ms[i] = 0.0;
+  const char* ng = getenv("PS2_NO_GRAPH");
+  const bool no_graph = ng != nullptr && ng[0] != '\0' && ng[0] != '0';
   for (int64_t k = 0; k < cap; ++k) {
+    if (c->iters_done > 0 && !no_graph && !c->graph_failed && !c->loop_exec) {
+      if (build_loop_graph(c, &c->graph_body_launches)) {
+        // capture refused (driver too old, ...): individual launches from here on
+        drop_loop_graph(c);
+        cudaGetLastError();
+        c->graph_failed = true;
+      }
+    }
+    if (c->iters_done > 0 && !no_graph && c->loop_exec) {
+      // iterations 2.. as one graph launch
+      const int64_t before = c->last.i_loop;
+      CK(cudaEventRecord(c->evpool[5], c->st));
+      CK(cudaGraphLaunch(c->loop_exec, c->st));
+      CK(cudaEventRecord(c->evpool[6], c->st));
+      CK(cudaMemcpyAsync(c->h_stats, c->stats.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+      CK(cudaStreamSynchronize(c->st));
+      float ms;
+      CK(cudaEventElapsedTime(&ms, c->evpool[5], c->evpool[6]));
+      c->last_ms += ms;
+      fill_stats(c->h_stats, &c->last);
+      const int64_t ran = c->last.i_loop - before;
+      c->iters_done += ran;
+      c->launches += ran * c->graph_body_launches;
+      c->last_run_graph = true;
+      break;
+    }
     rc = run_one_iteration(c, false, c->evpool.data());
     if (rc) return rc;
     CK(cudaMemcpyAsync(c->h_stats, c->stats.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
@@ -710,7 +796,7 @@ int ps2_download(ps2_ctx* c, ps2_outputs* o) {
     return PS2_OK;
   };
   int rc;
-  if ((rc = fetch_vec(c->K[c->kcur].p, o->K_ps))) return rc;
+  if ((rc = fetch_vec(c->K[0].p, o->K_ps))) return rc;
   if ((rc = fetch_vec(c->C.p, o->C_ps))) return rc;
   if ((rc = fetch_vec(c->coh.p, o->coh_ps))) return rc;
   if ((rc = fetch_vec(c->coh.p, o->coh_ps_save))) return rc;
@@ -776,7 +862,7 @@ int ps2_download(ps2_ctx* c, ps2_outputs* o) {
   if (want_w && c->iters_done > 0) {
     DevBuf out;
     CK(out.alloc(Cz * N * M));
-    BinArgs a = bin_args(c, 0, c->K[1 - c->kcur].p);
+    BinArgs a = bin_args(c, 0, c->K[1].p);
     CK(launch_ph_weight(a, N, fp64, perm, out.p, c->st));
     CK(cudaStreamSynchronize(c->st));
     if (fp64) {

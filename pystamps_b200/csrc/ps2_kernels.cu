@@ -1255,6 +1255,17 @@ __global__ void __launch_bounds__(256) k_finalize(FinalizeArgs a) {
   }
 }
 
+// Body tail of the graph that runs the loop to convergence: keep looping while
+// the finalize of this iteration did not raise the stop flag.
+__global__ void k_loop_continue(cudaGraphConditionalHandle h, const double* stats) {
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, stats[3] == 0.0 ? 1u : 0u);
+}
+
+cudaError_t launch_loop_continue(cudaGraphConditionalHandle h, const double* stats, cudaStream_t st) {
+  k_loop_continue<<<1, 32, 0, st>>>(h, stats);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t st) {
   k_finalize<<<1, 256, 0, st>>>(a);
   return cudaGetLastError();

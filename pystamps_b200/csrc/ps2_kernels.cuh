@@ -111,6 +111,7 @@ cudaError_t launch_overlap(const OverlapArgs& a, bool fp64, cudaStream_t st);
 cudaError_t launch_topofit(const TopoArgs& a, bool fp64, int grid_blocks, cudaStream_t st);
 int topofit_grid_blocks(int sm_count, bool fp64);
 cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t st);
+cudaError_t launch_loop_continue(cudaGraphConditionalHandle h, const double* stats, cudaStream_t st);
 cudaError_t launch_snr_weight(const TopoArgs& t, const float* amp, void* w_out, bool fp64, int sm_count,
                               cudaStream_t st);
 cudaError_t launch_random_hist(const double* rnd, int64_t n_rand, const double* bp, int m, const int64_t* ia,

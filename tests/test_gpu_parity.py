@@ -342,3 +342,24 @@ def test_stage2_deterministic_and_bounded_at_precision_size(S):
     assert st64["i_loop"] == st["i_loop"]
     d = np.abs(c["coh_ps"] - coh)
     assert np.median(d) <= GAMMA_TOL
+
+
+def test_graph_loop_matches_individual_launches(S, monkeypatch):
+    """The loop to convergence as one conditional-WHILE graph launch gives the
+    same bits as the same kernels launched one by one."""
+    from pystamps_b200 import synth
+
+    patch = synth.make_patch(5000, 20, 32, 41, seed=55, n_rand=5000)
+    prep = S.prepare_patch(patch)
+    monkeypatch.setenv("PS2_NO_GRAPH", "1")
+    a = S.run_stage2(prep, keys=["K_ps", "coh_ps", "ph_grid", "Nr"])
+    monkeypatch.setenv("PS2_NO_GRAPH", "0")
+    with S.Stage2Context() as ctx:
+        ctx.load(prep)
+        st = ctx.run()
+        b = ctx.download(["K_ps", "coh_ps", "ph_grid", "Nr"])
+        launches = ctx.launch_count()
+    assert st["i_loop"] == a["i_loop"] > 1
+    assert launches >= 5 * st["i_loop"]
+    for k in ("K_ps", "coh_ps", "ph_grid", "Nr"):
+        np.testing.assert_array_equal(a[k], b[k])
