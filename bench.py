@@ -40,9 +40,10 @@ sys.path.insert(0, str(ROOT))
 METRIC = "Stage-2 PS×ifg/s per gamma iter, FP32 vs plain FP64 GPU at max|Δγ|≤1e-4"
 UNIT = "PS*ifg/s"
 FP32_LANES_PER_SM = 128
-# DRAM bytes per topofit launch from the committed ncu capture (profiles/), scaled
-# to the full-scale workload; None until measured.
-TOPOFIT_TRAFFIC_BYTES = None
+# DRAM bytes (read + write) per PS x ifg of one k_topofit_f32 launch, from the ncu
+# capture at 250,000 PS x 60 ifg in profiles/kernels_precision_250k_ps_60_ifg.md
+# (195.5 MB per launch); the reported traffic scales it by N x M.
+TOPOFIT_TRAFFIC_BYTES_PER_PS_IFG = 195.5e6 / (250_000 * 60)
 
 
 def parse():
@@ -51,7 +52,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="E", help="A, B, D or E (default E, the full-scale patch)")
+    ap.add_argument("--workload", default="E",
+                    help="A, B, D or E (default E, the full-scale patch), or C: 64 uneven patches")
     ap.add_argument("--n-ps", type=int, default=0, help="override the PS count (profiling a smaller case)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-fp64", action="store_true")
@@ -259,7 +261,8 @@ def run_ours(args, rank: int, world: int, dist):
     roofline = {
         "kernel": "k_topofit_f32", "bound": "fp32", "achieved": achieved, "peak": fp32_peak_tflops,
         "unit": "TFLOP/s", "frac": achieved / fp32_peak_tflops,
-        "traffic": TOPOFIT_TRAFFIC_BYTES,
+        "traffic": TOPOFIT_TRAFFIC_BYTES_PER_PS_IFG * n * m,
+        "traffic_source": "ncu dram__bytes_read+write at 250k PS x 60 ifg scaled by PS x ifg",
         "algorithmic": f"(8*T+32) flop per PS x ifg, T={T}: {flops:.3e} flop per launch",
         "peak_source": f"nominal FP32 FMA rate {sms} SM x {FP32_LANES_PER_SM} lanes x 2 x {sm_max:.0f} MHz "
                        "(MEASURED_PEAKS.json has no FP32 figure)",
@@ -362,6 +365,64 @@ def run_ours(args, rank: int, world: int, dist):
         print(json.dumps(line), flush=True)
 
 
+def run_batched(args, rank: int, world: int, dist):
+    """The uneven multi-patch workload: 64 patches, PS log-uniform in 5k-400k,
+    30-120 interferograms, LPT-assigned to ranks, 4 concurrent streams per GPU.
+    One step = every patch of the rank loaded, iterated to convergence and its
+    K/C/coh/N_opt downloaded; value = sum(N*M*iterations) / t (max over ranks)."""
+    import torch
+
+    from pystamps_b200 import batch, stage2 as S, synth
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    shapes = synth.batched_workload_shapes(64)
+    costs = [batch.patch_cost(n, m, t, c, c) for n, m, c, t in shapes]
+    share = batch.lpt_assign(costs, world)[rank]
+    preps = []
+    for i in share:
+        n, m, cells, t = shapes[i]
+        p = synth.make_patch(n, m, cells, t, seed=2005 + 2000 + i)
+        preps.append(S.prepare_patch(p))
+    batch.run_patches(preps[:2], device=dev, streams=2)  # warm-up
+    work = sum(p.n_ps * p.n_ifg for p in preps)
+    times, done = [], []
+    for step in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        t0 = time.perf_counter()
+        res = batch.run_patches(preps, device=dev, streams=4)
+        ev1.record()
+        torch.cuda.synchronize()
+        t = max(time.perf_counter() - t0, ev0.elapsed_time(ev1) / 1e3)
+        iters = sum(r["i_loop"] * p.n_ps * p.n_ifg for r, p in zip(res, preps))
+        if step >= args.warmup:
+            times.append(t)
+            done.append(iters)
+    t_step = statistics.median(times)
+    local = torch.tensor([t_step, float(statistics.median(done))], dtype=torch.float64, device=f"cuda:{dev}")
+    if dist is not None:
+        tt = local.clone()
+        dist.all_reduce(tt[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(tt[1:2], op=dist.ReduceOp.SUM)
+        local = tt
+    if rank == 0:
+        t_max, units = float(local[0]), float(local[1])
+        line = {"metric": METRIC, "value": units / t_max, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_max * 1e3, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator pystamps_b200.synth)",
+                "config": {"workload": "batched-64-uneven-patches", "patches": 64,
+                           "ps_x_ifg_total": int(sum(n * m for n, m, _, _ in shapes)),
+                           "parallelism": f"LPT by patch over {world} GPU(s), 4 streams each"},
+                "e2e": {"value": units / t_max, "unit": UNIT,
+                        "h2d_bytes_per_step": int(sum(p.ph_nm.nbytes + p.bperp.nbytes for p in preps)),
+                        "d2h_bytes_per_step": int(sum(32 * p.n_ps for p in preps))}}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -381,6 +442,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.workload == "C":
+            run_batched(args, rank, world, dist)
         else:
             run_ours(args, rank, world, dist)
     finally:

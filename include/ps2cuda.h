@@ -133,6 +133,11 @@ int ps2_download(ps2_ctx* ctx, ps2_outputs* out);
  * each kernel family in it: [0] binning, [1] CLAP windows + overlap-add,
  * [2] topofit, [3] convergence / weighting update. */
 int ps2_last_timing(const ps2_ctx* ctx, double* total_ms, double* per_kernel_ms /*[4] or NULL*/);
+/* Times the FP32 topofit of the loaded patch with 4, 8, 16 and 32 lanes per PS
+ * and keeps the fastest for this context and for later loads with the same
+ * n_ifg and power-of-two PS bucket (process-wide table). ms_per_candidate:
+ * NULL or [4]. */
+int ps2_autotune(ps2_ctx* ctx, int32_t* chosen_lanes, double* ms_per_candidate);
 /* Number of kernel launches issued by the last iterate/run call. */
 int64_t ps2_last_launch_count(const ps2_ctx* ctx);
 

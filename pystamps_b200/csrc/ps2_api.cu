@@ -62,9 +62,12 @@ struct DevBuf {
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
+  // keeps the current allocation when it is large enough (a context reloads
+  // patches without returning to cudaMalloc/cudaFree, which synchronise)
   cudaError_t alloc(size_t n) {
-    release();
     if (n == 0) n = 16;
+    if (p && bytes >= n) return cudaSuccess;
+    release();
     cudaError_t e = cudaMalloc(&p, n);
     if (e == cudaSuccess) bytes = n;
     else p = nullptr;
@@ -183,6 +186,30 @@ std::vector<double> window_weight_scaled(int n_win, int n_ex) {
   return out;
 }
 
+// Autotuned lanes per PS for the FP32 topofit, keyed by (n_ifg, log2 n_ps).
+std::mutex g_tune_mu;
+std::vector<std::pair<int64_t, int>> g_tune_cache;
+int64_t tune_key(int64_t M, int64_t N) {
+  int64_t lb = 0;
+  while ((int64_t(1) << lb) < N) ++lb;
+  return M * 64 + lb;
+}
+int tune_lookup(int64_t key) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  for (auto& kv : g_tune_cache)
+    if (kv.first == key) return kv.second;
+  return 0;
+}
+void tune_store(int64_t key, int lanes) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  for (auto& kv : g_tune_cache)
+    if (kv.first == key) {
+      kv.second = lanes;
+      return;
+    }
+  g_tune_cache.emplace_back(key, lanes);
+}
+
 }  // namespace
 
 struct ps2_ctx {
@@ -201,12 +228,13 @@ struct ps2_ctx {
   Twiddles32f twf;
   Twiddles32d twd;
   DevBuf ph_nm, bp, amp, perm, cell_start, cell_of, w0, K[2], w, coh, C, nopt, grid, win, filt, low_pass, wscaled,
-      taps, lut, nr0, nr_scaled, state, stats, hist, n_invalid, rms_partial, ph_res, scratch;
+      taps, lut, nr0, nr_scaled, state, stats, hist, n_invalid, rms_partial, ph_res, scratch, stage;
   cudaGraph_t loop_graph = nullptr;
   cudaGraphExec_t loop_exec = nullptr;
   bool graph_failed = false;
   bool last_run_graph = false;
   int64_t graph_body_launches = 0;
+  int topo_lanes = 0;  // 0: rule from n_ifg; else chosen by ps2_autotune
   int topo_blocks = 0;
   int64_t iters_done = 0;  // since load/reset
   double* h_stats = nullptr;  // pinned [8]
@@ -308,6 +336,7 @@ TopoArgs topo_args(ps2_ctx* c, void* K_out, void* C_out, void* coh_io) {
   t.cutoff0 = c->cutoff0;
   t.dbin = c->dbin;
   t.accumulate_stats = 1;
+  t.lanes = c->topo_lanes;
   return t;
 }
 
@@ -501,7 +530,7 @@ void ps2_destroy(ps2_ctx* c) {
   DevBuf* bufs[] = {&c->ph_nm, &c->bp, &c->amp, &c->perm, &c->cell_start, &c->cell_of, &c->w0, &c->K[0], &c->K[1],
                     &c->w, &c->coh, &c->C, &c->nopt, &c->grid, &c->win, &c->filt, &c->low_pass, &c->wscaled,
                     &c->taps, &c->lut, &c->nr0, &c->nr_scaled, &c->state, &c->stats, &c->hist, &c->n_invalid,
-                    &c->rms_partial, &c->ph_res, &c->scratch};
+                    &c->rms_partial, &c->ph_res, &c->scratch, &c->stage};
   for (DevBuf* b : bufs) b->release();
   drop_loop_graph(c);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
@@ -589,34 +618,26 @@ int ps2_load_patch(ps2_ctx* c, const ps2_patch_desc* d) {
   CK(cudaMemcpyAsync(c->cell_of.p, cell_of.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, c->st));
   // row data, gathered into cell order on the device
   {
-    DevBuf tmp;
-    rc = copy_in(c, tmp, d->ph_nm, sizeof(float) * 2 * N * M, dev);
+    rc = copy_in(c, c->stage, d->ph_nm, sizeof(float) * 2 * N * M, dev);
     if (rc) return rc;
     CK(c->ph_nm.alloc(sizeof(float) * 2 * N * M));
-    CK(launch_gather_rows(tmp.p, c->ph_nm.p, c->perm.as<int32_t>(), N, sizeof(float) * 2 * M, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    tmp.release();
+    CK(launch_gather_rows(c->stage.p, c->ph_nm.p, c->perm.as<int32_t>(), N, sizeof(float) * 2 * M, c->st));
   }
   if (c->bp_row_inv) {
     rc = copy_in(c, c->bp, d->bperp, sizeof(float) * M, dev);
     if (rc) return rc;
   } else {
-    DevBuf tmp;
-    rc = copy_in(c, tmp, d->bperp, sizeof(float) * N * M, dev);
+    // the staging buffer is free again once the ph_nm gather (same stream) ran
+    rc = copy_in(c, c->stage, d->bperp, sizeof(float) * N * M, dev);
     if (rc) return rc;
     CK(c->bp.alloc(sizeof(float) * N * M));
-    CK(launch_gather_rows(tmp.p, c->bp.p, c->perm.as<int32_t>(), N, sizeof(float) * M, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    tmp.release();
+    CK(launch_gather_rows(c->stage.p, c->bp.p, c->perm.as<int32_t>(), N, sizeof(float) * M, c->st));
   }
   if (!c->psquare) {
-    DevBuf tmp;
-    rc = copy_in(c, tmp, d->amp, sizeof(float) * N * M, dev);
+    rc = copy_in(c, c->stage, d->amp, sizeof(float) * N * M, dev);
     if (rc) return rc;
     CK(c->amp.alloc(sizeof(float) * N * M));
-    CK(launch_gather_rows(tmp.p, c->amp.p, c->perm.as<int32_t>(), N, sizeof(float) * M, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    tmp.release();
+    CK(launch_gather_rows(c->stage.p, c->amp.p, c->perm.as<int32_t>(), N, sizeof(float) * M, c->st));
     CK(c->ph_res.alloc(R * N * M));
   } else {
     c->amp.release();
@@ -653,6 +674,8 @@ int ps2_load_patch(ps2_ctx* c, const ps2_patch_desc* d) {
   CK(c->hist.alloc(sizeof(int32_t) * PS2_COH_BINS));
   CK(c->n_invalid.alloc(sizeof(int32_t)));
   c->topo_blocks = topofit_grid_blocks(c->sm_count, c->fp64);
+  c->topo_lanes = tune_lookup(tune_key(c->M, c->N));
+  CK(cudaMemsetAsync(c->filt.p, 0, Cz * G * c->Mp, c->st));
   CK(c->rms_partial.alloc(sizeof(double) * c->topo_blocks));
   rc = reset_state(c);
   if (rc) return rc;
@@ -758,6 +781,47 @@ int ps2_run_to_convergence(ps2_ctx* c, ps2_iter_stats* last) {
     if (c->last.stop) break;
   }
   if (last) *last = c->last;
+  return PS2_OK;
+}
+
+int ps2_autotune(ps2_ctx* c, int32_t* chosen_lanes, double* ms_per_candidate) {
+  if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "no patch loaded");
+  CK(cudaSetDevice(c->device));
+  const int cands[4] = {4, 8, 16, 32};
+  if (c->fp64) {
+    if (chosen_lanes) *chosen_lanes = 0;
+    return PS2_OK;  // the plain FP64 kernel has a single shape
+  }
+  int rc = ensure_events(c, 2);
+  if (rc) return rc;
+  DevBuf kk, cc, hh;
+  CK(kk.alloc(rsz(c) * c->N));
+  CK(cc.alloc(rsz(c) * c->N));
+  CK(hh.alloc(rsz(c) * c->N));
+  int best = 0;
+  double best_ms = 1e300;
+  for (int i = 0; i < 4; ++i) {
+    TopoArgs t = topo_args(c, kk.p, cc.p, hh.p);
+    t.nopt = nullptr;
+    t.accumulate_stats = 0;
+    t.lanes = cands[i];
+    CK(launch_topofit(t, false, c->topo_blocks, c->st));  // warm-up
+    CK(cudaEventRecord(c->evpool[0], c->st));
+    CK(launch_topofit(t, false, c->topo_blocks, c->st));
+    CK(cudaEventRecord(c->evpool[1], c->st));
+    CK(cudaStreamSynchronize(c->st));
+    float ms;
+    CK(cudaEventElapsedTime(&ms, c->evpool[0], c->evpool[1]));
+    if (ms_per_candidate) ms_per_candidate[i] = ms;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = cands[i];
+    }
+  }
+  c->topo_lanes = best;
+  drop_loop_graph(c);  // the captured loop holds the previous shape
+  tune_store(tune_key(c->M, c->N), best);
+  if (chosen_lanes) *chosen_lanes = best;
   return PS2_OK;
 }
 

@@ -52,6 +52,20 @@ __device__ __forceinline__ double2 mk(double a, double b) { return make_double2(
 
 // ============================================================= binning ====
 template <typename R>
+__device__ __forceinline__ R bin_weight(const BinArgs& a, const R* __restrict__ W, const R* __restrict__ coh,
+                                        const int s) {
+  if (a.mode == 3) return R(1);
+  if (a.mode != 1) return W[s];
+  // psquare_weighting lookup (native_stage2.rs:1674-1682)
+  const double v = __dmul_rn(static_cast<double>(coh[s]), 1000.0);
+  double r = v >= 0.0 ? floor(__dadd_rn(v, 0.5)) : ceil(__dsub_rn(v, 0.5));
+  r = fmin(fmax(r, 0.0), static_cast<double>(a.lut_len - 1));
+  const int ix = isnan(r) ? 0 : static_cast<int>(r);
+  const double t = 1.0 - a.lut[ix];
+  return static_cast<R>(t * t);
+}
+
+template <typename R>
 __global__ void __launch_bounds__(256) k_bin(BinArgs a) {
   using C = typename CT<R>::C;
   const float2* __restrict__ ph = static_cast<const float2*>(a.ph_nm);
@@ -70,39 +84,49 @@ __global__ void __launch_bounds__(256) k_bin(BinArgs a) {
     const int chunk = static_cast<int>(task - cell * a.nchunk);
     const int c = chunk * 32 + lane;
     const bool active = c < a.M;
+    const bool write_w = a.mode == 1 && chunk == 0 && lane == 0;
     const int s0 = a.cell_start[cell], s1 = a.cell_start[cell + 1];
     R ax = R(0), ay = R(0);
-#pragma unroll 4
-    for (int s = s0; s < s1; ++s) {
-      R w = R(1);
-      if (a.mode == 3) {
-      } else if (a.mode == 1) {
-        // psquare_weighting lookup (native_stage2.rs:1674-1682)
-        const double v = __dmul_rn(static_cast<double>(coh[s]), 1000.0);
-        double r = v >= 0.0 ? floor(__dadd_rn(v, 0.5)) : ceil(__dsub_rn(v, 0.5));
-        r = fmin(fmax(r, 0.0), static_cast<double>(a.lut_len - 1));
-        const int ix = isnan(r) ? 0 : static_cast<int>(r);
-        const double t = 1.0 - a.lut[ix];
-        w = static_cast<R>(t * t);
-        if (chunk == 0 && lane == 0) W[s] = w;
-      } else {
-        w = W[s];
+    // rows are taken four at a time with every load issued before the
+    // arithmetic; the sum itself stays sequential in row order
+    for (int sb = s0; sb < s1; sb += 4) {
+      R wv[4], kv[4], bv[4];
+      float2 v[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int s = sb + i;
+        wv[i] = R(0);
+        kv[i] = R(0);
+        bv[i] = R(0);
+        v[i] = make_float2(0.f, 0.f);
+        if (s < s1) {
+          wv[i] = bin_weight<R>(a, W, coh, s);
+          if (a.mode != 3) kv[i] = K[s];
+          if (active) {
+            v[i] = ph[static_cast<int64_t>(s) * M + c];
+            if (a.mode != 3)
+              bv[i] = a.bp_row_inv ? static_cast<R>(bp[c]) : static_cast<R>(bp[static_cast<int64_t>(s) * M + c]);
+          }
+        }
       }
-      if (active && a.mode == 3) {
-        // accumulate_grid alone: ph_nm holds ph_weight, no ramp and no weight
-        const float2 v = ph[static_cast<int64_t>(s) * M + c];
-        ax = add_rn(ax, static_cast<R>(v.x));
-        ay = add_rn(ay, static_cast<R>(v.y));
-      } else if (active) {
-        const R k = K[s];
-        const R b = a.bp_row_inv ? static_cast<R>(bp[c]) : static_cast<R>(bp[static_cast<int64_t>(s) * M + c]);
-        const R phs = -(b * k);
-        R sn, cs;
-        sincos_r(phs, &sn, &cs);
-        const float2 v = ph[static_cast<int64_t>(s) * M + c];
-        const C r = cmul_rn(mk(static_cast<R>(v.x), static_cast<R>(v.y)), mk(cs, sn));
-        ax = add_rn(ax, mul_rn(r.x, w));
-        ay = add_rn(ay, mul_rn(r.y, w));
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int s = sb + i;
+        if (s >= s1) break;
+        if (write_w) W[s] = wv[i];
+        if (!active) continue;
+        if (a.mode == 3) {
+          // accumulate_grid alone: ph_nm holds ph_weight, no ramp and no weight
+          ax = add_rn(ax, static_cast<R>(v[i].x));
+          ay = add_rn(ay, static_cast<R>(v[i].y));
+        } else {
+          const R phs = -(bv[i] * kv[i]);
+          R sn, cs;
+          sincos_r(phs, &sn, &cs);
+          const C r = cmul_rn(mk(static_cast<R>(v[i].x), static_cast<R>(v[i].y)), mk(cs, sn));
+          ax = add_rn(ax, mul_rn(r.x, wv[i]));
+          ay = add_rn(ay, mul_rn(r.y, wv[i]));
+        }
       }
     }
     if (c < a.Mp) grid[cell * a.Mp + c] = active ? mk(ax, ay) : mk(R(0), R(0));
@@ -1158,7 +1182,7 @@ cudaError_t launch_topofit(const TopoArgs& a, bool fp64, int grid_blocks, cudaSt
     k_topofit_f64<<<blocks, 256, sm, st>>>(a);
     return cudaGetLastError();
   }
-  switch (topofit_lanes(a.M)) {
+  switch (a.lanes ? a.lanes : topofit_lanes(a.M)) {
     case 4: return launch_topofit_l<4>(a, grid_blocks, st);
     case 8: return launch_topofit_l<8>(a, grid_blocks, st);
     case 16: return launch_topofit_l<16>(a, grid_blocks, st);

@@ -79,6 +79,7 @@ struct TopoArgs {
   void* ph_res;           // real [N, M]
   void* ph_patch;         // complex [N, M]
   int accumulate_stats;   // 1: rms partials / histogram / invalid count
+  int lanes;              // lanes per PS in the FP32 kernel (4, 8, 16, 32); 0: from n_ifg
 };
 
 // -------------------------------------------------------------- finalize --
@@ -110,6 +111,7 @@ cudaError_t launch_clap(const ClapArgs& a, bool fp64, const Twiddles32f& tf, con
 cudaError_t launch_overlap(const OverlapArgs& a, bool fp64, cudaStream_t st);
 cudaError_t launch_topofit(const TopoArgs& a, bool fp64, int grid_blocks, cudaStream_t st);
 int topofit_grid_blocks(int sm_count, bool fp64);
+int topofit_lanes(int M);
 cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t st);
 cudaError_t launch_loop_continue(cudaGraphConditionalHandle h, const double* stats, cudaStream_t st);
 cudaError_t launch_snr_weight(const TopoArgs& t, const float* amp, void* w_out, bool fp64, int sm_count,

@@ -325,6 +325,13 @@ class Stage2Context:
         self.precision = prec
         self._keep = []
 
+    def autotune(self) -> tuple[int, list[float]]:
+        """Pick the fastest topofit shape (lanes per PS) for this patch."""
+        lanes = ctypes.c_int32(0)
+        ms = (ctypes.c_double * 4)()
+        check(self._lib.ps2_autotune(self._ctx, ctypes.byref(lanes), ms))
+        return int(lanes.value), list(ms)
+
     def reset(self) -> None:
         check(self._lib.ps2_reset(self._ctx))
 
