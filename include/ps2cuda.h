@@ -180,6 +180,42 @@ int ps2_clap_filter_grid_noalloc(const float* d_ph_grid, int64_t n_i, int64_t n_
                                  double alpha, double beta, const double* low_pass, int64_t n_win_ex, float* d_out,
                                  void* stream);
 
+
+/* ---- differentiable coherence (adjoints) ------------------------------------
+ * The gamma map with K given, as a function of the input phases, K and the
+ * CLAP parameters, on the loaded patch's geometry (cells, bperp, low-pass,
+ * CLAP window):
+ *   grid  = sum over each cell of ph * exp(-j K bperp) * w      (the binning)
+ *   filt  = CLAP(grid; alpha, beta) + pyramid overlap-add        (the filter)
+ *   p     = filt[cell] / |filt[cell]|                            (resample)
+ *   coh   = |sum_c conj(p_c) ph_c exp(-j K bperp_c)| / sum_c |conj(p_c) ph_c|
+ * which is the coherence topofit reports for that K (ps_topofit's coh0 at
+ * K0 = K; crates/pystamps-core/src/native_stage2.rs:1257-1303 and the
+ * filter/resample steps :888-1184), without the trial search.
+ * All arrays are device pointers in the caller's row order on the context's
+ * device: d_ph complex64 [n_ps, n_ifg] (interleaved float pairs), d_K, d_w,
+ * d_coh float [n_ps]. Work is queued on `stream` (a cudaStream_t; NULL is
+ * the legacy default stream), after the work already queued on the
+ * context's own stream, and is asynchronous; calls on different streams must
+ * be ordered by the caller. The context's gamma-loop state is untouched.
+ * The arithmetic runs in the context's precision (a patch loaded with
+ * PS2_PRECISION_FP64 gives FP64 forward and adjoint arithmetic on the same
+ * float inputs and outputs). No counterpart in the reference, which has no
+ * gradients. */
+int ps2_coherence_forward(ps2_ctx* ctx, const float* d_ph, const float* d_K, const float* d_w, double clap_alpha,
+                          double clap_beta, float* d_coh, void* stream);
+
+/* Vector-Jacobian product of ps2_coherence_forward: given d_gcoh = dL/dcoh
+ * [n_ps], writes dL/dph (complex64 [n_ps, n_ifg], as dL/dRe + j dL/dIm),
+ * dL/dK [n_ps] and d_galpha_beta[0..1] = dL/dclap_alpha, dL/dclap_beta (a
+ * device double[2]). The forward pass is recomputed; CLAP's window spectra
+ * are recomputed per window, not stored. The median of the smoothed spectrum
+ * passes its gradient to the elements equal to the 512th and 513th order
+ * statistics (half each, split evenly among ties); w is a constant. */
+int ps2_coherence_backward(ps2_ctx* ctx, const float* d_ph, const float* d_K, const float* d_w, double clap_alpha,
+                           double clap_beta, const float* d_gcoh, float* d_gph, float* d_gK, double* d_galpha_beta,
+                           void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -229,6 +229,11 @@ struct ps2_ctx {
   Twiddles32d twd;
   DevBuf ph_nm, bp, amp, perm, cell_start, cell_of, w0, K[2], w, coh, C, nopt, grid, win, filt, low_pass, wscaled,
       taps, lut, nr0, nr_scaled, state, stats, hist, n_invalid, rms_partial, ph_res, scratch, stage;
+  // differentiable coherence (ps2_coherence_forward / _backward): own buffers,
+  // the loop state above is left untouched
+  DevBuf ad_ph, ad_K, ad_w, ad_coh, ad_grid, ad_win, ad_filt, ad_gfilt, ad_gph, ad_gK, ad_gf, ad_part;
+  int ad_blocks = 0, ad_blocks64 = 0;
+  cudaEvent_t ad_ev = nullptr;
   cudaGraph_t loop_graph = nullptr;
   cudaGraphExec_t loop_exec = nullptr;
   bool graph_failed = false;
@@ -530,10 +535,13 @@ void ps2_destroy(ps2_ctx* c) {
   DevBuf* bufs[] = {&c->ph_nm, &c->bp, &c->amp, &c->perm, &c->cell_start, &c->cell_of, &c->w0, &c->K[0], &c->K[1],
                     &c->w, &c->coh, &c->C, &c->nopt, &c->grid, &c->win, &c->filt, &c->low_pass, &c->wscaled,
                     &c->taps, &c->lut, &c->nr0, &c->nr_scaled, &c->state, &c->stats, &c->hist, &c->n_invalid,
-                    &c->rms_partial, &c->ph_res, &c->scratch, &c->stage};
+                    &c->rms_partial, &c->ph_res, &c->scratch, &c->stage, &c->ad_ph, &c->ad_K, &c->ad_w,
+                    &c->ad_coh, &c->ad_grid, &c->ad_win, &c->ad_filt, &c->ad_gfilt, &c->ad_gph, &c->ad_gK,
+                    &c->ad_gf, &c->ad_part};
   for (DevBuf* b : bufs) b->release();
   drop_loop_graph(c);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
+  if (c->ad_ev) cudaEventDestroy(c->ad_ev);
   if (c->h_stats) cudaFreeHost(c->h_stats);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -1319,6 +1327,169 @@ int ps2_clap_filter_grid_noalloc(const float* d_ph_grid, int64_t n_i, int64_t n_
     CK(cudaMemsetAsync(filt, 0, cz * G * Mp, st));
   }
   CK(launch_unpad_grid(filt, d_out, G, static_cast<int>(m), Mp, 8, st));
+  return PS2_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------ differentiable coherence --
+namespace {
+
+int coh_check(ps2_ctx* c, const void* a, const void* b, const void* d, double alpha, double beta, const char* who) {
+  if (!c) return set_err(PS2_ERR_INVALID_ARG, "%s: NULL context", who);
+  if (!c->loaded) return set_err(PS2_ERR_NOT_LOADED, "%s: no patch loaded", who);
+  if (!a || !b || !d) return set_err(PS2_ERR_INVALID_ARG, "%s: a required device array is NULL", who);
+  if (!(alpha > 0.0) || !(beta >= 0.0) || !std::isfinite(alpha) || !std::isfinite(beta))
+    return set_err(PS2_ERR_INVALID_ARG, "%s: need alpha > 0 and beta >= 0 (got %g, %g)", who, alpha, beta);
+  return PS2_OK;
+}
+
+// gathers the caller's rows into cell order (widened to the context's
+// precision) and recomputes grid -> CLAP -> filt
+int coh_prologue(ps2_ctx* c, const float* d_ph, const float* d_K, const float* d_w, double alpha, double beta,
+                 cudaStream_t st, ClapArgs* ca_out) {
+  CK(cudaSetDevice(c->device));
+  // the patch upload and any loop work run on the context's stream: order after them
+  if (!c->ad_ev) CK(cudaEventCreateWithFlags(&c->ad_ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(c->ad_ev, c->st));
+  CK(cudaStreamWaitEvent(st, c->ad_ev, 0));
+  const bool fp64 = c->fp64;
+  const size_t R = rsz(c), Cz = csz(c);
+  const int64_t N = c->N, M = c->M, G = c->G;
+  const int64_t W = std::max<int64_t>(static_cast<int64_t>(c->nwi) * c->nwj, 1);
+  CK(c->ad_ph.alloc(sizeof(float) * 2 * N * M));
+  CK(c->ad_K.alloc(R * N));
+  CK(c->ad_w.alloc(R * N));
+  CK(c->ad_coh.alloc(sizeof(float) * N));
+  CK(c->ad_grid.alloc(Cz * G * c->Mp));
+  CK(c->ad_filt.alloc(Cz * G * c->Mp));
+  CK(c->ad_win.alloc(Cz * W * c->n_win * c->n_win * c->Mp));
+  const int32_t* perm = c->perm.as<int32_t>();
+  CK(launch_gather_rows(d_ph, c->ad_ph.p, perm, N, sizeof(float) * 2 * M, st));
+  if (fp64) {
+    CK(launch_gather_widen(d_K, c->ad_K.as<double>(), perm, N, st));
+    CK(launch_gather_widen(d_w, c->ad_w.as<double>(), perm, N, st));
+  } else {
+    CK(launch_gather_rows(d_K, c->ad_K.p, perm, N, sizeof(float), st));
+    CK(launch_gather_rows(d_w, c->ad_w.p, perm, N, sizeof(float), st));
+  }
+  BinArgs b = bin_args(c, 0, c->ad_K.p);
+  b.ph_nm = c->ad_ph.p;
+  b.w = c->ad_w.p;
+  b.grid = c->ad_grid.p;
+  CK(launch_bin(b, fp64, c->sm_count, st));
+  ClapArgs ca = clap_args(c, c->ad_grid.p, c->ad_win.p);
+  ca.alpha = alpha;
+  ca.beta = beta;
+  ca.alpha_is_one = alpha == 1.0 ? 1 : 0;
+  if (c->nwi > 0 && c->nwj > 0) {
+    CK(launch_clap(ca, fp64, c->twf, c->twd, c->sm_count, st));
+    CK(launch_overlap(overlap_args(c, c->ad_win.p, c->ad_filt.p), fp64, st));
+  } else {
+    CK(cudaMemsetAsync(c->ad_filt.p, 0, Cz * G * c->Mp, st));
+  }
+  *ca_out = ca;
+  c->launches = (c->nwi > 0 && c->nwj > 0) ? 6 : 4;
+  return PS2_OK;
+}
+
+CohArgs coh_args(ps2_ctx* c) {
+  CohArgs a{};
+  a.filt = c->ad_filt.p;
+  a.ph = c->ad_ph.as<float2>();
+  a.K = c->ad_K.p;
+  a.w = c->ad_w.p;
+  a.bp = c->bp.as<float>();
+  a.bp_row_inv = c->bp_row_inv;
+  a.cell_of = c->cell_of.as<int32_t>();
+  a.N = c->N;
+  a.M = c->M;
+  a.Mp = c->Mp;
+  return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ps2_coherence_forward(ps2_ctx* c, const float* d_ph, const float* d_K, const float* d_w, double alpha,
+                          double beta, float* d_coh, void* stream) {
+  int rc = coh_check(c, d_ph, d_K, d_w, alpha, beta, "ps2_coherence_forward");
+  if (rc) return rc;
+  if (!d_coh) return set_err(PS2_ERR_INVALID_ARG, "ps2_coherence_forward: d_coh is NULL");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  ClapArgs ca;
+  rc = coh_prologue(c, d_ph, d_K, d_w, alpha, beta, st, &ca);
+  if (rc) return rc;
+  CohArgs a = coh_args(c);
+  a.coh = c->ad_coh.as<float>();
+  CK(launch_coh(a, 0, c->fp64, c->sm_count, st));
+  CK(launch_scatter_rows(c->ad_coh.p, d_coh, c->perm.as<int32_t>(), c->N, sizeof(float), st));
+  c->launches += 2;
+  return PS2_OK;
+}
+
+int ps2_coherence_backward(ps2_ctx* c, const float* d_ph, const float* d_K, const float* d_w, double alpha,
+                           double beta, const float* d_gcoh, float* d_gph, float* d_gK, double* d_galpha_beta,
+                           void* stream) {
+  int rc = coh_check(c, d_ph, d_K, d_w, alpha, beta, "ps2_coherence_backward");
+  if (rc) return rc;
+  if (!d_gcoh || !d_gph || !d_gK || !d_galpha_beta)
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_coherence_backward: a gradient array is NULL");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  ClapArgs ca;
+  rc = coh_prologue(c, d_ph, d_K, d_w, alpha, beta, st, &ca);
+  if (rc) return rc;
+  const bool fp64 = c->fp64;
+  const size_t R = rsz(c), Cz = csz(c);
+  const int64_t N = c->N, M = c->M, G = c->G;
+  int& cap = fp64 ? c->ad_blocks64 : c->ad_blocks;
+  if (cap == 0) {
+    cap = clap_bwd_max_blocks(c->sm_count, fp64);
+    if (cap <= 0) return set_err(PS2_ERR_CUDA, "ps2_coherence_backward: occupancy query failed");
+  }
+  CK(c->ad_gfilt.alloc(Cz * G * c->Mp));
+  CK(c->ad_gph.alloc(Cz * N * M));
+  CK(c->ad_gf.alloc(Cz * N * M));
+  CK(c->ad_gK.alloc(R * N));
+  CK(c->ad_part.alloc(sizeof(double) * 2 * cap));
+  const int32_t* perm = c->perm.as<int32_t>();
+  // the incoming gradient is in the caller's row order
+  CK(launch_gather_rows(d_gcoh, c->ad_coh.p, perm, N, sizeof(float), st));
+  CohArgs a = coh_args(c);
+  a.gcoh = c->ad_coh.as<float>();
+  a.gph = c->ad_gph.p;
+  a.gK = c->ad_gK.p;
+  a.gf = c->ad_gf.p;
+  CK(launch_coh(a, 1, fp64, c->sm_count, st));
+  // sum of d L / d filt over each cell's PS = d L / d (CLAP output)
+  CK(launch_cell_sum(a, c->cell_start.as<int32_t>(), G, c->ad_gfilt.p, fp64, c->sm_count, st));
+  int launched = 0;
+  if (c->nwi > 0 && c->nwj > 0) {
+    ClapBwdArgs cb{};
+    cb.f = ca;
+    cb.gfilt = c->ad_gfilt.p;
+    cb.wgrad = c->ad_win.p;
+    cb.ab_partial = c->ad_part.as<double>();
+    launched = cap;
+    CK(launch_clap_bwd(cb, fp64, c->twf, c->twd, &launched, st));
+    // window-input gradients back onto the grid: the overlap gather is the
+    // adjoint of the window extraction
+    CK(launch_overlap(overlap_args(c, c->ad_win.p, c->ad_filt.p), fp64, st));
+  } else {
+    CK(cudaMemsetAsync(c->ad_filt.p, 0, Cz * G * c->Mp, st));
+  }
+  CK(launch_reduce_ab(c->ad_part.as<double>(), launched, d_galpha_beta, st));
+  a.ggrid = c->ad_filt.p;
+  CK(launch_coh(a, 2, fp64, c->sm_count, st));
+  if (fp64) {
+    CK(launch_scatter_narrow(c->ad_gph.as<double>(), d_gph, perm, N, 2 * M, st));
+    CK(launch_scatter_narrow(c->ad_gK.as<double>(), d_gK, perm, N, 1, st));
+  } else {
+    CK(launch_scatter_rows(c->ad_gph.p, d_gph, perm, N, sizeof(float) * 2 * M, st));
+    CK(launch_scatter_rows(c->ad_gK.p, d_gK, perm, N, sizeof(float), st));
+  }
+  c->launches += 7 + (launched > 0 ? 2 : 0);
   return PS2_OK;
 }
 

@@ -271,6 +271,45 @@ __device__ __forceinline__ R warp_median1024(const R (&o)[32]) {
   return (v0 + v1) * R(0.5);
 }
 
+template <typename R>
+__device__ __forceinline__ R warp_median1024_pair(const R (&o)[32], R& v0_out, R& v1_out) {
+  using U = typename CT<R>::U;
+  U lo = to_bits(o[0]), hi = lo;
+#pragma unroll
+  for (int i = 1; i < 32; ++i) {
+    const U u = to_bits(o[i]);
+    lo = min(lo, u);
+    hi = max(hi, u);
+  }
+  lo = warp_min_u(lo);
+  hi = warp_max_u(hi);
+  const int kth = 511;
+  while (lo < hi) {
+    const U mid = lo + ((hi - lo) >> 1);
+    int cnt = 0;
+#pragma unroll
+    for (int i = 0; i < 32; ++i) cnt += (to_bits(o[i]) <= mid) ? 1 : 0;
+    cnt = warp_sum(cnt);
+    if (cnt >= kth + 1)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  int cle = 0;
+  U nxt = ~U(0);
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    const U u = to_bits(o[i]);
+    cle += (u <= lo) ? 1 : 0;
+    if (u > lo) nxt = min(nxt, u);
+  }
+  cle = warp_sum(cle);
+  nxt = warp_min_u(nxt);
+  v0_out = from_bits(lo);
+  v1_out = (cle >= kth + 2) ? v0_out : from_bits(nxt);
+  return (v0_out + v1_out) * R(0.5);
+}
+
 // One 32-point FFT per lane over a row (rows = true, lane = row) or a column
 // (lane = column) of the tile, in place. Not inlined: the window code calls it
 // four times and one copy keeps the kernel inside the instruction cache.
@@ -1459,6 +1498,547 @@ cudaError_t launch_random_hist(const double* rnd, int64_t n_rand, const double* 
   if (blocks < 1) blocks = 1;
   k_random_hist<<<static_cast<unsigned>(blocks), 256, sm, st>>>(rnd, n_rand, bp, m, ia, ib, small_baseline, n_half,
                                                                 cutoff0, dbin, hist);
+  return cudaGetLastError();
+}
+
+
+// ============================================================== adjoints ==
+// Differentiable stage-2 coherence with K given (no trial search):
+//   grid  = bin(ph e^{-j K bp} w)              (k_bin, mode 0)
+//   filt  = CLAP(grid; alpha, beta)            (k_clap + k_overlap)
+//   p     = filt[cell] / |filt[cell]|          (resample + normalise)
+//   gamma = |sum_c conj(p_c) ph_c e^{-j K bp_c}| / sum_c |conj(p_c) ph_c|
+// Gradients use the complex convention g = dL/dRe + j dL/dIm. CLAP's window
+// spectra are recomputed in the backward pass, not stored. R is the working
+// precision (the context's): inputs arrive as float and are widened.
+
+template <typename R>
+__device__ __forceinline__ typename CT<R>::C unit_or_zero(const typename CT<R>::C f, R* mag) {
+  const R m = hypot_r(f.x, f.y);
+  *mag = m;
+  return m != R(0) ? mk(f.x / m, f.y / m) : mk(R(0), R(0));
+}
+
+template <typename R>
+__device__ __forceinline__ R row_bp(const CohArgs& a, int64_t s, int c) {
+  return a.bp_row_inv ? static_cast<R>(a.bp[c]) : static_cast<R>(a.bp[s * a.M + c]);
+}
+
+template <typename R>
+__device__ __forceinline__ typename CT<R>::C load_ph(const CohArgs& a, int64_t s, int c) {
+  const float2 v = a.ph[s * a.M + c];
+  return mk(static_cast<R>(v.x), static_cast<R>(v.y));
+}
+
+// S = sum_c conj(p_c) ph_c e^{-j K bp_c} and D = sum_c |conj(p_c) ph_c| of one PS (whole warp)
+template <typename R>
+__device__ __forceinline__ void coh_sums(const CohArgs& a, int64_t s, int lane, R* sx_o, R* sy_o, R* d_o) {
+  using C = typename CT<R>::C;
+  const C* __restrict__ filt = static_cast<const C*>(a.filt);
+  const int64_t cell = a.cell_of[s];
+  const R k = static_cast<const R*>(a.K)[s];
+  R sx = R(0), sy = R(0), d = R(0);
+  for (int c = lane; c < a.M; c += 32) {
+    R mag;
+    const C pp = unit_or_zero<R>(filt[cell * a.Mp + c], &mag);
+    const C z = cmul(mk(pp.x, -pp.y), load_ph<R>(a, s, c));
+    R sn, cs;
+    sincos_r(k * row_bp<R>(a, s, c), &sn, &cs);
+    const C r = cmul(z, mk(cs, -sn));
+    sx += r.x;
+    sy += r.y;
+    d += hypot_r(z.x, z.y);
+  }
+  *sx_o = warp_sum(sx);
+  *sy_o = warp_sum(sy);
+  *d_o = warp_sum(d);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_coh_fwd(CohArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t s = gw; s < a.N; s += nw) {
+    R sx, sy, d;
+    coh_sums<R>(a, s, lane, &sx, &sy, &d);
+    if (lane == 0) a.coh[s] = static_cast<float>(hypot_r(sx, sy) / (d != R(0) ? d : R(1)));
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_coh_bwd(CohArgs a) {
+  using C = typename CT<R>::C;
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  const C* __restrict__ filt = static_cast<const C*>(a.filt);
+  C* __restrict__ gph = static_cast<C*>(a.gph);
+  C* __restrict__ gf_out = static_cast<C*>(a.gf);
+  for (int64_t s = gw; s < a.N; s += nw) {
+    R sx, sy, d;
+    coh_sums<R>(a, s, lane, &sx, &sy, &d);
+    const int64_t cell = a.cell_of[s];
+    const R k = static_cast<const R*>(a.K)[s];
+    const R dd = d != R(0) ? d : R(1);
+    const R sm = hypot_r(sx, sy);
+    const R g = static_cast<R>(a.gcoh[s]);
+    const R gam = sm / dd;
+    // d gamma / d S = S / (|S| D); d gamma / d |z_c| = -gamma / D
+    const C gS = sm > R(0) ? mk(g * sx / (sm * dd), g * sy / (sm * dd)) : mk(R(0), R(0));
+    const R gD = -g * gam / dd;
+    R gk = R(0);
+    for (int c = lane; c < a.M; c += 32) {
+      R mag;
+      const C pp = unit_or_zero<R>(filt[cell * a.Mp + c], &mag);
+      const C h = load_ph<R>(a, s, c);
+      const C z = cmul(mk(pp.x, -pp.y), h);
+      const R b = row_bp<R>(a, s, c);
+      R sn, cs;
+      sincos_r(k * b, &sn, &cs);
+      const C e = mk(cs, -sn);
+      const C r = cmul(z, e);
+      // r = z e:  g_z = conj(e) g_S (+ the denominator term);  dr/dK = -j bp r
+      C gz = cmul(mk(e.x, -e.y), gS);
+      const R zm = hypot_r(z.x, z.y);
+      if (zm > R(0)) {
+        gz.x += gD * z.x / zm;
+        gz.y += gD * z.y / zm;
+      }
+      gk += gS.x * (b * r.y) + gS.y * (-b * r.x);
+      // z = conj(p) h:  g_h = p g_z,  g_p = conj(g_z) h
+      gph[s * a.M + c] = cmul(pp, gz);
+      const C gp = cmul(mk(gz.x, -gz.y), h);
+      // p = f / |f|:  g_f = (g_p - p Re(conj(p) g_p)) / |f|
+      C gf = mk(R(0), R(0));
+      if (mag > R(0)) {
+        const R rp = pp.x * gp.x + pp.y * gp.y;
+        gf = mk((gp.x - pp.x * rp) / mag, (gp.y - pp.y * rp) / mag);
+      }
+      gf_out[s * a.M + c] = gf;
+    }
+    gk = warp_sum(gk);
+    if (lane == 0) static_cast<R*>(a.gK)[s] = gk;
+  }
+}
+
+// bin backward: grid[cell, c] += a ph with a = e^{-j K bp} w
+template <typename R>
+__global__ void __launch_bounds__(256) k_bin_bwd(CohArgs a) {
+  using C = typename CT<R>::C;
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  const C* __restrict__ ggrid = static_cast<const C*>(a.ggrid);
+  C* __restrict__ gph = static_cast<C*>(a.gph);
+  for (int64_t s = gw; s < a.N; s += nw) {
+    const int64_t cell = a.cell_of[s];
+    const R k = static_cast<const R*>(a.K)[s], w = static_cast<const R*>(a.w)[s];
+    R gk = R(0);
+    for (int c = lane; c < a.M; c += 32) {
+      const R b = row_bp<R>(a, s, c);
+      R sn, cs;
+      sincos_r(-(b * k), &sn, &cs);
+      const C co = mk(cs * w, sn * w);
+      const C gg = ggrid[cell * a.Mp + c];
+      const C gh = cmul(mk(co.x, -co.y), gg);
+      const C prev = gph[s * a.M + c];
+      gph[s * a.M + c] = mk(prev.x + gh.x, prev.y + gh.y);
+      const C v = cmul(co, load_ph<R>(a, s, c));  // d(a h)/dK = -j bp a h
+      gk += gg.x * (b * v.y) + gg.y * (-b * v.x);
+    }
+    gk = warp_sum(gk);
+    if (lane == 0) static_cast<R*>(a.gK)[s] += gk;
+  }
+}
+
+// per-cell sum of complex rows [N, M] in cell order (rows of one cell are
+// contiguous), sequential in row order: d L / d filt from d L / d p_c
+template <typename R>
+__global__ void __launch_bounds__(256) k_cell_sum(CohArgs a, const int32_t* __restrict__ cell_start, int64_t G,
+                                                  int nchunk, void* out_v) {
+  using C = typename CT<R>::C;
+  const C* __restrict__ src = static_cast<const C*>(a.gf);
+  C* __restrict__ out = static_cast<C*>(out_v);
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t task = gw; task < G * nchunk; task += nw) {
+    const int64_t cell = task / nchunk;
+    const int c = static_cast<int>(task - cell * nchunk) * 32 + lane;
+    R ax = R(0), ay = R(0);
+    if (c < a.M) {
+      for (int s = cell_start[cell]; s < cell_start[cell + 1]; ++s) {
+        const C v = src[static_cast<int64_t>(s) * a.M + c];
+        ax += v.x;
+        ay += v.y;
+      }
+    }
+    if (c < a.Mp) out[cell * a.Mp + c] = mk(ax, ay);
+  }
+}
+
+template <typename R>
+static cudaError_t coh_launch(const CohArgs& a, int which, int sm_count, cudaStream_t st) {
+  int64_t blocks = (a.N + 7) / 8;
+  if (blocks > static_cast<int64_t>(sm_count) * 16) blocks = static_cast<int64_t>(sm_count) * 16;
+  if (blocks < 1) blocks = 1;
+  if (which == 0)
+    k_coh_fwd<R><<<static_cast<unsigned>(blocks), 256, 0, st>>>(a);
+  else if (which == 1)
+    k_coh_bwd<R><<<static_cast<unsigned>(blocks), 256, 0, st>>>(a);
+  else
+    k_bin_bwd<R><<<static_cast<unsigned>(blocks), 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_coh(const CohArgs& a, int which, bool fp64, int sm_count, cudaStream_t st) {
+  return fp64 ? coh_launch<double>(a, which, sm_count, st) : coh_launch<float>(a, which, sm_count, st);
+}
+
+cudaError_t launch_cell_sum(const CohArgs& a, const int32_t* cell_start, int64_t G, void* out, bool fp64,
+                            int sm_count, cudaStream_t st) {
+  const int nchunk = (a.M + 31) / 32;
+  int64_t blocks = (G * nchunk + 7) / 8;
+  if (blocks > static_cast<int64_t>(sm_count) * 16) blocks = static_cast<int64_t>(sm_count) * 16;
+  if (blocks < 1) blocks = 1;
+  if (fp64)
+    k_cell_sum<double><<<static_cast<unsigned>(blocks), 256, 0, st>>>(a, cell_start, G, nchunk, out);
+  else
+    k_cell_sum<float><<<static_cast<unsigned>(blocks), 256, 0, st>>>(a, cell_start, G, nchunk, out);
+  return cudaGetLastError();
+}
+
+template <typename R>
+struct ClapBwdTile {
+  R re[32][33];
+  R im[32][33];
+  R hs[32][33];
+  R gre[32][33];
+  R gim[32][33];
+  R pad[8];
+};
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_clap_bwd(ClapBwdArgs b, typename CT<R>::Tw tw) {
+  using C = typename CT<R>::C;
+  const ClapArgs& a = b.f;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ClapBwdTile<R>* tiles = reinterpret_cast<ClapBwdTile<R>*>(smem_raw);
+  R* lp = reinterpret_cast<R*>(tiles + 4);
+  R* wt = lp + 1024;
+  C* twf = reinterpret_cast<C*>(wt + 1024);
+  C* twi = twf + 16;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nw = a.n_win, nw2 = nw * nw;
+  for (int i = tid; i < 1024; i += 128) lp[i] = static_cast<R>(a.low_pass[i]);
+  for (int i = tid; i < nw2; i += 128) wt[i] = static_cast<R>(a.wscaled[i]);
+  if (tid < 16) {
+    twf[tid] = tw.w[tid];
+    twi[tid] = mk(tw.w[tid].x, -tw.w[tid].y);
+  }
+  R g7[7];
+#pragma unroll
+  for (int i = 0; i < 7; ++i) g7[i] = static_cast<R>(a.g7[i]);
+  const int n_inc = nw / 4 > 1 ? nw / 4 : 1;
+  const int ngroups = a.Mp / 4;
+  const int64_t ntask = static_cast<int64_t>(a.nwi) * a.nwj * ngroups;
+  const C* __restrict__ grid = static_cast<const C*>(a.grid);
+  const C* __restrict__ gfilt = static_cast<const C*>(b.gfilt);
+  C* __restrict__ wgrad = static_cast<C*>(b.wgrad);
+  ClapBwdTile<R>& T = tiles[warp];
+  const R alpha = static_cast<R>(a.alpha), beta = static_cast<R>(a.beta);
+  double ga_acc = 0.0, gb_acc = 0.0;
+  for (int64_t task = blockIdx.x; task < ntask; task += gridDim.x) {
+    const int64_t wi = task / ngroups;
+    const int g = static_cast<int>(task - wi * ngroups);
+    const int ix1 = static_cast<int>(wi / a.nwj), ix2 = static_cast<int>(wi - static_cast<int64_t>(ix1) * a.nwj);
+    int i1 = ix1 * n_inc, rs = 0;
+    if (i1 + nw > a.n_i) {
+      rs = i1 + nw - a.n_i;
+      i1 = a.n_i - nw;
+    }
+    int j1 = ix2 * n_inc, cs = 0;
+    if (j1 + nw > a.n_j) {
+      cs = j1 + nw - a.n_j;
+      j1 = a.n_j - nw;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < 4 * 32 * 32; idx += 128) {
+      const int q = idx >> 10, e = idx & 1023, r = e >> 5, cc = e & 31;
+      if (r >= nw || cc >= nw) {
+        tiles[q].re[r][cc] = R(0);
+        tiles[q].im[r][cc] = R(0);
+        tiles[q].gre[r][cc] = R(0);
+        tiles[q].gim[r][cc] = R(0);
+      }
+    }
+    for (int idx = tid; idx < nw2 * 4; idx += 128) {
+      const int pix = idx >> 2, q = idx & 3;
+      const int li = pix / nw, lj = pix - li * nw;
+      const int c = 4 * g + q;
+      C v = mk(R(0), R(0)), gy = mk(R(0), R(0));
+      if (c < a.M) {
+        const int64_t cell = static_cast<int64_t>(i1 + li) * a.n_j + (j1 + lj);
+        v = grid[cell * a.Mp + c];
+        if (isnan(v.x) || isnan(v.y)) v = mk(R(0), R(0));
+        const R wv = (li < rs || lj < cs) ? R(0) : wt[(li - rs) * nw + (lj - cs)];
+        const C go = gfilt[cell * a.Mp + c];
+        gy = mk(go.x * wv, go.y * wv);  // out += w y  =>  g_y = w g_out
+      }
+      tiles[q].re[li][lj] = v.x;
+      tiles[q].im[li][lj] = v.y;
+      tiles[q].gre[li][lj] = gy.x;
+      tiles[q].gim[li][lj] = gy.y;
+    }
+    __syncthreads();
+    if (4 * g + warp < a.M) {
+      // recompute the forward spectrum X = FFT2(x) and the smoothed magnitude
+      if (lane < nw) fft_pass<R>(T.re, T.im, twf, lane, true);
+      __syncwarp();
+      fft_pass<R>(T.re, T.im, twf, lane, false);
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        const R xr = T.re[k][lane], xi = T.im[k][lane];
+        T.hs[k][lane] = sqrt(xr * xr + xi * xi);
+      }
+      __syncwarp();
+      R t[32];
+      const int sj = (lane + 16) & 31;
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        R acc = R(0);
+#pragma unroll
+        for (int d = -3; d <= 3; ++d)
+          if (sj + d >= 0 && sj + d < 32) acc += T.hs[k][(lane + d) & 31] * g7[d + 3];
+        t[k] = acc;
+      }
+      R o[32];
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        const int sk = (k + 16) & 31;
+        R acc = R(0);
+#pragma unroll
+        for (int d = -3; d <= 3; ++d)
+          if (sk + d >= 0 && sk + d < 32) acc += t[(k + d) & 31] * g7[d + 3];
+        o[k] = acc;
+      }
+      R v0, v1;
+      const R med = warp_median1024_pair<R>(o, v0, v1);
+      // g_Y = FFT2(g_y) (adjoint of the unnormalised inverse FFT)
+      if (lane < nw) fft_pass<R>(T.gre, T.gim, twf, lane, true);
+      __syncwarp();
+      fft_pass<R>(T.gre, T.gim, twf, lane, false);
+      const R inv_med = med != R(0) ? R(1) / med : R(1);
+      R gmed = R(0), ga = R(0), gb = R(0);
+      // t becomes dL/d(smoothed |X|), starting with the direct term
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        const R xr = T.re[k][lane], xi = T.im[k][lane];
+        const R gyr = T.gre[k][lane], gyi = T.gim[k][lane];
+        const R hn = o[k] * inv_med;
+        const R pw = a.alpha_is_one ? hn : pow(hn, alpha);
+        const bool act = pw - R(1) > R(0);
+        const R G = (act ? pw - R(1) : R(0)) * beta + lp[k * 32 + lane];
+        const R gG = xr * gyr + xi * gyi;
+        R ghn = R(0);
+        if (act) {
+          ghn = gG * beta * (a.alpha_is_one ? R(1) : alpha * pow(hn, alpha - R(1)));
+          gb += gG * (pw - R(1));
+          ga += gG * beta * pw * log(hn);
+        }
+        if (med != R(0)) gmed += ghn * (-o[k] * inv_med * inv_med);
+        t[k] = med != R(0) ? ghn * inv_med : ghn;
+        T.gre[k][lane] = gyr * G;  // g_X from Y = X G
+        T.gim[k][lane] = gyi * G;
+      }
+      gmed = warp_sum(gmed);
+      ga = warp_sum(ga);
+      gb = warp_sum(gb);
+      if (med != R(0)) {
+        // med = (v0 + v1) / 2 of the smoothed magnitudes; ties share evenly
+        int c0 = 0, c1 = 0;
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+          c0 += o[k] == v0 ? 1 : 0;
+          c1 += o[k] == v1 ? 1 : 0;
+        }
+        c0 = warp_sum(c0);
+        c1 = warp_sum(c1);
+        const R share0 = v0 == v1 ? gmed / static_cast<R>(c0) : R(0.5) * gmed / static_cast<R>(c0);
+        const R share1 = v0 == v1 ? R(0) : R(0.5) * gmed / static_cast<R>(c1);
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+          if (o[k] == v0)
+            t[k] += share0;
+          else if (o[k] == v1)
+            t[k] += share1;
+        }
+      }
+      // adjoint of the separable smoothing: along k in registers, then across lanes
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        const int sk = (k + 16) & 31;
+        R acc = R(0);
+#pragma unroll
+        for (int d = -3; d <= 3; ++d)
+          if (sk + d >= 0 && sk + d < 32) acc += t[(k + d) & 31] * g7[d + 3];
+        o[k] = acc;
+      }
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < 32; ++k) T.hs[k][lane] = o[k];
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        R acc = R(0);
+#pragma unroll
+        for (int d = -3; d <= 3; ++d)
+          if (sj + d >= 0 && sj + d < 32) acc += T.hs[k][(lane + d) & 31] * g7[d + 3];
+        // H = |X|:  g_X += g_H X / |X|
+        const R xr = T.re[k][lane], xi = T.im[k][lane];
+        const R xm = sqrt(xr * xr + xi * xi);
+        if (xm > R(0)) {
+          T.gre[k][lane] += acc * xr / xm;
+          T.gim[k][lane] += acc * xi / xm;
+        }
+      }
+      // g_x = IFFT2_unnormalised(g_X) (adjoint of the forward FFT)
+      __syncwarp();
+      fft_pass<R>(T.gre, T.gim, twi, lane, false);
+      __syncwarp();
+      if (lane < nw) fft_pass<R>(T.gre, T.gim, twi, lane, true);
+      __syncwarp();
+      if (lane == 0) {
+        ga_acc += static_cast<double>(ga);
+        gb_acc += static_cast<double>(gb);
+      }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < nw2 * 4; idx += 128) {
+      const int pix = idx >> 2, q = idx & 3;
+      const int li = pix / nw, lj = pix - li * nw;
+      const int c = 4 * g + q;
+      C v = mk(tiles[q].gre[li][lj], tiles[q].gim[li][lj]);
+      if (c < a.M) {
+        const C x = grid[(static_cast<int64_t>(i1 + li) * a.n_j + (j1 + lj)) * a.Mp + c];
+        if (isnan(x.x) || isnan(x.y)) v = mk(R(0), R(0));  // NaN inputs enter as constants
+      } else {
+        v = mk(R(0), R(0));
+      }
+      wgrad[(wi * nw2 + pix) * a.Mp + 4 * g + q] = v;
+    }
+  }
+  __shared__ double sh_ab[8];
+  if (lane == 0) {
+    sh_ab[2 * warp] = ga_acc;
+    sh_ab[2 * warp + 1] = gb_acc;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    b.ab_partial[2 * blockIdx.x] = sh_ab[0] + sh_ab[2] + sh_ab[4] + sh_ab[6];
+    b.ab_partial[2 * blockIdx.x + 1] = sh_ab[1] + sh_ab[3] + sh_ab[5] + sh_ab[7];
+  }
+}
+
+// d L / d alpha and d L / d beta: the per-block partials summed in a fixed order
+__global__ void __launch_bounds__(256) k_reduce_ab(const double* __restrict__ part, int n, double* __restrict__ out) {
+  __shared__ double sh[2][256];
+  const int t = threadIdx.x;
+  double a = 0.0, b = 0.0;
+  for (int i = t; i < n; i += 256) {
+    a += part[2 * i];
+    b += part[2 * i + 1];
+  }
+  sh[0][t] = a;
+  sh[1][t] = b;
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if (t < h) {
+      sh[0][t] += sh[0][t + h];
+      sh[1][t] += sh[1][t + h];
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    out[0] = sh[0][0];
+    out[1] = sh[1][0];
+  }
+}
+
+cudaError_t launch_reduce_ab(const double* part, int n, double* out, cudaStream_t st) {
+  k_reduce_ab<<<1, 256, 0, st>>>(part, n, out);
+  return cudaGetLastError();
+}
+
+template <typename R>
+static size_t clap_bwd_smem() {
+  return 4 * sizeof(ClapBwdTile<R>) + 2048 * sizeof(R) + 32 * sizeof(typename CT<R>::C);
+}
+
+template <typename R>
+static int clap_bwd_blocks(int sm_count) {
+  const size_t sm = clap_bwd_smem<R>();
+  if (cudaFuncSetAttribute(k_clap_bwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+    return 0;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clap_bwd<R>, 128, sm) != cudaSuccess) return 0;
+  return sm_count * std::max(per_sm, 1);
+}
+
+// Resident blocks of k_clap_bwd on the whole device (the size of the
+// alpha/beta partial array); 0 on error.
+int clap_bwd_max_blocks(int sm_count, bool fp64) {
+  return fp64 ? clap_bwd_blocks<double>(sm_count) : clap_bwd_blocks<float>(sm_count);
+}
+
+// Launches at most *blocks_out blocks (the partial array's capacity) and
+// returns the number launched (0 when there are no windows).
+cudaError_t launch_clap_bwd(const ClapBwdArgs& b, bool fp64, const Twiddles32f& tf, const Twiddles32d& td,
+                            int* blocks_out, cudaStream_t st) {
+  const int64_t ntask = static_cast<int64_t>(b.f.nwi) * b.f.nwj * (b.f.Mp / 4);
+  const int64_t blocks = std::min<int64_t>(ntask, static_cast<int64_t>(*blocks_out));
+  *blocks_out = static_cast<int>(std::max<int64_t>(blocks, 0));
+  if (blocks <= 0) return cudaSuccess;
+  if (fp64)
+    k_clap_bwd<double><<<static_cast<unsigned>(blocks), 128, clap_bwd_smem<double>(), st>>>(b, td);
+  else
+    k_clap_bwd<float><<<static_cast<unsigned>(blocks), 128, clap_bwd_smem<float>(), st>>>(b, tf);
+  return cudaGetLastError();
+}
+
+// dst[s] = double(src[perm[s]])
+__global__ void k_gather_widen(const float* __restrict__ src, double* __restrict__ dst,
+                               const int32_t* __restrict__ perm, int64_t n) {
+  for (int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; s < n;
+       s += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    dst[s] = static_cast<double>(src[perm[s]]);
+}
+
+// dst[perm[s] * words + k] = float(src[s * words + k])
+__global__ void k_scatter_narrow(const double* __restrict__ src, float* __restrict__ dst,
+                                 const int32_t* __restrict__ perm, int64_t n, int64_t words) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t s = gw; s < n; s += nw) {
+    const int64_t r = perm[s];
+    for (int64_t k = lane; k < words; k += 32) dst[r * words + k] = static_cast<float>(src[s * words + k]);
+  }
+}
+
+cudaError_t launch_gather_widen(const float* src, double* dst, const int32_t* perm, int64_t n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int64_t blocks = std::min<int64_t>((n + 255) / 256, 148 * 16);
+  k_gather_widen<<<static_cast<unsigned>(blocks), 256, 0, st>>>(src, dst, perm, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_narrow(const double* src, float* dst, const int32_t* perm, int64_t n, int64_t words,
+                                  cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int64_t blocks = std::min<int64_t>((n + 7) / 8, 148 * 16);
+  k_scatter_narrow<<<static_cast<unsigned>(blocks), 256, 0, st>>>(src, dst, perm, n, words);
   return cudaGetLastError();
 }
 

@@ -104,6 +104,33 @@ struct FinalizeArgs {
   int force_continue;        // iterate past the stop rule (timing runs)
 };
 
+// -------------------------------------------------------------- adjoints --
+// R-typed arrays are float or double by the context's precision.
+struct CohArgs {
+  const void* filt;       // complex R [G, Mp]
+  const float2* ph;       // [N, M] sorted (the caller's phases)
+  const void* K;          // R [N] sorted
+  const void* w;          // R [N] sorted (bin backward)
+  const float* bp;        // [N, M] sorted or [M]
+  int bp_row_inv;
+  const int32_t* cell_of; // [N]
+  int64_t N;
+  int M, Mp;
+  float* coh;             // forward out [N]
+  const float* gcoh;      // backward in [N]
+  void* gph;              // backward out: complex R [N, M]
+  void* gK;               // backward out: R [N]
+  void* gf;               // backward out: d L / d filt per (PS, ifg), complex R [N, M]
+  const void* ggrid;      // bin backward in: complex R [G, Mp]
+};
+
+struct ClapBwdArgs {
+  ClapArgs f;           // the forward call's arguments (grid = its input)
+  const void* gfilt;    // complex R [G, Mp]: d L / d CLAP output
+  void* wgrad;          // complex R [W, n_win^2, Mp]: d L / d window input
+  double* ab_partial;   // [2 * blocks]: d L / d alpha, d L / d beta per block
+};
+
 // ---------------------------------------------------------- launchers -----
 cudaError_t launch_bin(const BinArgs& a, bool fp64, int sm_count, cudaStream_t st);
 cudaError_t launch_clap(const ClapArgs& a, bool fp64, const Twiddles32f& tf, const Twiddles32d& td, int sm_count,
@@ -114,6 +141,17 @@ int topofit_grid_blocks(int sm_count, bool fp64);
 int topofit_lanes(int M);
 cudaError_t launch_finalize(const FinalizeArgs& a, cudaStream_t st);
 cudaError_t launch_loop_continue(cudaGraphConditionalHandle h, const double* stats, cudaStream_t st);
+cudaError_t launch_coh(const CohArgs& a, int which /*0 fwd, 1 coherence bwd, 2 bin bwd*/, bool fp64,
+                       int sm_count, cudaStream_t st);
+cudaError_t launch_cell_sum(const CohArgs& a, const int32_t* cell_start, int64_t G, void* out, bool fp64,
+                            int sm_count, cudaStream_t st);
+cudaError_t launch_clap_bwd(const ClapBwdArgs& b, bool fp64, const Twiddles32f& tf, const Twiddles32d& td,
+                            int* blocks_out, cudaStream_t st);
+int clap_bwd_max_blocks(int sm_count, bool fp64);
+cudaError_t launch_gather_widen(const float* src, double* dst, const int32_t* perm, int64_t n, cudaStream_t st);
+cudaError_t launch_scatter_narrow(const double* src, float* dst, const int32_t* perm, int64_t n, int64_t words,
+                                  cudaStream_t st);
+cudaError_t launch_reduce_ab(const double* part, int n, double* out, cudaStream_t st);
 cudaError_t launch_snr_weight(const TopoArgs& t, const float* amp, void* w_out, bool fp64, int sm_count,
                               cudaStream_t st);
 cudaError_t launch_random_hist(const double* rnd, int64_t n_rand, const double* bp, int m, const int64_t* ia,

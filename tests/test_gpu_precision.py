@@ -1,14 +1,37 @@
 """FP32 path against the plain FP64 GPU path on the 250k-PS x 60-ifg x 128^2
 precision-study shape, first gamma iteration (both paths start from the same
 state): max |d gamma| <= 1e-4 and max |d K| <= 1e-3 m of DEM error for every
-PS whose topofit peak is not an argmax tie (best and runner-up trial
-coherence within 1e-6 relative); ties are counted and reported."""
+PS that is not a tie. Two kinds of tie are counted and reported, not held to
+the tolerance:
+  argmax ties: best and runner-up trial coherence within 1e-6 relative;
+  wrap ties: a refinement residual angle arg(res * conj(offset))
+  (native_stage2.rs:1259-1303) within 1e-4 rad of +-pi, where arg() jumps by
+  2 pi and the FP32 and FP64 filtered phases (which differ by up to ~6e-5 rad)
+  can land on different sides.
+"""
 import math
 
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
+
+ARGMAX_TIE_REL = 1e-6
+WRAP_TIE_RAD = 1e-4
+
+
+def wrap_distance(ph_nm, ph_patch, bperp, best_ix, n_trial_wraps, trials):
+    """min over interferograms of pi - |arg(res * conj(offset))| at the
+    winning trial, per PS (FP64)."""
+    z = ph_nm.astype(np.complex128) * np.conj(ph_patch.astype(np.complex128))
+    bp = np.broadcast_to(bperp, z.shape).astype(np.float64)
+    rng = bp.max(axis=1) - bp.min(axis=1)
+    rng[rng == 0] = 1.0
+    k0 = (math.pi / 4) / rng * trials[best_ix]
+    res = z * np.exp(-1j * k0[:, None] * bp)
+    off = res.sum(axis=1)
+    ang = np.angle(res * np.conj(off)[:, None])
+    return (math.pi - np.abs(ang)).min(axis=1)
 
 
 def test_fp32_vs_fp64_first_iteration_precision_size(cuda_lib, oracle):
@@ -23,15 +46,22 @@ def test_fp32_vs_fp64_first_iteration_precision_size(cuda_lib, oracle):
         c64.load(prep, "fp64")
         c32.iterate(1)
         c64.iterate(1)
-        a = c32.download(["coh_ps", "K_ps"])
+        a = c32.download(["coh_ps", "K_ps", "ph_patch"])
         b = c64.download(["coh_ps", "K_ps", "ph_patch"])
-    fr = oracle.fit_rows(b["ph_patch"].astype(np.complex64), prep.ph_nm, prep.bperp.astype(np.float64),
-                         prep.n_trial_wraps)
-    tie = (fr.best_coh - fr.second_coh) <= 1e-6 * np.maximum(fr.best_coh, 1e-30)
+    bp = prep.bperp.astype(np.float64)
+    fr = oracle.fit_rows(b["ph_patch"].astype(np.complex64), prep.ph_nm, bp, prep.n_trial_wraps)
+    argmax_tie = (fr.best_coh - fr.second_coh) <= ARGMAX_TIE_REL * np.maximum(fr.best_coh, 1e-30)
+    wd = wrap_distance(prep.ph_nm, b["ph_patch"], bp, fr.best_ix, prep.n_trial_wraps,
+                       oracle.trial_values(prep.n_trial_wraps))
+    wrap_tie = wd < WRAP_TIE_RAD
+    tie = argmax_tie | wrap_tie
     ok = ~tie & ~np.isnan(a["K_ps"]) & ~np.isnan(b["K_ps"])
     dg = np.abs(a["coh_ps"] - b["coh_ps"])
     dk_m = np.abs(a["K_ps"] - b["K_ps"]) * k_to_m
-    print(f"ties: {int(tie.sum())} of {tie.size}; non-tie max|dgamma| {dg[ok].max():.2e}, "
-          f"max|dK| {dk_m[ok].max():.2e} m; all-PS max|dgamma| {dg.max():.2e}")
+    dpp = float(np.abs(a["ph_patch"] - b["ph_patch"]).max())
+    print(f"argmax ties {int(argmax_tie.sum())}, wrap ties {int(wrap_tie.sum())} of {tie.size}; "
+          f"non-tie max|dgamma| {dg[ok].max():.2e}, max|dK| {dk_m[ok].max():.2e} m; all-PS max|dgamma| "
+          f"{dg.max():.2e} (PS above 1e-4: {int((dg > 1e-4).sum())}); max|d ph_patch| {dpp:.2e}")
+    assert dpp < WRAP_TIE_RAD
     assert dg[ok].max() <= 1e-4
     assert dk_m[ok].max() <= 1e-3
