@@ -181,6 +181,21 @@ int ps2_clap_filter_grid_noalloc(const float* d_ph_grid, int64_t n_i, int64_t n_
                                  void* stream);
 
 
+/* ---- batches ----------------------------------------------------------------
+ * Runs every loaded context of `ctxs` (FP32, P-square weighting, one device,
+ * each context once) to its own convergence together: each gamma iteration is
+ * one launch per step (binning, CLAP, overlap-add, finalize) covering every
+ * still-iterating patch, and one persistent topofit launch per lane-width
+ * class (4, 8, 16 or 32 lanes per PS, from the patch's interferogram count).
+ * A patch that meets its stop rule drops out; each patch's results are those
+ * of ps2_run_to_convergence on that context alone (same arithmetic, same
+ * per-block partial sums). Work runs on ctxs[0]'s stream after the work
+ * already queued on every context's stream. last[p] (optional, [n]) receives
+ * each patch's final statistics; ps2_download then reads each context. The
+ * reference runs patches one after another
+ * (pystamps/pipeline/stages.py:184-221); this batching has no counterpart. */
+int ps2_batch_run(ps2_ctx* const* ctxs, int64_t n, ps2_iter_stats* last);
+
 /* ---- differentiable coherence (adjoints) ------------------------------------
  * The gamma map with K given, as a function of the input phases, K and the
  * CLAP parameters, on the loaded patch's geometry (cells, bperp, low-pass,

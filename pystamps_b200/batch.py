@@ -1,5 +1,11 @@
-"""Many stage-2 patches: several per GPU on concurrent streams, spread over
-GPUs by longest-processing-time (LPT) assignment.
+"""Many stage-2 patches on one GPU and across GPUs.
+
+`run_batched` loads every patch into its own context and runs them together
+with ps2_batch_run: each gamma iteration is one launch per step over all
+still-iterating patches (one persistent topofit launch per lane-width class).
+`run_patches` is the stream-per-patch alternative (a context per worker
+thread). Across GPUs, patches are spread by longest-processing-time (LPT)
+assignment.
 
 Patches are independent (the reference runs them one after another,
 pystamps/pipeline/stages.py:184-221), so the multi-GPU split is by patch:
@@ -8,11 +14,14 @@ gathered to rank 0 at the end; no collective touches the data path.
 """
 from __future__ import annotations
 
+import ctypes
 import math
 import threading
 from concurrent.futures import ThreadPoolExecutor
 from typing import Callable, Sequence
 
+from . import _lib
+from ._lib import check
 from .stage2 import PreparedPatch, Stage2Context
 
 SUMMARY_KEYS = ("K_ps", "C_ps", "coh_ps", "N_opt")
@@ -42,6 +51,61 @@ def lpt_assign(costs: Sequence[float], n_ranks: int) -> list[list[int]]:
         out[r].append(i)
         loads[r] += costs[i]
     return out
+
+
+class Batch:
+    """Loaded contexts of many patches, run together by ps2_batch_run."""
+
+    def __init__(self, patches: Sequence[PreparedPatch], device: int = 0):
+        self.patches = list(patches)
+        self.ctxs = [Stage2Context(device) for _ in self.patches]
+        try:
+            for c, p in zip(self.ctxs, self.patches):
+                c.load(p, "fp32")
+        except Exception:
+            self.close()
+            raise
+
+    def run(self) -> list[dict]:
+        """All patches to convergence; per-patch last-iteration statistics."""
+        n = len(self.ctxs)
+        arr = (ctypes.c_void_p * n)(*[c._ctx.value for c in self.ctxs])
+        st = (_lib.IterStats * n)()
+        check(_lib.lib().ps2_batch_run(arr, ctypes.c_int64(n), st))
+        return [s.as_dict() for s in st]
+
+    def reset(self) -> None:
+        for c in self.ctxs:
+            c.reset()
+
+    def timing_ms(self) -> float:
+        return self.ctxs[0].timing()[0]
+
+    def launch_count(self) -> int:
+        return self.ctxs[0].launch_count()
+
+    def download(self, keys=SUMMARY_KEYS) -> list[dict]:
+        return [c.download(keys) for c in self.ctxs]
+
+    def close(self) -> None:
+        for c in self.ctxs:
+            c.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def run_batched(patches: Sequence[PreparedPatch], *, device: int = 0, keys=SUMMARY_KEYS) -> list[dict]:
+    """Load, run together to convergence and download every patch."""
+    with Batch(patches, device) as b:
+        stats = b.run()
+        res = b.download(keys)
+        for r, st in zip(res, stats):
+            r["stats"] = st
+        return res
 
 
 def run_patches(patches: Sequence[PreparedPatch], *, device: int = 0, streams: int = 4, precision: str = "fp32",

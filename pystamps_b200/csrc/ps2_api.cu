@@ -234,6 +234,9 @@ struct ps2_ctx {
   DevBuf ad_ph, ad_K, ad_w, ad_coh, ad_grid, ad_win, ad_filt, ad_gfilt, ad_gph, ad_gK, ad_gf, ad_part;
   int ad_blocks = 0, ad_blocks64 = 0;
   cudaEvent_t ad_ev = nullptr;
+  // batches led by this context (ps2_batch_run): per-patch arguments and tables
+  DevBuf bt;
+  int* h_active = nullptr;  // pinned [1]
   cudaGraph_t loop_graph = nullptr;
   cudaGraphExec_t loop_exec = nullptr;
   bool graph_failed = false;
@@ -367,6 +370,29 @@ int copy_in(ps2_ctx* c, DevBuf& dst, const void* src, size_t bytes, bool on_devi
   return PS2_OK;
 }
 
+FinalizeArgs finalize_args(ps2_ctx* c, bool force_continue) {
+  FinalizeArgs f{};
+  f.rms_partial = c->rms_partial.as<double>();
+  f.n_partial = c->topo_blocks;  // unlaunched blocks' partials stay zero
+  f.N = c->N;
+  f.hist = c->hist.as<int32_t>();
+  f.nr_scaled = c->nr_scaled.as<double>();
+  f.nr_max_nz_ix = c->nr_max_nz_ix;
+  f.low_coh_thresh = c->low_coh_thresh;
+  f.psquare = c->psquare;
+  f.gamma_change_convergence = c->conv;
+  f.gamma_max_iterations = c->max_iter;
+  for (int i = 0; i < 7; ++i) f.g7w[i] = c->g7[i];
+  f.g7sum = c->g7sum;
+  f.taps79 = c->taps.as<double>();
+  f.lut = c->lut.as<double>();
+  f.state = c->state.as<double>();
+  f.stats_out = c->stats.as<double>();
+  f.n_invalid = c->n_invalid.as<int32_t>();
+  f.force_continue = force_continue ? 1 : 0;
+  return f;
+}
+
 // Queues one gamma iteration on the context's stream. `later` selects the form
 // of iterations 2.. (P-square weights from the previous table, or the SNR
 // weight kernel); `capturing` queues into a graph without touching counters.
@@ -399,26 +425,7 @@ int enqueue_iteration(ps2_ctx* c, bool later, bool force_continue, cudaEvent_t* 
   CK(launch_topofit(t, fp64, c->topo_blocks, c->st));
   ++launched;
   if (ev) CK(cudaEventRecord(ev[3], c->st));
-  FinalizeArgs f{};
-  f.rms_partial = c->rms_partial.as<double>();
-  f.n_partial = c->topo_blocks;  // unlaunched blocks' partials stay zero
-  f.N = c->N;
-  f.hist = c->hist.as<int32_t>();
-  f.nr_scaled = c->nr_scaled.as<double>();
-  f.nr_max_nz_ix = c->nr_max_nz_ix;
-  f.low_coh_thresh = c->low_coh_thresh;
-  f.psquare = c->psquare;
-  f.gamma_change_convergence = c->conv;
-  f.gamma_max_iterations = c->max_iter;
-  for (int i = 0; i < 7; ++i) f.g7w[i] = c->g7[i];
-  f.g7sum = c->g7sum;
-  f.taps79 = c->taps.as<double>();
-  f.lut = c->lut.as<double>();
-  f.state = c->state.as<double>();
-  f.stats_out = c->stats.as<double>();
-  f.n_invalid = c->n_invalid.as<int32_t>();
-  f.force_continue = force_continue ? 1 : 0;
-  CK(launch_finalize(f, c->st));
+  CK(launch_finalize(finalize_args(c, force_continue), c->st));
   ++launched;
   if (ev) CK(cudaEventRecord(ev[4], c->st));
   if (launched_out) *launched_out = launched;
@@ -542,6 +549,8 @@ void ps2_destroy(ps2_ctx* c) {
   drop_loop_graph(c);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
   if (c->ad_ev) cudaEventDestroy(c->ad_ev);
+  c->bt.release();
+  if (c->h_active) cudaFreeHost(c->h_active);
   if (c->h_stats) cudaFreeHost(c->h_stats);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -1490,6 +1499,162 @@ int ps2_coherence_backward(ps2_ctx* c, const float* d_ph, const float* d_K, cons
     CK(launch_scatter_rows(c->ad_gK.p, d_gK, perm, N, sizeof(float), st));
   }
   c->launches += 7 + (launched > 0 ? 2 : 0);
+  return PS2_OK;
+}
+
+}  // extern "C"
+
+// ============================================================ batch runner ==
+namespace {
+
+// device image of a batch, laid out in one allocation
+struct BatchPlan {
+  std::vector<PatchDev> patch;
+  std::vector<int64_t> bin_prefix, clap_prefix, ov_prefix;
+  std::vector<int32_t> units[4];  // (patch, virtual block) pairs per lane class 4, 8, 16, 32
+  int mpad_max[4] = {0, 0, 0, 0};
+};
+
+int lane_class(int L) { return L == 4 ? 0 : L == 8 ? 1 : L == 16 ? 2 : 3; }
+
+size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+}  // namespace
+
+extern "C" {
+
+int ps2_batch_run(ps2_ctx* const* ctxs, int64_t n, ps2_iter_stats* last) {
+  if (!ctxs || n <= 0) return set_err(PS2_ERR_INVALID_ARG, "ps2_batch_run: need at least one context");
+  if (n > INT32_MAX / 2) return set_err(PS2_ERR_INVALID_ARG, "ps2_batch_run: too many patches");
+  ps2_ctx* c0 = ctxs[0];
+  for (int64_t p = 0; p < n; ++p) {
+    ps2_ctx* c = ctxs[p];
+    if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "ps2_batch_run: context %lld has no patch", (long long)p);
+    if (c->fp64) return set_err(PS2_ERR_UNSUPPORTED, "ps2_batch_run: context %lld is FP64 (batches are FP32)", (long long)p);
+    if (!c->psquare)
+      return set_err(PS2_ERR_UNSUPPORTED, "ps2_batch_run: context %lld uses SNR weighting (batches are P-square)",
+                     (long long)p);
+    if (c->device != c0->device)
+      return set_err(PS2_ERR_INVALID_ARG, "ps2_batch_run: context %lld is on device %d, not %d", (long long)p,
+                     c->device, c0->device);
+    for (int64_t q = 0; q < p; ++q)
+      if (ctxs[q] == c) return set_err(PS2_ERR_INVALID_ARG, "ps2_batch_run: context %lld appears twice", (long long)p);
+  }
+  CK(cudaSetDevice(c0->device));
+  cudaStream_t st = c0->st;
+  int rc = ensure_events(c0, 2);
+  if (rc) return rc;
+  // start after every patch's own queued work (its upload)
+  for (int64_t p = 1; p < n; ++p) {
+    rc = ensure_events(ctxs[p], 1);
+    if (rc) return rc;
+    CK(cudaEventRecord(ctxs[p]->evpool[0], ctxs[p]->st));
+    CK(cudaStreamWaitEvent(st, ctxs[p]->evpool[0], 0));
+  }
+  BatchPlan plan;
+  plan.patch.resize(static_cast<size_t>(n));
+  plan.bin_prefix.assign(1, 0);
+  plan.clap_prefix.assign(1, 0);
+  plan.ov_prefix.assign(1, 0);
+  int64_t cap_iter = 1;
+  for (int64_t p = 0; p < n; ++p) {
+    ps2_ctx* c = ctxs[p];
+    PatchDev& d = plan.patch[p];
+    d.bin = bin_args(c, 0, c->K[0].p);
+    d.clap = clap_args(c, c->grid.p, c->win.p);
+    d.ov = overlap_args(c, c->win.p, c->filt.p);
+    d.topo = topo_args(c, c->K[0].p, c->C.p, c->coh.p);
+    d.fin = finalize_args(c, false);
+    d.K1 = c->K[1].as<float>();
+    d.psquare = c->psquare;
+    int L = 0, mpad = 0, nvb = 0;
+    CK(topofit_geometry(d.topo, c->topo_blocks, &L, &mpad, &nvb));
+    d.mpad = mpad;
+    d.nvb = nvb;
+    d.lanes = L;
+    const int cls = lane_class(L);
+    plan.mpad_max[cls] = std::max(plan.mpad_max[cls], mpad);
+    for (int vb = 0; vb < nvb; ++vb) {
+      plan.units[cls].push_back(static_cast<int32_t>(p));
+      plan.units[cls].push_back(vb);
+    }
+    plan.bin_prefix.push_back(plan.bin_prefix.back() + c->G * c->nchunk);
+    plan.clap_prefix.push_back(plan.clap_prefix.back() + static_cast<int64_t>(c->nwi) * c->nwj * (c->Mp / 4));
+    plan.ov_prefix.push_back(plan.ov_prefix.back() + c->G * c->Mp);
+    cap_iter = std::max<int64_t>(cap_iter, std::max<int64_t>(c->max_iter, 1) + 1);
+  }
+  // one device allocation: patches | active | n_active | prefixes | unit lists
+  const size_t o_patch = 0;
+  const size_t o_active = align256(o_patch + sizeof(PatchDev) * n);
+  const size_t o_nact = align256(o_active + sizeof(int) * n);
+  const size_t o_pref = align256(o_nact + sizeof(int));
+  const size_t o_units = align256(o_pref + sizeof(int64_t) * 3 * (n + 1));
+  size_t o_cls[4], end = o_units;
+  for (int k = 0; k < 4; ++k) {
+    o_cls[k] = end;
+    end = align256(end + sizeof(int32_t) * plan.units[k].size());
+  }
+  std::vector<unsigned char> img(end, 0);
+  std::memcpy(img.data() + o_patch, plan.patch.data(), sizeof(PatchDev) * n);
+  for (int64_t p = 0; p < n; ++p) reinterpret_cast<int*>(img.data() + o_active)[p] = 1;
+  *reinterpret_cast<int*>(img.data() + o_nact) = static_cast<int>(n);
+  int64_t* pref = reinterpret_cast<int64_t*>(img.data() + o_pref);
+  std::memcpy(pref, plan.bin_prefix.data(), sizeof(int64_t) * (n + 1));
+  std::memcpy(pref + (n + 1), plan.clap_prefix.data(), sizeof(int64_t) * (n + 1));
+  std::memcpy(pref + 2 * (n + 1), plan.ov_prefix.data(), sizeof(int64_t) * (n + 1));
+  for (int k = 0; k < 4; ++k)
+    if (!plan.units[k].empty())
+      std::memcpy(img.data() + o_cls[k], plan.units[k].data(), sizeof(int32_t) * plan.units[k].size());
+  CK(c0->bt.alloc(end));
+  CK(cudaMemcpyAsync(c0->bt.p, img.data(), end, cudaMemcpyHostToDevice, st));
+  if (!c0->h_active) CK(cudaMallocHost(reinterpret_cast<void**>(&c0->h_active), sizeof(int)));
+  unsigned char* base = static_cast<unsigned char*>(c0->bt.p);
+  BatchArgs b{};
+  b.patch = reinterpret_cast<const PatchDev*>(base + o_patch);
+  b.P = static_cast<int>(n);
+  b.active = reinterpret_cast<int*>(base + o_active);
+  b.n_active = reinterpret_cast<int*>(base + o_nact);
+  b.bin_prefix = reinterpret_cast<const int64_t*>(base + o_pref);
+  b.clap_prefix = b.bin_prefix + (n + 1);
+  b.ov_prefix = b.bin_prefix + 2 * (n + 1);
+  std::vector<int64_t> before(static_cast<size_t>(n));
+  for (int64_t p = 0; p < n; ++p) before[p] = ctxs[p]->last.i_loop;
+  const int lanes_of[4] = {4, 8, 16, 32};
+  int64_t launched = 0;
+  CK(cudaEventRecord(c0->evpool[0], st));
+  for (int64_t k = 0; k < cap_iter; ++k) {
+    CK(launch_batch_reset(b, st));
+    CK(launch_batch_bin(b, plan.bin_prefix.back(), c0->sm_count, st));
+    CK(launch_batch_clap(b, plan.clap_prefix.back(), c0->twf, c0->sm_count, st));
+    CK(launch_batch_overlap(b, plan.ov_prefix.back(), c0->sm_count, st));
+    launched += 4;
+    for (int cls = 0; cls < 4; ++cls) {
+      if (plan.units[cls].empty()) continue;
+      CK(launch_batch_topofit(b, lanes_of[cls], reinterpret_cast<const int32_t*>(base + o_cls[cls]),
+                              static_cast<int>(plan.units[cls].size() / 2), plan.mpad_max[cls], c0->sm_count, st));
+      ++launched;
+    }
+    CK(launch_batch_finalize(b, st));
+    ++launched;
+    CK(cudaMemcpyAsync(c0->h_active, b.n_active, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (*c0->h_active == 0) break;
+  }
+  CK(cudaEventRecord(c0->evpool[1], st));
+  CK(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, c0->evpool[0], c0->evpool[1]));
+  for (int64_t p = 0; p < n; ++p) {
+    ps2_ctx* c = ctxs[p];
+    CK(cudaMemcpy(c->h_stats, c->stats.p, 8 * sizeof(double), cudaMemcpyDeviceToHost));
+    fill_stats(c->h_stats, &c->last);
+    c->iters_done += c->last.i_loop - before[p];
+    c->launches = launched;
+    c->last_ms = ms;
+    c->last_run_graph = false;
+    for (int i = 0; i < 4; ++i) c->kernel_ms[i] = 0.0;
+    if (last) last[p] = c->last;
+  }
   return PS2_OK;
 }
 

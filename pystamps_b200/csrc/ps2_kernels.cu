@@ -65,8 +65,10 @@ __device__ __forceinline__ R bin_weight(const BinArgs& a, const R* __restrict__ 
   return static_cast<R>(t * t);
 }
 
+// One warp-task of the binning: cell `task / nchunk`, interferograms
+// 32 * (task % nchunk) + lane.
 template <typename R>
-__global__ void __launch_bounds__(256) k_bin(BinArgs a) {
+__device__ __forceinline__ void bin_task(const BinArgs& a, const int64_t task, const int lane) {
   using C = typename CT<R>::C;
   const float2* __restrict__ ph = static_cast<const float2*>(a.ph_nm);
   const R* __restrict__ K = static_cast<const R*>(a.K);
@@ -74,12 +76,8 @@ __global__ void __launch_bounds__(256) k_bin(BinArgs a) {
   const R* __restrict__ coh = static_cast<const R*>(a.coh);
   C* __restrict__ grid = static_cast<C*>(a.grid);
   const float* __restrict__ bp = a.bp;
-  const int lane = threadIdx.x & 31;
-  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
-  const int64_t ntask = a.G * a.nchunk;
   const int64_t M = a.M;
-  for (int64_t task = gw; task < ntask; task += nw) {
+  {
     const int64_t cell = task / a.nchunk;
     const int chunk = static_cast<int>(task - cell * a.nchunk);
     const int c = chunk * 32 + lane;
@@ -131,6 +129,15 @@ __global__ void __launch_bounds__(256) k_bin(BinArgs a) {
     }
     if (c < a.Mp) grid[cell * a.Mp + c] = active ? mk(ax, ay) : mk(R(0), R(0));
   }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_bin(BinArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  const int64_t ntask = a.G * a.nchunk;
+  for (int64_t task = gw; task < ntask; task += nw) bin_task<R>(a, task, lane);
 }
 
 cudaError_t launch_bin(const BinArgs& a, bool fp64, int sm_count, cudaStream_t st) {
@@ -431,33 +438,29 @@ __device__ __forceinline__ void clap_window_warp(ClapTile<R>& T, const int lane,
   __syncwarp();
 }
 
+// Per-patch constants of the CLAP blocks: the low-pass filter and the
+// pyramid weights (the twiddles and smoothing taps are the same for every patch).
 template <typename R>
-__global__ void __launch_bounds__(128) k_clap(ClapArgs a, typename CT<R>::Tw tw) {
+__device__ __forceinline__ void clap_consts(const ClapArgs& a, R* lp, R* wt) {
+  const int nw2 = a.n_win * a.n_win;
+  for (int i = threadIdx.x; i < 1024; i += blockDim.x) lp[i] = static_cast<R>(a.low_pass[i]);
+  for (int i = threadIdx.x; i < nw2; i += blockDim.x) wt[i] = static_cast<R>(a.wscaled[i]);
+}
+
+// One block-task of CLAP: window task / (Mp/4), interferograms 4 * (task % (Mp/4)) + warp.
+template <typename R>
+__device__ __forceinline__ void clap_task(const ClapArgs& a, const int64_t task, ClapTile<R>* tiles,
+                                          const typename CT<R>::C* twf, const typename CT<R>::C* twi, const R* lp,
+                                          const R* wt, const R (&g7)[7]) {
   using C = typename CT<R>::C;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  ClapTile<R>* tiles = reinterpret_cast<ClapTile<R>*>(smem_raw);
-  R* lp = reinterpret_cast<R*>(tiles + 4);
-  R* wt = lp + 1024;
-  C* twf = reinterpret_cast<C*>(wt + 1024);
-  C* twi = twf + 16;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nw = a.n_win, nw2 = nw * nw;
-  for (int i = tid; i < 1024; i += 128) lp[i] = static_cast<R>(a.low_pass[i]);
-  for (int i = tid; i < nw2; i += 128) wt[i] = static_cast<R>(a.wscaled[i]);
-  if (tid < 16) {
-    twf[tid] = tw.w[tid];
-    twi[tid] = mk(tw.w[tid].x, -tw.w[tid].y);
-  }
-  R g7[7];
-#pragma unroll
-  for (int i = 0; i < 7; ++i) g7[i] = static_cast<R>(a.g7[i]);
   const int n_inc = nw / 4 > 1 ? nw / 4 : 1;
   const int ngroups = a.Mp / 4;
-  const int64_t ntask = static_cast<int64_t>(a.nwi) * a.nwj * ngroups;
   const C* __restrict__ grid = static_cast<const C*>(a.grid);
   C* __restrict__ out = static_cast<C*>(a.win_out);
   ClapTile<R>& T = tiles[warp];
-  for (int64_t task = blockIdx.x; task < ntask; task += gridDim.x) {
+  {
     const int64_t wi = task / ngroups;
     const int g = static_cast<int>(task - wi * ngroups);
     const int ix1 = static_cast<int>(wi / a.nwj), ix2 = static_cast<int>(wi - static_cast<int64_t>(ix1) * a.nwj);
@@ -504,6 +507,44 @@ __global__ void __launch_bounds__(128) k_clap(ClapArgs a, typename CT<R>::Tw tw)
   }
 }
 
+// shared-memory carve-up of a CLAP block: 4 tiles, low-pass, weights, twiddles
+template <typename R>
+struct ClapSmem {
+  ClapTile<R>* tiles;
+  R* lp;
+  R* wt;
+  typename CT<R>::C* twf;
+  typename CT<R>::C* twi;
+};
+
+template <typename R>
+__device__ __forceinline__ ClapSmem<R> clap_smem(unsigned char* raw, const typename CT<R>::Tw& tw) {
+  ClapSmem<R> m;
+  m.tiles = reinterpret_cast<ClapTile<R>*>(raw);
+  m.lp = reinterpret_cast<R*>(m.tiles + 4);
+  m.wt = m.lp + 1024;
+  m.twf = reinterpret_cast<typename CT<R>::C*>(m.wt + 1024);
+  m.twi = m.twf + 16;
+  if (threadIdx.x < 16) {
+    m.twf[threadIdx.x] = tw.w[threadIdx.x];
+    m.twi[threadIdx.x] = mk(tw.w[threadIdx.x].x, -tw.w[threadIdx.x].y);
+  }
+  return m;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_clap(ClapArgs a, typename CT<R>::Tw tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const ClapSmem<R> m = clap_smem<R>(smem_raw, tw);
+  clap_consts<R>(a, m.lp, m.wt);
+  R g7[7];
+#pragma unroll
+  for (int i = 0; i < 7; ++i) g7[i] = static_cast<R>(a.g7[i]);
+  const int64_t ntask = static_cast<int64_t>(a.nwi) * a.nwj * (a.Mp / 4);
+  for (int64_t task = blockIdx.x; task < ntask; task += gridDim.x)
+    clap_task<R>(a, task, m.tiles, m.twf, m.twi, m.lp, m.wt, g7);
+}
+
 template <typename R>
 static size_t clap_smem_bytes() {
   return 4 * sizeof(ClapTile<R>) + (1024 + 1024) * sizeof(R) + 32 * 2 * sizeof(R);
@@ -536,14 +577,12 @@ cudaError_t launch_clap(const ClapArgs& a, bool fp64, const Twiddles32f& tf, con
 // Overlap-add as a gather: cell (i, j) sums the windows that cover it, in the
 // reference's raster window order, in f64 (the reference accumulates in f64).
 template <typename R>
-__global__ void __launch_bounds__(256) k_overlap(OverlapArgs a) {
+__device__ __forceinline__ void overlap_elem(const OverlapArgs& a, const int64_t idx) {
   using C = typename CT<R>::C;
   const C* __restrict__ win = static_cast<const C*>(a.win_out);
   C* __restrict__ filt = static_cast<C*>(a.filt);
-  const int64_t total = static_cast<int64_t>(a.n_i) * a.n_j * a.Mp;
   const int nw = a.n_win, nw2 = nw * nw;
-  for (int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
-       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+  {
     const int64_t cell = idx / a.Mp;
     const int c = static_cast<int>(idx - cell * a.Mp);
     const int i = static_cast<int>(cell / a.n_j), j = static_cast<int>(cell - static_cast<int64_t>(i) * a.n_j);
@@ -567,6 +606,14 @@ __global__ void __launch_bounds__(256) k_overlap(OverlapArgs a) {
     }
     filt[idx] = mk(static_cast<R>(sx), static_cast<R>(sy));
   }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_overlap(OverlapArgs a) {
+  const int64_t total = static_cast<int64_t>(a.n_i) * a.n_j * a.Mp;
+  for (int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    overlap_elem<R>(a, idx);
 }
 
 cudaError_t launch_overlap(const OverlapArgs& a, bool fp64, cudaStream_t st) {
@@ -780,15 +827,17 @@ __device__ __forceinline__ void sweep_block(const ColumnSmem& cs, const float qr
   }
 }
 
+// The work of block `vb` of a launch of `nvb` blocks over one patch: PS
+// groups s0 = (vb * 4 + warp) * G + k * nvb * 4 * G. The batched kernel runs
+// the same virtual blocks, so a patch's per-block rms partials, and with them
+// its stop decisions, are the same as when it runs alone.
 template <int L>
-__global__ void __launch_bounds__(128) k_topofit_f32(TopoArgs a, int mpad) {
+__device__ __forceinline__ void topofit_vblock(const TopoArgs& a, const int mpad, const int vb, const int nvb,
+                                               unsigned char* smem_raw, int* sh_hist, double* sh_rms, int* sh_inv) {
   constexpr int G = 32 / L;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ int sh_hist[kCohBins];
-  __shared__ double sh_rms[4];
-  __shared__ int sh_inv[4];
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   const int g = lane / L, gl = lane % L;
+  __syncthreads();
   for (int i = tid; i < kCohBins; i += blockDim.x) sh_hist[i] = 0;
   __syncthreads();
   // per-PS slot stride = L (mod 32) floats so the groups of a warp hit different banks
@@ -810,8 +859,8 @@ __global__ void __launch_bounds__(128) k_topofit_f32(TopoArgs a, int mpad) {
   const unsigned gmask = (L == 32) ? kFull : (((1u << L) - 1u) << (g * L));
   double rms_acc = 0.0;
   int inv_acc = 0;
-  const int64_t step = static_cast<int64_t>(gridDim.x) * 4 * G;
-  for (int64_t s0 = (static_cast<int64_t>(blockIdx.x) * 4 + wib) * G; s0 < a.N; s0 += step) {
+  const int64_t step = static_cast<int64_t>(nvb) * 4 * G;
+  for (int64_t s0 = (static_cast<int64_t>(vb) * 4 + wib) * G; s0 < a.N; s0 += step) {
     const int64_t s = s0 + g;
     const bool active = s < a.N;
     const int64_t cell = (active && !cpx) ? a.cell_of[s] : 0;
@@ -993,12 +1042,21 @@ __global__ void __launch_bounds__(128) k_topofit_f32(TopoArgs a, int mpad) {
   }
   __syncthreads();
   if (tid == 0) {
-    a.rms_partial[blockIdx.x] = sh_rms[0] + sh_rms[1] + sh_rms[2] + sh_rms[3];
+    a.rms_partial[vb] = sh_rms[0] + sh_rms[1] + sh_rms[2] + sh_rms[3];
     const int iv = sh_inv[0] + sh_inv[1] + sh_inv[2] + sh_inv[3];
     if (iv) atomicAdd(a.n_invalid, iv);
   }
   for (int i = tid; i < kCohBins; i += blockDim.x)
     if (sh_hist[i]) atomicAdd(&a.hist[i], sh_hist[i]);
+}
+
+template <int L>
+__global__ void __launch_bounds__(128) k_topofit_f32(TopoArgs a, int mpad) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int sh_hist[kCohBins];
+  __shared__ double sh_rms[4];
+  __shared__ int sh_inv[4];
+  topofit_vblock<L>(a, mpad, blockIdx.x, gridDim.x, smem_raw, sh_hist, sh_rms, sh_inv);
 }
 
 // Plain FP64 topofit: direct sincos for every (trial, column), lanes over
@@ -1188,11 +1246,17 @@ int topofit_lanes(int M) {
   return L;
 }
 
-template <int L>
-static cudaError_t launch_topofit_l(const TopoArgs& a, int grid_cap, cudaStream_t st) {
-  const int mpad = ((a.M + L - 1) / L) * L;
+size_t topofit_smem_bytes(int L, int mpad) {
   const int stride = ((5 * mpad + 31) / 32) * 32 + (L % 32);
-  const size_t sm = static_cast<size_t>(4 * (32 / L)) * stride * sizeof(float);
+  return static_cast<size_t>(4 * (32 / L)) * stride * sizeof(float);
+}
+
+int topofit_mpad(int L, int M) { return ((M + L - 1) / L) * L; }
+
+template <int L>
+static cudaError_t topofit_geometry_l(const TopoArgs& a, int grid_cap, size_t* smem, int* blocks_out) {
+  const int mpad = topofit_mpad(L, a.M);
+  const size_t sm = topofit_smem_bytes(L, mpad);
   cudaError_t e = cudaFuncSetAttribute(k_topofit_f32<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -1206,7 +1270,36 @@ static cudaError_t launch_topofit_l(const TopoArgs& a, int grid_cap, cudaStream_
   const int64_t cap = std::min<int64_t>(grid_cap, static_cast<int64_t>(sms) * std::max(per_sm, 1));
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
-  k_topofit_f32<L><<<static_cast<unsigned>(blocks), 128, sm, st>>>(a, mpad);
+  *smem = sm;
+  *blocks_out = static_cast<int>(blocks);
+  return cudaSuccess;
+}
+
+// Blocks of the FP32 topofit launch for this patch (the virtual blocks a batch
+// reproduces); the lane count is a.lanes or the rule from M.
+cudaError_t topofit_geometry(const TopoArgs& a, int grid_cap, int* L_out, int* mpad_out, int* blocks_out) {
+  const int L = a.lanes ? a.lanes : topofit_lanes(a.M);
+  size_t sm = 0;
+  cudaError_t e;
+  switch (L) {
+    case 4: e = topofit_geometry_l<4>(a, grid_cap, &sm, blocks_out); break;
+    case 8: e = topofit_geometry_l<8>(a, grid_cap, &sm, blocks_out); break;
+    case 16: e = topofit_geometry_l<16>(a, grid_cap, &sm, blocks_out); break;
+    case 32: e = topofit_geometry_l<32>(a, grid_cap, &sm, blocks_out); break;
+    default: return cudaErrorInvalidValue;
+  }
+  *L_out = L;
+  *mpad_out = topofit_mpad(L, a.M);
+  return e;
+}
+
+template <int L>
+static cudaError_t launch_topofit_l(const TopoArgs& a, int grid_cap, cudaStream_t st) {
+  size_t sm = 0;
+  int blocks = 0;
+  cudaError_t e = topofit_geometry_l<L>(a, grid_cap, &sm, &blocks);
+  if (e != cudaSuccess) return e;
+  k_topofit_f32<L><<<static_cast<unsigned>(blocks), 128, sm, st>>>(a, topofit_mpad(L, a.M));
   return cudaGetLastError();
 }
 
@@ -1234,7 +1327,7 @@ cudaError_t launch_topofit(const TopoArgs& a, bool fp64, int grid_blocks, cudaSt
 // P-square update (:364-381, :1642-1683) producing the prand_hi table that the
 // next k_bin turns into weights. Sums use explicit _rn arithmetic and the
 // reference's order so the table matches the reference given equal inputs.
-__global__ void __launch_bounds__(256) k_finalize(FinalizeArgs a) {
+__device__ __forceinline__ void finalize_body(const FinalizeArgs& a) {
   __shared__ double sh[256];
   __shared__ double na[kCohBins], prand[kCohBins], interp_in[kCohBins + 1];
   __shared__ double scale_s;
@@ -1317,6 +1410,8 @@ __global__ void __launch_bounds__(256) k_finalize(FinalizeArgs a) {
     a.lut[i] = __dmul_rn(acc, 10.0);
   }
 }
+
+__global__ void __launch_bounds__(256) k_finalize(FinalizeArgs a) { finalize_body(a); }
 
 // Body tail of the graph that runs the loop to convergence: keep looping while
 // the finalize of this iteration did not raise the stop flag.
@@ -1501,6 +1596,182 @@ cudaError_t launch_random_hist(const double* rnd, int64_t n_rand, const double* 
   return cudaGetLastError();
 }
 
+
+// ============================================================== batches ===
+// Many patches, each iteration one launch per step over every active patch.
+// Work units are numbered patch after patch (prefix tables); a unit finds its
+// patch by binary search. Each unit runs the single-patch code on its patch's
+// arguments, so a patch's results do not depend on what it is batched with.
+
+__device__ __forceinline__ int find_patch(const int64_t* __restrict__ prefix, int P, int64_t u) {
+  int lo = 0, hi = P - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (prefix[mid] <= u)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// per-iteration reset of the active patches: histogram, invalid count, rms
+// partials, and K[1] <- K[0] (the K this iteration bins with)
+__global__ void __launch_bounds__(256) k_batch_reset(BatchArgs b) {
+  const int p = blockIdx.x;
+  if (p >= b.P || !b.active[p]) return;
+  const PatchDev& d = b.patch[p];
+  for (int i = threadIdx.x; i < kCohBins; i += blockDim.x) d.topo.hist[i] = 0;
+  if (threadIdx.x == 0) *d.topo.n_invalid = 0;
+  for (int i = threadIdx.x; i < d.fin.n_partial; i += blockDim.x) d.topo.rms_partial[i] = 0.0;
+  const float* __restrict__ k0 = static_cast<const float*>(d.bin.K);
+  float* __restrict__ k1 = d.K1;
+  for (int64_t i = threadIdx.x; i < d.topo.N; i += blockDim.x) k1[i] = k0[i];
+}
+
+__global__ void __launch_bounds__(256) k_batch_bin(BatchArgs b) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  const int64_t total = b.bin_prefix[b.P];
+  for (int64_t u = gw; u < total; u += nw) {
+    const int p = find_patch(b.bin_prefix, b.P, u);
+    if (!b.active[p]) continue;
+    const PatchDev& d = b.patch[p];
+    BinArgs a = d.bin;
+    // iteration 1 bins with the initial weights, later ones with the P-square table
+    a.mode = (d.psquare && d.fin.state[1] > 1.0) ? 1 : 0;
+    bin_task<float>(a, u - b.bin_prefix[p], lane);
+  }
+}
+
+__global__ void __launch_bounds__(128) k_batch_clap(BatchArgs b, Twiddles32f tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const ClapSmem<float> m = clap_smem<float>(smem_raw, tw);
+  float g7[7];
+  int cur = -1;
+  const int64_t total = b.clap_prefix[b.P];
+  for (int64_t u = blockIdx.x; u < total; u += gridDim.x) {
+    const int p = find_patch(b.clap_prefix, b.P, u);
+    if (!b.active[p]) continue;
+    const ClapArgs& a = b.patch[p].clap;
+    if (p != cur) {
+      // the previous task's readers of lp / wt passed its last barrier
+      clap_consts<float>(a, m.lp, m.wt);
+#pragma unroll
+      for (int i = 0; i < 7; ++i) g7[i] = static_cast<float>(a.g7[i]);
+      cur = p;
+    }
+    clap_task<float>(a, u - b.clap_prefix[p], m.tiles, m.twf, m.twi, m.lp, m.wt, g7);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_batch_overlap(BatchArgs b) {
+  const int64_t total = b.ov_prefix[b.P];
+  for (int64_t u = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; u < total;
+       u += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int p = find_patch(b.ov_prefix, b.P, u);
+    if (!b.active[p]) continue;
+    overlap_elem<float>(b.patch[p].ov, u - b.ov_prefix[p]);
+  }
+}
+
+template <int L>
+__global__ void __launch_bounds__(128) k_batch_topofit(BatchArgs b, const int32_t* __restrict__ units, int n_units) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int sh_hist[kCohBins];
+  __shared__ double sh_rms[4];
+  __shared__ int sh_inv[4];
+  for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
+    const int p = units[2 * u], vb = units[2 * u + 1];
+    if (!b.active[p]) continue;
+    const PatchDev& d = b.patch[p];
+    topofit_vblock<L>(d.topo, d.mpad, vb, d.nvb, smem_raw, sh_hist, sh_rms, sh_inv);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_batch_finalize(BatchArgs b) {
+  const int p = blockIdx.x;
+  if (p >= b.P || !b.active[p]) return;
+  const FinalizeArgs& f = b.patch[p].fin;
+  finalize_body(f);
+  __syncthreads();
+  if (threadIdx.x == 0 && f.stats_out[3] != 0.0 && !f.force_continue) {
+    b.active[p] = 0;
+    atomicSub(b.n_active, 1);
+  }
+}
+
+__global__ void k_batch_continue(cudaGraphConditionalHandle h, const int* n_active) {
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, *n_active > 0 ? 1u : 0u);
+}
+
+cudaError_t launch_batch_reset(const BatchArgs& b, cudaStream_t st) {
+  k_batch_reset<<<b.P, 256, 0, st>>>(b);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_bin(const BatchArgs& b, int64_t total, int sm_count, cudaStream_t st) {
+  const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((total + 7) / 8, static_cast<int64_t>(sm_count) * 16));
+  k_batch_bin<<<static_cast<unsigned>(blocks), 256, 0, st>>>(b);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_clap(const BatchArgs& b, int64_t total, const Twiddles32f& tf, int sm_count,
+                              cudaStream_t st) {
+  if (total <= 0) return cudaSuccess;
+  const size_t sm = clap_smem_bytes<float>();
+  cudaError_t e = cudaFuncSetAttribute(k_batch_clap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_clap, 128, sm);
+  if (e != cudaSuccess) return e;
+  const int64_t blocks = std::min<int64_t>(total, static_cast<int64_t>(sm_count) * std::max(per_sm, 1));
+  k_batch_clap<<<static_cast<unsigned>(blocks), 128, sm, st>>>(b, tf);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_overlap(const BatchArgs& b, int64_t total, int sm_count, cudaStream_t st) {
+  const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, static_cast<int64_t>(sm_count) * 32));
+  k_batch_overlap<<<static_cast<unsigned>(blocks), 256, 0, st>>>(b);
+  return cudaGetLastError();
+}
+
+template <int L>
+static cudaError_t batch_topofit_l(const BatchArgs& b, const int32_t* units, int n_units, int mpad_max, int sm_count,
+                                   cudaStream_t st) {
+  const size_t sm = topofit_smem_bytes(L, mpad_max);
+  cudaError_t e = cudaFuncSetAttribute(k_batch_topofit<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_topofit<L>, 128, sm);
+  if (e != cudaSuccess) return e;
+  const int64_t blocks = std::min<int64_t>(n_units, static_cast<int64_t>(sm_count) * std::max(per_sm, 1));
+  k_batch_topofit<L><<<static_cast<unsigned>(blocks), 128, sm, st>>>(b, units, n_units);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_topofit(const BatchArgs& b, int L, const int32_t* units, int n_units, int mpad_max,
+                                 int sm_count, cudaStream_t st) {
+  if (n_units <= 0) return cudaSuccess;
+  switch (L) {
+    case 4: return batch_topofit_l<4>(b, units, n_units, mpad_max, sm_count, st);
+    case 8: return batch_topofit_l<8>(b, units, n_units, mpad_max, sm_count, st);
+    case 16: return batch_topofit_l<16>(b, units, n_units, mpad_max, sm_count, st);
+    case 32: return batch_topofit_l<32>(b, units, n_units, mpad_max, sm_count, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_batch_finalize(const BatchArgs& b, cudaStream_t st) {
+  k_batch_finalize<<<b.P, 256, 0, st>>>(b);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_continue(cudaGraphConditionalHandle h, const int* n_active, cudaStream_t st) {
+  k_batch_continue<<<1, 32, 0, st>>>(h, n_active);
+  return cudaGetLastError();
+}
 
 // ============================================================== adjoints ==
 // Differentiable stage-2 coherence with K given (no trial search):

@@ -104,6 +104,30 @@ struct FinalizeArgs {
   int force_continue;        // iterate past the stop rule (timing runs)
 };
 
+// --------------------------------------------------------------- batches --
+// One patch of a batch: the single-patch arguments of every step.
+struct PatchDev {
+  BinArgs bin;        // bin.K = K[0]; mode is set per iteration from fin.state
+  ClapArgs clap;
+  OverlapArgs ov;
+  TopoArgs topo;
+  FinalizeArgs fin;
+  float* K1;          // K[1]: the K this iteration binned with
+  int mpad, nvb;      // topofit column padding and virtual blocks
+  int psquare;
+  int lanes;
+};
+
+struct BatchArgs {
+  const PatchDev* patch;      // [P]
+  int P;
+  int* active;                // [P] 1 while the patch iterates
+  int* n_active;              // [1]
+  const int64_t* bin_prefix;  // [P + 1] warp-tasks (G * nchunk)
+  const int64_t* clap_prefix; // [P + 1] block-tasks (W * Mp / 4)
+  const int64_t* ov_prefix;   // [P + 1] elements (G * Mp)
+};
+
 // -------------------------------------------------------------- adjoints --
 // R-typed arrays are float or double by the context's precision.
 struct CohArgs {
@@ -152,6 +176,17 @@ cudaError_t launch_gather_widen(const float* src, double* dst, const int32_t* pe
 cudaError_t launch_scatter_narrow(const double* src, float* dst, const int32_t* perm, int64_t n, int64_t words,
                                   cudaStream_t st);
 cudaError_t launch_reduce_ab(const double* part, int n, double* out, cudaStream_t st);
+size_t topofit_smem_bytes(int L, int mpad);
+cudaError_t topofit_geometry(const TopoArgs& a, int grid_cap, int* L_out, int* mpad_out, int* blocks_out);
+cudaError_t launch_batch_reset(const BatchArgs& b, cudaStream_t st);
+cudaError_t launch_batch_bin(const BatchArgs& b, int64_t total, int sm_count, cudaStream_t st);
+cudaError_t launch_batch_clap(const BatchArgs& b, int64_t total, const Twiddles32f& tf, int sm_count,
+                              cudaStream_t st);
+cudaError_t launch_batch_overlap(const BatchArgs& b, int64_t total, int sm_count, cudaStream_t st);
+cudaError_t launch_batch_topofit(const BatchArgs& b, int L, const int32_t* units, int n_units, int mpad_max,
+                                 int sm_count, cudaStream_t st);
+cudaError_t launch_batch_finalize(const BatchArgs& b, cudaStream_t st);
+cudaError_t launch_batch_continue(cudaGraphConditionalHandle h, const int* n_active, cudaStream_t st);
 cudaError_t launch_snr_weight(const TopoArgs& t, const float* amp, void* w_out, bool fp64, int sm_count,
                               cudaStream_t st);
 cudaError_t launch_random_hist(const double* rnd, int64_t n_rand, const double* bp, int m, const int64_t* ia,
