@@ -56,15 +56,34 @@ def lpt_assign(costs: Sequence[float], n_ranks: int) -> list[list[int]]:
 class Batch:
     """Loaded contexts of many patches, run together by ps2_batch_run."""
 
-    def __init__(self, patches: Sequence[PreparedPatch], device: int = 0):
-        self.patches = list(patches)
-        self.ctxs = [Stage2Context(device) for _ in self.patches]
+    def __init__(self, patches: Sequence[PreparedPatch], device: int = 0, load_threads: int = 8):
+        self.device = device
+        self.load_threads = load_threads
+        self.patches: list[PreparedPatch] = []
+        self.ctxs: list[Stage2Context] = []
         try:
-            for c, p in zip(self.ctxs, self.patches):
-                c.load(p, "fp32")
+            self.load(patches)
         except Exception:
             self.close()
             raise
+
+    def load(self, patches: Sequence[PreparedPatch]) -> None:
+        """(Re)load the patches, one context each; contexts and their device
+        buffers are kept from the previous load where the counts allow. Loads
+        run on `load_threads` host threads (the library releases the GIL; each
+        context has its own stream)."""
+        patches = list(patches)
+        while len(self.ctxs) < len(patches):
+            self.ctxs.append(Stage2Context(self.device))
+        while len(self.ctxs) > len(patches):
+            self.ctxs.pop().close()
+        self.patches = patches
+        if len(patches) > 1 and self.load_threads > 1:
+            with ThreadPoolExecutor(max_workers=min(self.load_threads, len(patches))) as ex:
+                list(ex.map(lambda cp: cp[0].load(cp[1], "fp32"), zip(self.ctxs, patches)))
+        else:
+            for c, p in zip(self.ctxs, patches):
+                c.load(p, "fp32")
 
     def run(self) -> list[dict]:
         """All patches to convergence; per-patch last-iteration statistics."""
@@ -85,6 +104,9 @@ class Batch:
         return self.ctxs[0].launch_count()
 
     def download(self, keys=SUMMARY_KEYS) -> list[dict]:
+        if len(self.ctxs) > 1 and self.load_threads > 1:
+            with ThreadPoolExecutor(max_workers=min(self.load_threads, len(self.ctxs))) as ex:
+                return list(ex.map(lambda c: c.download(keys), self.ctxs))
         return [c.download(keys) for c in self.ctxs]
 
     def close(self) -> None:
