@@ -24,6 +24,17 @@ Fixtures (all seeded):
 * stage2_3ps.npz      -- the same entry point on the reference's 3-PS fixture
                          (native_stage2.rs:2698-2769: empty CLAP, all rows
                          invalid).
+* stage3_units.npz    -- ported._clap_filt_patch on seeded 32x32 patches
+                         (alpha 1 and 1.7, one patch with a zeroed cell and a
+                         NaN), ported._ps_topofit_single in the stage-3 form
+                         (complex64 unit phasors, f32 bperp) on 128 rows, and
+                         ported._coh_threshold_from_dist for both selection
+                         methods.
+* stage3_select.npz   -- ported.stage3_select_ps after the Python stage 2 on a
+                         10,000 PS x 8 ifg patch over a 40 x 40 grid: the
+                         select1.mat variables (ix, keep_ix, ph_patch2,
+                         ph_res2, K_ps2, C_ps2, coh_ps2, coh_thresh, ...)
+                         with the pm1.mat inputs they came from.
 """
 from __future__ import annotations
 
@@ -176,13 +187,102 @@ def make_stage2_3ps(ported) -> None:
     np.savez_compressed(HERE / "stage2_3ps.npz", **{"pm_" + k: v for k, v in pm.items()})
 
 
+def make_stage3_units(ported) -> None:
+    rng = np.random.default_rng(31)
+    n_win = 32
+    freq0 = 1.0 / 800.0
+    freq_i = np.arange(-n_win / 2, n_win / 2) / float(50.0 * n_win)
+    butter = 1.0 / (1.0 + (freq_i / freq0) ** (2 * 5))
+    lp = np.fft.fftshift(np.outer(butter, butter)).astype(np.float64)
+    patches, outs, params = [], [], []
+    for k, (alpha, beta) in enumerate([(1.0, 0.3), (1.7, 0.45), (1.0, 0.3), (0.8, 0.5)]):
+        amp = rng.uniform(0.0, 4.0, (32, 32))
+        g = amp * np.exp(1j * (rng.uniform(-np.pi, np.pi, (32, 32)) + 0.2 * np.arange(32)[None, :]))
+        if k == 2:
+            g[9, 14] = 0
+            g[3, 3] = np.nan
+        patches.append(g)
+        outs.append(ported._clap_filt_patch(g, alpha, beta, lp))
+        params.append((alpha, beta))
+    # topofit rows in the stage-3 form: normalised psdph (complex64), f32 bperp
+    n_row, n_col = 128, 24
+    bp_ifg = rng.uniform(-300, 300, n_col)
+    grad = 1.0 + 0.02 * rng.uniform(-0.5, 0.5, n_row)
+    bperp = (grad[:, None] * bp_ifg[None, :]).astype(np.float32)
+    n_trial_wraps = 7.44
+    k_true = rng.uniform(-0.04, 0.04, n_row)
+    noise = rng.normal(0.0, rng.uniform(0.1, 1.8, n_row)[:, None], (n_row, n_col))
+    cpx = np.exp(1j * (k_true[:, None] * bperp + noise)).astype(np.complex64)
+    cpx[5, 3] = 0  # a zero column is skipped by _ps_topofit_single
+    K = np.empty(n_row); C = np.empty(n_row); coh = np.empty(n_row)
+    res = np.empty((n_row, n_col), np.complex64)
+    for r in range(n_row):
+        k, c, h, pr = ported._ps_topofit_single(cpx[r], bperp[r], n_trial_wraps)
+        K[r], C[r], coh[r] = k, c, h
+        res[r] = pr
+    # coherence thresholds from the distribution
+    n = 30000
+    coh_v = np.clip(np.concatenate([rng.beta(2, 5, 21000), rng.beta(8, 2, 9000)]), 0, 1)
+    coh_v[::997] = np.nan
+    d_a = rng.uniform(0.2, 0.6, n)
+    d_s = np.sort(d_a)
+    d_max = np.concatenate(([0.0], d_s[2000:n - 2000:2000], [d_s[-1]]))
+    centers = np.arange(0.005, 1.0, 0.01)
+    nr = np.exp(-0.5 * ((centers - 0.25) / 0.1) ** 2) * 3000
+    th = {}
+    for meth, mpr in (("DENSITY", 40.0), ("PERCENT", 5.0)):
+        t, cf = ported._coh_threshold_from_dist(coh_values=coh_v, D_A=d_a, D_A_max=d_max, coh_bins=centers,
+                                                Nr_dist=nr, low_coh_thresh=31, max_percent_rand=mpr,
+                                                select_method=meth)
+        th[meth] = (mpr, t, np.asarray(cf, dtype=np.float64))
+    np.savez_compressed(
+        HERE / "stage3_units.npz",
+        clap_in=np.stack(patches), clap_out=np.stack(outs), clap_params=np.asarray(params), low_pass=lp,
+        topo_cpx=cpx, topo_bperp=bperp, topo_ntw=n_trial_wraps, topo_K=K, topo_C=C, topo_coh=coh, topo_res=res,
+        th_coh=coh_v, th_da=d_a, th_damax=d_max, th_centers=centers, th_nr=nr,
+        th_density_mpr=th["DENSITY"][0], th_density=th["DENSITY"][1], th_density_cf=th["DENSITY"][2],
+        th_percent_mpr=th["PERCENT"][0], th_percent=th["PERCENT"][1], th_percent_cf=th["PERCENT"][2],
+    )
+
+
+def make_stage3_select(ported) -> None:
+    from scipy.io import loadmat
+
+    sys.path.insert(0, str(HERE.parents[1]))
+    from pystamps_b200 import synth
+
+    p = synth.make_patch(10000, 8, 40, 41, seed=909, max_topo_err=20.0, gamma_max_iterations=4, n_rand=20000)
+    p["inc"] = np.full(p["ph"].shape[0], p["mean_incidence"])
+    p["parms"].update({"select_method": "DENSITY", "density_rand": 20.0, "slc_osf": 1.0,
+                       "gamma_stdev_reject": 0.0})
+    with tempfile.TemporaryDirectory() as tmp:
+        os.environ["HOME"] = tmp
+        patch = Path(tmp) / "PATCH_1"
+        _write_patch(ported, patch, p)
+        ported.stage2_estimate_gamma(patch, kernel_backend="python")
+        ported.stage3_select_ps(patch)
+        pm = loadmat(patch / "pm1.mat")
+        sel = loadmat(patch / "select1.mat")
+    pm_keys = ["K_ps", "C_ps", "coh_ps", "ph_res", "ph_patch", "ph_grid", "grid_ij", "n_trial_wraps", "Nr",
+               "coh_bins", "low_pass"]
+    sel_keys = ["ix", "keep_ix", "ph_patch2", "ph_res2", "K_ps2", "C_ps2", "coh_ps2", "coh_thresh",
+                "coh_thresh_coeffs", "max_percent_rand", "ifg_index"]
+    np.savez_compressed(
+        HERE / "stage3_select.npz",
+        ph=p["ph"], bperp=p["bperp"], bperp_mat=p["bperp_mat"], D_A=p["D_A"], xy=p["xy"],
+        **{"pm_" + k: np.asarray(pm[k]) for k in pm_keys if k in pm},
+        **{"sel_" + k: np.asarray(sel[k]) for k in sel_keys if k in sel},
+    )
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, type=Path)
     ap.add_argument("--only", default="")
     a = ap.parse_args()
     ported = _import_reference(a.reference)
-    todo = {"clap": make_clap, "topofit": make_topofit, "iter1": make_stage2_iter1, "3ps": make_stage2_3ps}
+    todo = {"clap": make_clap, "topofit": make_topofit, "iter1": make_stage2_iter1, "3ps": make_stage2_3ps,
+            "stage3_units": make_stage3_units, "stage3_select": make_stage3_select}
     for name, fn in todo.items():
         if a.only and name not in a.only.split(","):
             continue
