@@ -196,6 +196,47 @@ int ps2_clap_filter_grid_noalloc(const float* d_ph_grid, int64_t n_i, int64_t n_
  * (pystamps/pipeline/stages.py:184-221); this batching has no counterpart. */
 int ps2_batch_run(ps2_ctx* const* ctxs, int64_t n, ps2_iter_stats* last);
 
+/* ---- stage-3 re-estimate -------------------------------------------------
+ * The re-estimate of stage-3 selection (pystamps/pipeline/ported.py:4429-4575,
+ * inside stage3_select_ps): for each selected PS, the clap_win x clap_win
+ * patch of the stage-2 filtered grid around its cell, with that cell zeroed
+ * (and, for the first interferogram, the slc_osf neighbourhood), is
+ * CLAP-filtered (_clap_filt_patch, :992-1009) and the value at the cell kept
+ * (ph_patch2, 0 where the patch does not fit); then
+ * psdph = ph * conj(ph_patch2) is normalised and re-fitted by the reference's
+ * stage-3 topofit (_ps_topofit_single, :2355-2431: near-max candidates within
+ * 2e-4, each refined, the reference's choice among them) on the fit_ifg
+ * columns. Rows with any zero psdph get K = coh = NaN, C = 0. All pointers are
+ * host pointers; the call is synchronous. FP32 arithmetic (the reference uses
+ * complex128 for the patch filter and complex64 for the fit). */
+typedef struct ps3_reestimate_desc {
+  int64_t n_sel;            /* selected PS rows */
+  int64_t n_ifg;            /* M: interferograms (master column removed) */
+  const float* ph;          /* complex64 [n_sel, M]: the selected rows of ph */
+  const float* bperp;       /* f32 [n_sel, M]: their bp1.bperp_mat rows */
+  const int64_t* grid_ij;   /* [n_sel, 2]: their 1-based pm1.grid_ij cells */
+  const float* ph_grid;     /* complex64 [grid_rows, grid_cols, M]: pm1.ph_grid */
+  int64_t grid_rows, grid_cols;
+  int64_t n_i, n_j;         /* max of pm1.grid_ij over all PS (the patch placement limits) */
+  const int64_t* fit_ifg;   /* [n_fit] 0-based columns the fit uses (ifg_index - 1) */
+  int64_t n_fit;
+  int64_t clap_win;         /* 32 */
+  double clap_alpha, clap_beta;
+  const double* low_pass;   /* [clap_win * clap_win] pm1.low_pass */
+  int64_t slc_osf;
+  double n_trial_wraps;     /* pm1.n_trial_wraps */
+} ps3_reestimate_desc;
+
+typedef struct ps3_reestimate_out {
+  float* ph_patch2;         /* complex64 [n_sel, M] */
+  double* K_ps2;            /* [n_sel] */
+  double* C_ps2;            /* [n_sel] */
+  double* coh_ps2;          /* [n_sel] */
+  float* ph_res2;           /* f32 [n_sel, M]: residual angle on fit_ifg columns, 0 elsewhere */
+} ps3_reestimate_out;
+
+int ps3_reestimate(const ps3_reestimate_desc* desc, ps3_reestimate_out* out, int device);
+
 /* ---- differentiable coherence (adjoints) ------------------------------------
  * The gamma map with K given, as a function of the input phases, K and the
  * CLAP parameters, on the loaded patch's geometry (cells, bperp, low-pass,

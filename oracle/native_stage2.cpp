@@ -1193,3 +1193,367 @@ int orc_stage2_run_f64(const orc_stage2_in* in, orc_stage2_out* out, int threads
 }
 
 }  // extern "C"
+
+// ============================================================ stage 3 ======
+// Stage-3 re-estimate (pystamps/pipeline/ported.py:4429-4575, the Python
+// reference; the Rust native stage 3 has no re-estimate). numpy semantics:
+// _clap_filt_patch in complex128 (ported.py:992-1009); _ps_topofit_single in
+// complex64 / float32 (ported.py:2355-2431) with the near-max candidate rule
+// (:2433-2448, tolerance 2e-4), per-candidate refinement (:2473-2508) and the
+// candidate choice (:2451-2470). numpy's 1-D float sums are pairwise (blocks
+// of 8 partial sums, halving above 128 elements); a reduction over the
+// non-contiguous axis of a 2-D array adds rows in order. The first element of a
+// reduction seeds the accumulator.
+
+namespace s3 {
+
+float pw_f32(const float* a, int64_t n, int64_t stride) {
+  if (n < 8) {
+    float r = -0.0f;
+    for (int64_t i = 0; i < n; ++i) r += a[i * stride];
+    return r;
+  }
+  if (n <= 128) {
+    float r[8];
+    for (int j = 0; j < 8; ++j) r[j] = a[j * stride];
+    int64_t i = 8;
+    for (; i < n - (n % 8); i += 8)
+      for (int j = 0; j < 8; ++j) r[j] += a[(i + j) * stride];
+    float res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+    for (; i < n; ++i) res += a[i * stride];
+    return res;
+  }
+  int64_t n2 = n / 2;
+  n2 -= n2 % 8;
+  return pw_f32(a, n2, stride) + pw_f32(a + n2 * stride, n - n2, stride);
+}
+
+// np.sum of a contiguous float32 vector
+float sum_f32(const float* a, int64_t n) {
+  if (n == 0) return 0.0f;
+  return a[0] + pw_f32(a + 1, n - 1, 1);
+}
+
+// pairwise sum over interleaved complex64 (n = 2 * count floats)
+void pw_c64(const float* a, int64_t n, float* rr, float* ri) {
+  if (n < 8) {
+    float x = -0.0f, y = -0.0f;
+    for (int64_t i = 0; i < n; i += 2) {
+      x += a[i];
+      y += a[i + 1];
+    }
+    *rr = x;
+    *ri = y;
+    return;
+  }
+  if (n <= 128) {
+    float r[8];
+    for (int j = 0; j < 8; ++j) r[j] = a[j];
+    int64_t i = 8;
+    for (; i < n - (n % 8); i += 8)
+      for (int j = 0; j < 8; ++j) r[j] += a[i + j];
+    float x = (r[0] + r[2]) + (r[4] + r[6]);
+    float y = (r[1] + r[3]) + (r[5] + r[7]);
+    for (; i < n; i += 2) {
+      x += a[i];
+      y += a[i + 1];
+    }
+    *rr = x;
+    *ri = y;
+    return;
+  }
+  int64_t n2 = n / 2;
+  n2 -= n2 % 8;
+  float x1, y1, x2, y2;
+  pw_c64(a, n2, &x1, &y1);
+  pw_c64(a + n2, n - n2, &x2, &y2);
+  *rr = x1 + x2;
+  *ri = y1 + y2;
+}
+
+Cx<float> sum_c64(const std::vector<Cx<float>>& v) {
+  if (v.empty()) return {0.0f, 0.0f};
+  float x, y;
+  pw_c64(reinterpret_cast<const float*>(v.data()) + 2, 2 * static_cast<int64_t>(v.size() - 1), &x, &y);
+  return {v[0].re + x, v[0].im + y};
+}
+
+// np.exp(-1j * x) for a float32 x: (cos x, -sin x) through cexpf
+inline Cx<float> cis_neg(float x) { return {std::cos(x), -std::sin(x)}; }
+
+inline Cx<float> mul(Cx<float> a, Cx<float> b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+
+// _clap_filt_patch (ported.py:992-1009) on an n x n complex128 patch
+void clap_patch(const std::complex<double>* in, int64_t n, double alpha, double beta, const double* lp,
+                std::complex<double>* out) {
+  std::vector<std::complex<double>> x(in, in + n * n);
+  for (auto& v : x)
+    if (std::isnan(v.real()) || std::isnan(v.imag())) v = {0.0, 0.0};
+  Fft fft(static_cast<int>(n));
+  for (int64_t r = 0; r < n; ++r) fft.run(&x[r * n], 1, false);
+  for (int64_t c = 0; c < n; ++c) fft.run(&x[c], static_cast<int>(n), false);
+  std::vector<double> h(n * n), hs(n * n), hc(n * n);
+  for (int64_t k = 0; k < n * n; ++k) h[k] = std::abs(x[k]);
+  const int64_t sh = n / 2, ish = (n + 1) / 2;
+  for (int64_t r = 0; r < n; ++r)
+    for (int64_t c = 0; c < n; ++c) hs[r * n + c] = h[((r + sh) % n) * n + (c + sh) % n];
+  // convolve2d(mode="same", fill 0) with outer(g, g); the kernel is symmetric
+  std::vector<double> g = clap_kernel_1d();
+  for (int64_t r = 0; r < n; ++r)
+    for (int64_t c = 0; c < n; ++c) {
+      double s = 0.0;
+      for (int64_t a = -3; a <= 3; ++a)
+        for (int64_t b = -3; b <= 3; ++b) {
+          const int64_t rr = r + a, cc = c + b;
+          if (rr < 0 || rr >= n || cc < 0 || cc >= n) continue;
+          s += hs[rr * n + cc] * (g[a + 3] * g[b + 3]);
+        }
+      hc[r * n + c] = s;
+    }
+  for (int64_t r = 0; r < n; ++r)
+    for (int64_t c = 0; c < n; ++c) h[r * n + c] = hc[((r + ish) % n) * n + (c + ish) % n];
+  std::vector<double> srt(h);
+  std::sort(srt.begin(), srt.end());
+  const size_t mid = srt.size() / 2;
+  const double med = srt.size() % 2 == 0 ? (srt[mid - 1] + srt[mid]) / 2.0 : srt[mid];
+  for (int64_t k = 0; k < n * n; ++k) {
+    double v = h[k];
+    if (med != 0.0) v /= med;
+    v = std::pow(v, alpha) - 1.0;
+    if (v < 0.0) v = 0.0;
+    x[k] *= v * beta + lp[k];
+  }
+  for (int64_t r = 0; r < n; ++r) fft.run(&x[r * n], 1, true);
+  for (int64_t c = 0; c < n; ++c) fft.run(&x[c], static_cast<int>(n), true);
+  const double inv = 1.0 / static_cast<double>(n * n);
+  for (int64_t k = 0; k < n * n; ++k) out[k] = x[k] * inv;
+}
+
+struct Fit {
+  double K, C, coh;
+  std::vector<Cx<float>> res;
+};
+
+// _ps_topofit_refine_candidate (ported.py:2473-2508) in float32
+Fit refine(const std::vector<Cx<float>>& cpx, const std::vector<float>& bp, const std::vector<float>& wgt,
+           const std::vector<float>& wb, double den_lin, double coarse_k0) {
+  const int64_t m = static_cast<int64_t>(cpx.size());
+  float K0 = static_cast<float>(coarse_k0);
+  std::vector<Cx<float>> r(m);
+  for (int64_t c = 0; c < m; ++c) r[c] = mul(cpx[c], cis_neg(K0 * bp[c]));
+  const Cx<float> off = sum_c64(r);
+  std::vector<float> t(m);
+  for (int64_t c = 0; c < m; ++c) {
+    const Cx<float> q = mul(r[c], Cx<float>{off.re, -off.im});
+    t[c] = wb[c] * (wgt[c] * std::atan2(q.im, q.re));
+  }
+  const float mopt = sum_f32(t.data(), m) / static_cast<float>(den_lin);
+  K0 = K0 + mopt;
+  Fit f;
+  f.res.resize(m);
+  std::vector<float> ab(m);
+  for (int64_t c = 0; c < m; ++c) {
+    f.res[c] = mul(cpx[c], cis_neg(K0 * bp[c]));
+    ab[c] = std::hypot(f.res[c].re, f.res[c].im);
+  }
+  const Cx<float> mean = sum_c64(f.res);
+  double den2 = static_cast<double>(sum_f32(ab.data(), m));
+  if (den2 == 0.0) den2 = 1.0;
+  f.K = static_cast<double>(K0);
+  f.C = static_cast<double>(std::atan2(mean.im, mean.re));
+  f.coh = static_cast<double>(std::hypot(mean.re, mean.im) / static_cast<float>(den2));
+  return f;
+}
+
+// _ps_topofit_single (ported.py:2355-2431), complex64 / float32 form.
+// Returns the candidate count (0: no valid column).
+int64_t topofit_single(const Cx<float>* cpx_in, const float* bp_in, int64_t m_in, double n_trial_wraps,
+                       double* K, double* C, double* coh, Cx<float>* res_out) {
+  for (int64_t c = 0; c < m_in; ++c) res_out[c] = {0.0f, 0.0f};
+  std::vector<Cx<float>> cpx;
+  std::vector<float> bp;
+  std::vector<int64_t> col;
+  for (int64_t c = 0; c < m_in; ++c)
+    if (cpx_in[c].re != 0.0f || cpx_in[c].im != 0.0f) {
+      cpx.push_back(cpx_in[c]);
+      bp.push_back(bp_in[c]);
+      col.push_back(c);
+    }
+  const int64_t m = static_cast<int64_t>(cpx.size());
+  if (m == 0) {
+    *K = *C = *coh = std::numeric_limits<double>::quiet_NaN();
+    return 0;
+  }
+  const int64_t nt = static_cast<int64_t>(std::ceil(8.0 * n_trial_wraps));
+  const int64_t T = 2 * nt + 1;
+  float mn = bp[0], mx = bp[0];
+  for (float v : bp) {
+    mn = std::min(mn, v);
+    mx = std::max(mx, v);
+  }
+  double range = static_cast<double>(mx - mn);
+  if (range == 0.0) range = 1.0;
+  const float rf = static_cast<float>(range), qp = static_cast<float>(M_PI / 4.0);
+  std::vector<float> tp(m);
+  for (int64_t c = 0; c < m; ++c) tp[c] = bp[c] / rf * qp;
+  std::vector<float> ab(m), wgt(m), wb(m), wb2(m);
+  for (int64_t c = 0; c < m; ++c) {
+    ab[c] = std::hypot(cpx[c].re, cpx[c].im);
+    wgt[c] = ab[c];
+    wb[c] = wgt[c] * bp[c];
+    wb2[c] = wb[c] * wb[c];
+  }
+  double denom = static_cast<double>(sum_f32(ab.data(), m));
+  if (denom == 0.0) denom = 1.0;
+  double den_lin = static_cast<double>(sum_f32(wb2.data(), m));
+  if (den_lin == 0.0) den_lin = 1.0;
+  std::vector<double> ct(T);
+  for (int64_t t = 0; t < T; ++t) {
+    const float tm = static_cast<float>(t - nt);
+    float sx = 0.0f, sy = 0.0f;
+    for (int64_t c = 0; c < m; ++c) {  // rows of the (m, T) product added in order
+      const Cx<float> p = mul(cis_neg(tp[c] * tm), cpx[c]);
+      if (c == 0) {
+        sx = p.re;
+        sy = p.im;
+      } else {
+        sx += p.re;
+        sy += p.im;
+      }
+    }
+    ct[t] = static_cast<double>(std::hypot(sx, sy) / static_cast<float>(denom));
+  }
+  // _ps_topofit_near_max_trial_indices (ported.py:2433-2448)
+  std::vector<int64_t> cand;
+  const double cmax = *std::max_element(ct.begin(), ct.end());
+  for (int64_t t = 0; t < T; ++t) {
+    bool lm;
+    if (T == 1) lm = true;
+    else if (t == 0) lm = ct[0] >= ct[1];
+    else if (t == T - 1) lm = ct[T - 1] >= ct[T - 2];
+    else lm = ct[t] >= ct[t - 1] && ct[t] >= ct[t + 1];
+    if (lm && ct[t] >= cmax - 2.0e-4) cand.push_back(t);
+  }
+  if (cand.empty()) cand.push_back(std::max_element(ct.begin(), ct.end()) - ct.begin());
+  std::vector<Fit> fits;
+  for (int64_t t : cand)
+    fits.push_back(refine(cpx, bp, wgt, wb, den_lin, (M_PI / 4.0) / range * static_cast<double>(t - nt)));
+  // _ps_topofit_select_candidate (ported.py:2451-2470)
+  size_t pick = 0;
+  if (cand.size() > 1) {
+    size_t coarse_best = 0;
+    for (size_t i = 1; i < cand.size(); ++i)
+      if (ct[cand[i]] > ct[cand[coarse_best]]) coarse_best = i;
+    const bool endpoints = cand.size() == 2 && cand[0] == 0 && cand[1] == T - 1;
+    if (endpoints) {
+      pick = coarse_best;
+    } else {
+      size_t rb = 0;
+      for (size_t i = 1; i < fits.size(); ++i)
+        if (fits[i].coh > fits[rb].coh) rb = i;
+      pick = rb;
+    }
+  }
+  *K = fits[pick].K;
+  *C = fits[pick].C;
+  *coh = fits[pick].coh;
+  for (int64_t k = 0; k < m; ++k) res_out[col[k]] = fits[pick].res[k];
+  return static_cast<int64_t>(cand.size());
+}
+
+}  // namespace s3
+
+extern "C" {
+
+void orc_s3_clap_patch(const double* in, int64_t n, double alpha, double beta, const double* lp, double* out) {
+  s3::clap_patch(reinterpret_cast<const std::complex<double>*>(in), n, alpha, beta, lp,
+                 reinterpret_cast<std::complex<double>*>(out));
+}
+
+int64_t orc_s3_topofit_single(const float* cpx, const float* bp, int64_t m, double n_trial_wraps, double* K,
+                              double* C, double* coh, float* res) {
+  return s3::topofit_single(reinterpret_cast<const Cx<float>*>(cpx), bp, m, n_trial_wraps, K, C, coh,
+                            reinterpret_cast<Cx<float>*>(res));
+}
+
+// The re-estimate loop of ported.py:4489-4550 for the selected rows `sel`.
+// ph_grid complex64 [gi, gj, m]; grid_ij [n_ps, 2] 1-based; ph_work complex64
+// [n_ps, m]; bperp f64 [n_ps, m]; fit: 0-based columns topofit uses. Outputs:
+// ph_patch2 complex128 [n_sel, m], K2/C2/coh2 [n_sel], ph_res2 f32 [n_sel, m].
+int orc_s3_reestimate(const float* ph_grid, int64_t gi, int64_t gj, int64_t m, const int64_t* grid_ij,
+                      const int64_t* sel, int64_t n_sel, const float* ph_work, const double* bperp,
+                      const int64_t* fit, int64_t n_fit, int64_t n_i, int64_t n_j, int64_t n_win, double alpha,
+                      double beta, const double* lp, int64_t slc_osf, double n_trial_wraps, double* ph_patch2,
+                      double* K2, double* C2, double* coh2, float* ph_res2, int threads) {
+  (void)gi;
+  const int64_t half = n_win / 2;
+  const Cx<float>* grid = reinterpret_cast<const Cx<float>*>(ph_grid);
+  const Cx<float>* work = reinterpret_cast<const Cx<float>*>(ph_work);
+  std::complex<double>* pp2 = reinterpret_cast<std::complex<double>*>(ph_patch2);
+  parallel_for(n_sel, threads, [&](int64_t b, int64_t e) {
+    std::vector<std::complex<double>> bit(n_win * n_win), filt(n_win * n_win);
+    std::vector<Cx<float>> cpx(n_fit), res(n_fit);
+    std::vector<float> bpf(n_fit);
+    for (int64_t r = b; r < e; ++r) {
+      const int64_t ps = sel[r];
+      const int64_t pi = grid_ij[2 * ps], pj = grid_ij[2 * ps + 1];
+      int64_t i_min = std::max<int64_t>(pi - half, 1), i_max = i_min + n_win - 1;
+      if (i_max > n_i) {
+        i_min = i_min - i_max + n_i;
+        i_max = n_i;
+      }
+      int64_t j_min = std::max<int64_t>(pj - half, 1), j_max = j_min + n_win - 1;
+      if (j_max > n_j) {
+        j_min = j_min - j_max + n_j;
+        j_max = n_j;
+      }
+      std::complex<double>* out = pp2 + r * m;
+      if (i_min < 1 || j_min < 1) {
+        for (int64_t c = 0; c < m; ++c) out[c] = {0.0, 0.0};
+      } else {
+        const int64_t bi = pi - i_min, bj = pj - j_min;  // 0-based PS cell in the patch
+        const int64_t rad = slc_osf - 1;
+        for (int64_t c = 0; c < m; ++c) {
+          for (int64_t li = 0; li < n_win; ++li)
+            for (int64_t lj = 0; lj < n_win; ++lj) {
+              const Cx<float> v = grid[((i_min - 1 + li) * gj + (j_min - 1 + lj)) * m + c];
+              bit[li * n_win + lj] = {static_cast<double>(v.re), static_cast<double>(v.im)};
+            }
+          bit[bi * n_win + bj] = {0.0, 0.0};
+          if (c == 0)
+            for (int64_t li = std::max<int64_t>(bi - rad, 0); li <= std::min<int64_t>(bi + rad, n_win - 1); ++li)
+              for (int64_t lj = std::max<int64_t>(bj - rad, 0); lj <= std::min<int64_t>(bj + rad, n_win - 1); ++lj)
+                bit[li * n_win + lj] = {0.0, 0.0};
+          s3::clap_patch(bit.data(), n_win, alpha, beta, lp, filt.data());
+          out[c] = filt[bi * n_win + bj];
+        }
+      }
+      // psdph = ph_work * conj(ph_patch2) (complex128); any zero -> NaN row
+      bool any_zero = false;
+      std::vector<std::complex<double>> psd(m);
+      for (int64_t c = 0; c < m; ++c) {
+        const Cx<float> w = work[ps * m + c];
+        psd[c] = std::complex<double>(w.re, w.im) * std::conj(out[c]);
+        if (psd[c] == std::complex<double>(0.0, 0.0)) any_zero = true;
+      }
+      float* pr = ph_res2 + r * m;
+      for (int64_t c = 0; c < m; ++c) pr[c] = 0.0f;
+      if (any_zero) {
+        K2[r] = std::numeric_limits<double>::quiet_NaN();
+        coh2[r] = std::numeric_limits<double>::quiet_NaN();
+        C2[r] = 0.0;
+        continue;
+      }
+      for (int64_t k = 0; k < n_fit; ++k) {
+        const std::complex<double> v = psd[fit[k]] / std::abs(psd[fit[k]]);
+        cpx[k] = {static_cast<float>(v.real()), static_cast<float>(v.imag())};
+        bpf[k] = static_cast<float>(bperp[ps * m + fit[k]]);
+      }
+      s3::topofit_single(cpx.data(), bpf.data(), n_fit, n_trial_wraps, &K2[r], &C2[r], &coh2[r], res.data());
+      for (int64_t k = 0; k < n_fit; ++k) pr[fit[k]] = std::atan2(res[k].im, res[k].re);
+    }
+  });
+  return 0;
+}
+
+}  // extern "C"

@@ -353,3 +353,52 @@ def topofit(cpxphase, bperp, n_trial_wraps: float, threads=None, fp64: bool | No
     fn(_p(cpx, pt), _p(bp, _c_f64p), ctypes.c_int(row_inv), ctypes.c_double(n_trial_wraps), _c_i64(n), _c_i64(m),
        _p(K, _c_f64p), _p(C, _c_f64p), _p(coh, _c_f64p), _p(res, pt), _p(bix, _c_i64p), ctypes.c_int(_threads(threads)))
     return K, C, coh, res, bix
+
+
+# ------------------------------------------------------ stage-3 re-estimate --
+def s3_clap_patch(patch, alpha: float, beta: float, low_pass) -> np.ndarray:
+    """ported._clap_filt_patch (ported.py:992-1009), complex128."""
+    x = np.ascontiguousarray(patch, dtype=np.complex128)
+    n = x.shape[0]
+    lp = np.ascontiguousarray(low_pass, dtype=np.float64)
+    out = np.empty_like(x)
+    lib().orc_s3_clap_patch(_p(x, _c_f64p), _c_i64(n), ctypes.c_double(alpha), ctypes.c_double(beta),
+                            _p(lp, _c_f64p), _p(out, _c_f64p))
+    return out
+
+
+def s3_topofit_single(cpx, bperp, n_trial_wraps: float):
+    """ported._ps_topofit_single (ported.py:2355-2431) in the complex64 / float32
+    form stage 3 uses. Returns (K, C, coh, residual complex64, candidate count)."""
+    c = np.ascontiguousarray(cpx, dtype=np.complex64)
+    b = np.ascontiguousarray(bperp, dtype=np.float32)
+    K = ctypes.c_double(); C = ctypes.c_double(); h = ctypes.c_double()
+    res = np.empty_like(c)
+    lib().orc_s3_topofit_single.restype = ctypes.c_int64
+    nc = lib().orc_s3_topofit_single(_p(c, _c_f32p), _p(b, _c_f32p), _c_i64(c.size), ctypes.c_double(n_trial_wraps),
+                                     ctypes.byref(K), ctypes.byref(C), ctypes.byref(h), _p(res, _c_f32p))
+    return K.value, C.value, h.value, res, int(nc)
+
+
+def s3_reestimate(ph_grid, grid_ij, sel, ph_work, bperp, fit_ix, *, alpha: float, beta: float, low_pass,
+                  n_trial_wraps: float, slc_osf: int = 1, n_win: int = 32, threads=None) -> dict:
+    """The stage-3 re-estimate loop (ported.py:4489-4550) for rows `sel`."""
+    g = np.ascontiguousarray(ph_grid, dtype=np.complex64)
+    gi, gj, m = g.shape
+    ij = np.ascontiguousarray(np.asarray(grid_ij).reshape(-1, 2), dtype=np.int64)
+    s = np.ascontiguousarray(sel, dtype=np.int64)
+    w = np.ascontiguousarray(ph_work, dtype=np.complex64)
+    bp = np.ascontiguousarray(bperp, dtype=np.float64)
+    f = np.ascontiguousarray(fit_ix, dtype=np.int64)
+    lp = np.ascontiguousarray(low_pass, dtype=np.float64)
+    n_i, n_j = int(ij[:, 0].max()), int(ij[:, 1].max())
+    pp2 = np.empty((s.size, m), dtype=np.complex128)
+    K = np.empty(s.size); C = np.empty(s.size); coh = np.empty(s.size)
+    res = np.empty((s.size, m), dtype=np.float32)
+    lib().orc_s3_reestimate(_p(g, _c_f32p), _c_i64(gi), _c_i64(gj), _c_i64(m), _p(ij, _c_i64p), _p(s, _c_i64p),
+                            _c_i64(s.size), _p(w, _c_f32p), _p(bp, _c_f64p), _p(f, _c_i64p), _c_i64(f.size),
+                            _c_i64(n_i), _c_i64(n_j), _c_i64(n_win), ctypes.c_double(alpha), ctypes.c_double(beta),
+                            _p(lp, _c_f64p), _c_i64(slc_osf), ctypes.c_double(n_trial_wraps), _p(pp2, _c_f64p),
+                            _p(K, _c_f64p), _p(C, _c_f64p), _p(coh, _c_f64p), _p(res, _c_f32p),
+                            ctypes.c_int(_threads(threads)))
+    return {"ph_patch2": pp2, "K_ps2": K, "C_ps2": C, "coh_ps2": coh, "ph_res2": res}

@@ -35,7 +35,7 @@ EXPORTED = (
     "ps2_create", "ps2_destroy", "ps2_last_error", "ps2_load_patch", "ps2_iterate", "ps2_run_to_convergence",
     "ps2_reset", "ps2_download", "ps2_last_timing", "ps2_last_launch_count", "ps2_grid_accumulate", "ps2_topofit",
     "ps2_clap_filter_grid", "ps2_random_coherence_histogram", "ps2_clap_filter_grid_noalloc", "ps2_autotune",
-    "ps2_coherence_forward", "ps2_coherence_backward", "ps2_batch_run",
+    "ps2_coherence_forward", "ps2_coherence_backward", "ps2_batch_run", "ps3_reestimate",
 )
 
 
@@ -80,6 +80,19 @@ class Outputs(ctypes.Structure):
         ("i_loop", c_vp), ("ph_res_f64", c_vp), ("ph_patch_f64", c_vp), ("ph_grid_f64", c_vp),
         ("ph_weight_f64", c_vp),
     ]
+
+
+class S3Desc(ctypes.Structure):
+    _fields_ = [
+        ("n_sel", c_i64), ("n_ifg", c_i64), ("ph", c_vp), ("bperp", c_vp), ("grid_ij", c_vp), ("ph_grid", c_vp),
+        ("grid_rows", c_i64), ("grid_cols", c_i64), ("n_i", c_i64), ("n_j", c_i64), ("fit_ifg", c_vp),
+        ("n_fit", c_i64), ("clap_win", c_i64), ("clap_alpha", ctypes.c_double), ("clap_beta", ctypes.c_double),
+        ("low_pass", c_vp), ("slc_osf", c_i64), ("n_trial_wraps", ctypes.c_double),
+    ]
+
+
+class S3Out(ctypes.Structure):
+    _fields_ = [("ph_patch2", c_vp), ("K_ps2", c_vp), ("C_ps2", c_vp), ("coh_ps2", c_vp), ("ph_res2", c_vp)]
 
 
 _lib = None

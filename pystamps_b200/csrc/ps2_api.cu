@@ -1659,3 +1659,137 @@ int ps2_batch_run(ps2_ctx* const* ctxs, int64_t n, ps2_iter_stats* last) {
 }
 
 }  // extern "C"
+
+// ======================================================= stage-3 re-estimate ==
+extern "C" {
+
+int ps3_reestimate(const ps3_reestimate_desc* d, ps3_reestimate_out* o, int device) {
+  if (!d || !o) return set_err(PS2_ERR_INVALID_ARG, "ps3_reestimate: NULL argument");
+  if (d->n_sel < 0 || d->n_ifg <= 0 || d->n_ifg > 4096)
+    return set_err(PS2_ERR_INVALID_ARG, "ps3_reestimate: n_sel %lld / n_ifg %lld out of range", (long long)d->n_sel,
+                   (long long)d->n_ifg);
+  if (d->clap_win != 32) return set_err(PS2_ERR_UNSUPPORTED, "ps3_reestimate: clap_win %lld unsupported (32)", (long long)d->clap_win);
+  if (d->n_fit <= 0 || d->n_fit > d->n_ifg || d->n_fit > 1024)
+    return set_err(PS2_ERR_INVALID_ARG, "ps3_reestimate: n_fit %lld out of range", (long long)d->n_fit);
+  if (!(d->n_trial_wraps >= 0.0) || d->n_trial_wraps > 512.0)
+    return set_err(PS2_ERR_INVALID_ARG, "ps3_reestimate: n_trial_wraps %g out of range", d->n_trial_wraps);
+  if (d->slc_osf < 1) return set_err(PS2_ERR_INVALID_ARG, "ps3_reestimate: slc_osf must be >= 1");
+  if (d->n_i > d->grid_rows || d->n_j > d->grid_cols || d->n_i < 1 || d->n_j < 1)
+    return set_err(PS2_ERR_UNSUPPORTED,
+                   "ps3_reestimate: cell range %lldx%lld outside the %lldx%lld ph_grid (the reference would filter a "
+                   "truncated patch)", (long long)d->n_i, (long long)d->n_j, (long long)d->grid_rows,
+                   (long long)d->grid_cols);
+  if (d->n_sel > 0 && (!d->ph || !d->bperp || !d->grid_ij || !d->ph_grid || !d->fit_ifg || !d->low_pass))
+    return set_err(PS2_ERR_INVALID_ARG, "ps3_reestimate: a required array is NULL");
+  if (d->n_sel > 0 && (!o->ph_patch2 || !o->K_ps2 || !o->C_ps2 || !o->coh_ps2 || !o->ph_res2))
+    return set_err(PS2_ERR_INVALID_ARG, "ps3_reestimate: an output array is NULL");
+  for (int64_t k = 0; k < d->n_fit; ++k)
+    if (d->fit_ifg[k] < 0 || d->fit_ifg[k] >= d->n_ifg)
+      return set_err(PS2_ERR_INVALID_ARG, "ps3_reestimate: fit_ifg[%lld] = %lld outside 0..%lld", (long long)k,
+                     (long long)d->fit_ifg[k], (long long)d->n_ifg - 1);
+  if (d->n_sel == 0) return PS2_OK;
+  CK(cudaSetDevice(device));
+  const int64_t M = d->n_ifg, n = d->n_sel, n_i = d->n_i, n_j = d->n_j, half = d->clap_win / 2, nw = d->clap_win;
+  // one patch per distinct PS cell (ported.py:4496-4516)
+  std::vector<int32_t> cell_job(static_cast<size_t>(n_i * n_j), -1), job_of(n), jobs;
+  for (int64_t r = 0; r < n; ++r) {
+    const int64_t pi = d->grid_ij[2 * r], pj = d->grid_ij[2 * r + 1];
+    if (pi < 1 || pi > n_i || pj < 1 || pj > n_j)
+      return set_err(PS2_ERR_INVALID_ARG, "ps3_reestimate: grid_ij of row %lld = (%lld, %lld) outside 1..%lld x 1..%lld",
+                     (long long)r, (long long)pi, (long long)pj, (long long)n_i, (long long)n_j);
+    int32_t& j = cell_job[(pi - 1) * n_j + (pj - 1)];
+    if (j < 0) {
+      j = static_cast<int32_t>(jobs.size() / 4);
+      int64_t i_min = std::max<int64_t>(pi - half, 1), i_max = i_min + nw - 1;
+      if (i_max > n_i) i_min = i_min - i_max + n_i;
+      int64_t j_min = std::max<int64_t>(pj - half, 1), j_max = j_min + nw - 1;
+      if (j_max > n_j) j_min = j_min - j_max + n_j;
+      const bool ok = i_min >= 1 && j_min >= 1;
+      jobs.push_back(ok ? static_cast<int32_t>(i_min - 1) : -1);
+      jobs.push_back(ok ? static_cast<int32_t>(j_min - 1) : -1);
+      jobs.push_back(static_cast<int32_t>(pi - i_min));
+      jobs.push_back(static_cast<int32_t>(pj - j_min));
+    }
+    job_of[r] = j;
+  }
+  const int64_t n_jobs = static_cast<int64_t>(jobs.size() / 4);
+  std::vector<int32_t> fit(d->fit_ifg, d->fit_ifg + d->n_fit);
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, device));
+  cudaStream_t st;
+  CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() { cudaStreamDestroy(s); }
+  } guard{st};
+  DevBuf grid, ph, bp, djobs, djob_of, jout, dfit, lp, pp2, K2, C2, coh2, res2;
+  const size_t gbytes = sizeof(float2) * d->grid_rows * d->grid_cols * M;
+  CK(grid.alloc(gbytes));
+  CK(cudaMemcpyAsync(grid.p, d->ph_grid, gbytes, cudaMemcpyHostToDevice, st));
+  CK(ph.alloc(sizeof(float2) * n * M));
+  CK(cudaMemcpyAsync(ph.p, d->ph, sizeof(float2) * n * M, cudaMemcpyHostToDevice, st));
+  CK(bp.alloc(sizeof(float) * n * M));
+  CK(cudaMemcpyAsync(bp.p, d->bperp, sizeof(float) * n * M, cudaMemcpyHostToDevice, st));
+  CK(djobs.alloc(sizeof(int32_t) * jobs.size()));
+  CK(cudaMemcpyAsync(djobs.p, jobs.data(), sizeof(int32_t) * jobs.size(), cudaMemcpyHostToDevice, st));
+  CK(djob_of.alloc(sizeof(int32_t) * n));
+  CK(cudaMemcpyAsync(djob_of.p, job_of.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+  CK(dfit.alloc(sizeof(int32_t) * fit.size()));
+  CK(cudaMemcpyAsync(dfit.p, fit.data(), sizeof(int32_t) * fit.size(), cudaMemcpyHostToDevice, st));
+  CK(lp.alloc(sizeof(double) * 1024));
+  CK(cudaMemcpyAsync(lp.p, d->low_pass, sizeof(double) * 1024, cudaMemcpyHostToDevice, st));
+  CK(jout.alloc(sizeof(float2) * n_jobs * M));
+  CK(pp2.alloc(sizeof(float2) * n * M));
+  CK(res2.alloc(sizeof(float) * n * M));
+  CK(K2.alloc(sizeof(double) * n));
+  CK(C2.alloc(sizeof(double) * n));
+  CK(coh2.alloc(sizeof(double) * n));
+  Twiddles32f tf;
+  Twiddles32d td;
+  twiddles(&tf, &td);
+  S3ClapArgs ca{};
+  ca.grid = grid.as<float2>();
+  ca.grid_cols = static_cast<int>(d->grid_cols);
+  ca.M = static_cast<int>(M);
+  ca.jobs = djobs.as<int32_t>();
+  ca.n_jobs = n_jobs;
+  ca.ngroups = static_cast<int>((M + 3) / 4);
+  ca.slc_rad = static_cast<int>(d->slc_osf - 1);
+  ca.alpha = d->clap_alpha;
+  ca.beta = d->clap_beta;
+  ca.alpha_is_one = d->clap_alpha == 1.0 ? 1 : 0;
+  ca.low_pass = lp.as<double>();
+  gauss7(ca.g7, nullptr);
+  ca.job_out = jout.as<float2>();
+  CK(launch_s3_clap(ca, tf, prop.multiProcessorCount, st));
+  S3FitArgs fa{};
+  fa.ph = ph.as<float2>();
+  fa.bp = bp.as<float>();
+  fa.job_of = djob_of.as<int32_t>();
+  fa.job_out = jout.as<float2>();
+  fa.fit = dfit.as<int32_t>();
+  fa.n_fit = static_cast<int>(d->n_fit);
+  fa.M = static_cast<int>(M);
+  fa.n_half = static_cast<int>(std::ceil(8.0 * d->n_trial_wraps));
+  fa.n_sel = n;
+  const int T = 2 * fa.n_half + 1;
+  fa.warp_smem = (static_cast<size_t>(d->n_fit) * 16 + static_cast<size_t>(T) * 4 + 15) & ~size_t(15);
+  if (4 * fa.warp_smem > 200 * 1024)
+    return set_err(PS2_ERR_UNSUPPORTED, "ps3_reestimate: %lld fit interferograms x %d trials exceed shared memory",
+                   (long long)d->n_fit, T);
+  fa.ph_patch2 = pp2.as<float2>();
+  fa.K2 = K2.as<double>();
+  fa.C2 = C2.as<double>();
+  fa.coh2 = coh2.as<double>();
+  fa.ph_res2 = res2.as<float>();
+  CK(launch_s3_fit(fa, prop.multiProcessorCount, st));
+  CK(cudaMemcpyAsync(o->ph_patch2, pp2.p, sizeof(float2) * n * M, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(o->ph_res2, res2.p, sizeof(float) * n * M, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(o->K_ps2, K2.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(o->C_ps2, C2.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(o->coh_ps2, coh2.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return PS2_OK;
+}
+
+}  // extern "C"

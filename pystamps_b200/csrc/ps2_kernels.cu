@@ -1597,6 +1597,336 @@ cudaError_t launch_random_hist(const double* rnd, int64_t n_rand, const double* 
 }
 
 
+// ============================================================== stage 3 ===
+// Stage-3 re-estimate (pystamps/pipeline/ported.py:4489-4550): for every grid
+// cell holding a selected PS, the 32x32 patch of the stage-2 grid around it with
+// the PS's own cell zeroed is CLAP-filtered (_clap_filt_patch, :992-1009) and
+// the filtered value at that cell is kept; then each selected PS is re-fitted
+// (_ps_topofit_single, :2355-2431) against it.
+
+// One warp: the 32x32 patch in its tile -> the filtered value at (bi, bj),
+// times 1024. The inverse FFT is evaluated at that one point:
+// y = sum_{k1,k2} Y[k1][k2] e^{+2 pi i (k1 bi + k2 bj) / 32}.
+__device__ __forceinline__ float2 s3_patch_point(ClapTile<float>& T, const int lane, const S3ClapArgs& a,
+                                                 const float2* twf, const float2* wp, const float* lp,
+                                                 const float (&g7)[7], const int bi, const int bj) {
+  fft_pass<float>(T.re, T.im, twf, lane, true);
+  __syncwarp();
+  fft_pass<float>(T.re, T.im, twf, lane, false);
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    const float xr = T.re[k][lane], xi = T.im[k][lane];
+    T.hs[k][lane] = sqrtf(xr * xr + xi * xi);
+  }
+  __syncwarp();
+  // 7x7 Gaussian 'same' smoothing of fftshift(|X|), then ifftshift, in
+  // unshifted coordinates (the seam at the Nyquist row / column)
+  float t[32];
+  const int sj = (lane + 16) & 31;
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    float acc = 0.f;
+#pragma unroll
+    for (int d = -3; d <= 3; ++d)
+      if (sj + d >= 0 && sj + d < 32) acc += T.hs[k][(lane + d) & 31] * g7[d + 3];
+    t[k] = acc;
+  }
+  float o[32];
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    const int sk = (k + 16) & 31;
+    float acc = 0.f;
+#pragma unroll
+    for (int d = -3; d <= 3; ++d)
+      if (sk + d >= 0 && sk + d < 32) acc += t[(k + d) & 31] * g7[d + 3];
+    o[k] = acc;
+  }
+  const float med = warp_median1024<float>(o);
+  const float beta = static_cast<float>(a.beta), alpha = static_cast<float>(a.alpha);
+  const float inv_med = med != 0.f ? 1.f / med : 1.f;
+  float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    float v = o[k] * inv_med;
+    v = a.alpha_is_one ? v - 1.f : powf(v, alpha) - 1.f;
+    if (v < 0.f) v = 0.f;
+    const float gk = v * beta + lp[k * 32 + lane];
+    const float2 y = make_float2(T.re[k][lane] * gk, T.im[k][lane] * gk);
+    const float2 w = wp[(k * bi) & 31];
+    acc.x += y.x * w.x - y.y * w.y;
+    acc.y += y.x * w.y + y.y * w.x;
+  }
+  const float2 w = wp[(lane * bj) & 31];
+  float2 r = make_float2(acc.x * w.x - acc.y * w.y, acc.x * w.y + acc.y * w.x);
+  r.x = warp_sum(r.x);
+  r.y = warp_sum(r.y);
+  return r;
+}
+
+__global__ void __launch_bounds__(128) k_s3_clap(S3ClapArgs a, Twiddles32f tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ClapTile<float>* tiles = reinterpret_cast<ClapTile<float>*>(smem_raw);
+  float* lp = reinterpret_cast<float*>(tiles + 4);
+  float2* twf = reinterpret_cast<float2*>(lp + 1024);
+  float2* wp = twf + 16;  // e^{+2 pi i k / 32}, k < 32
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int i = tid; i < 1024; i += 128) lp[i] = static_cast<float>(a.low_pass[i]);
+  if (tid < 16) {
+    twf[tid] = tw.w[tid];
+    wp[tid] = make_float2(tw.w[tid].x, -tw.w[tid].y);
+    wp[tid + 16] = make_float2(-tw.w[tid].x, tw.w[tid].y);
+  }
+  float g7[7];
+#pragma unroll
+  for (int i = 0; i < 7; ++i) g7[i] = static_cast<float>(a.g7[i]);
+  const int M = a.M;
+  const int64_t ntask = a.n_jobs * a.ngroups;
+  for (int64_t task = blockIdx.x; task < ntask; task += gridDim.x) {
+    const int64_t job = task / a.ngroups;
+    const int g = static_cast<int>(task - job * a.ngroups);
+    const int i0 = a.jobs[4 * job], j0 = a.jobs[4 * job + 1], bi = a.jobs[4 * job + 2], bj = a.jobs[4 * job + 3];
+    const int c_warp = 4 * g + warp;
+    if (i0 < 0) {
+      // the 32-cell patch does not fit: the reference sets ph_patch2 to 0
+      if (lane == 0 && c_warp < M) a.job_out[job * M + c_warp] = make_float2(0.f, 0.f);
+      continue;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < 4 * 1024; idx += 128) {
+      const int pix = idx >> 2, q = idx & 3;
+      const int li = pix >> 5, lj = pix & 31;
+      const int c = 4 * g + q;
+      float2 v = make_float2(0.f, 0.f);
+      if (c < M) {
+        v = a.grid[(static_cast<int64_t>(i0 + li) * a.grid_cols + (j0 + lj)) * M + c];
+        if (isnan(v.x) || isnan(v.y)) v = make_float2(0.f, 0.f);
+        const bool own = li == bi && lj == bj;
+        const bool osf = c == 0 && abs(li - bi) <= a.slc_rad && abs(lj - bj) <= a.slc_rad;
+        if (own || osf) v = make_float2(0.f, 0.f);
+      }
+      tiles[q].re[li][lj] = v.x;
+      tiles[q].im[li][lj] = v.y;
+    }
+    __syncthreads();
+    if (c_warp < M) {
+      const float2 r = s3_patch_point(tiles[warp], lane, a, twf, wp, lp, g7, bi, bj);
+      if (lane == 0) a.job_out[job * M + c_warp] = make_float2(r.x * (1.f / 1024.f), r.y * (1.f / 1024.f));
+    }
+  }
+}
+
+size_t s3_clap_smem() { return 4 * sizeof(ClapTile<float>) + 1024 * sizeof(float) + 48 * sizeof(float2); }
+
+cudaError_t launch_s3_clap(const S3ClapArgs& a, const Twiddles32f& tf, int sm_count, cudaStream_t st) {
+  const int64_t ntask = a.n_jobs * a.ngroups;
+  if (ntask <= 0) return cudaSuccess;
+  const size_t sm = s3_clap_smem();
+  cudaError_t e = cudaFuncSetAttribute(k_s3_clap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_s3_clap, 128, sm);
+  if (e != cudaSuccess) return e;
+  const int64_t blocks = std::min<int64_t>(ntask, static_cast<int64_t>(sm_count) * std::max(per_sm, 1));
+  k_s3_clap<<<static_cast<unsigned>(blocks), 128, sm, st>>>(a, tf);
+  return cudaGetLastError();
+}
+
+// np.exp(-1j * x) in complex64: (cos x, -sin x)
+__device__ __forceinline__ float2 s3_cis_neg(float x) {
+  float s, c;
+  sincosf(x, &s, &c);
+  return make_float2(c, -s);
+}
+
+struct S3Fit {
+  float K, C, coh;
+};
+
+// _ps_topofit_refine_candidate (ported.py:2473-2508), float32, lanes over columns
+__device__ S3Fit s3_refine(const float2* cpx, const float* bp, int n, double den_lin, double coarse_k0, int lane) {
+  float K0 = static_cast<float>(coarse_k0);
+  float ox = 0.f, oy = 0.f;
+  for (int k = lane; k < n; k += 32) {
+    const float2 r = cmul_rn(cpx[k], s3_cis_neg(__fmul_rn(K0, bp[k])));
+    ox += r.x;
+    oy += r.y;
+  }
+  ox = warp_sum(ox);
+  oy = warp_sum(oy);
+  float mo = 0.f;
+  for (int k = lane; k < n; k += 32) {
+    const float2 r = cmul_rn(cpx[k], s3_cis_neg(__fmul_rn(K0, bp[k])));
+    const float2 q = cmul_rn(r, make_float2(ox, -oy));
+    const float wgt = hypotf(cpx[k].x, cpx[k].y);
+    mo += __fmul_rn(__fmul_rn(wgt, bp[k]), __fmul_rn(wgt, atan2f(q.y, q.x)));
+  }
+  mo = warp_sum(mo);
+  K0 = __fadd_rn(K0, __fdiv_rn(mo, static_cast<float>(den_lin)));
+  float mx = 0.f, my = 0.f, den = 0.f;
+  for (int k = lane; k < n; k += 32) {
+    const float2 r = cmul_rn(cpx[k], s3_cis_neg(__fmul_rn(K0, bp[k])));
+    mx += r.x;
+    my += r.y;
+    den += hypotf(r.x, r.y);
+  }
+  mx = warp_sum(mx);
+  my = warp_sum(my);
+  den = warp_sum(den);
+  if (den == 0.f) den = 1.f;
+  return {K0, atan2f(my, mx), hypotf(mx, my) / den};
+}
+
+// One warp per selected PS: psdph against the re-estimated patch phase, the
+// reference's invalid-row rule, then _ps_topofit_single with the near-max
+// candidate rule (tolerance 2e-4), refinement of every candidate and the
+// reference's choice among them.
+__global__ void __launch_bounds__(128) k_s3_fit(S3FitArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int T = 2 * a.n_half + 1;
+  const int nf = a.n_fit, M = a.M;
+  unsigned char* base = smem_raw + static_cast<size_t>(wib) * a.warp_smem;
+  float2* cpx = reinterpret_cast<float2*>(base);
+  float* bp = reinterpret_cast<float*>(cpx + nf);
+  float* tp = bp + nf;
+  float* ct = tp + nf;
+  const int64_t gw = static_cast<int64_t>(blockIdx.x) * 4 + wib;
+  const int64_t nw = static_cast<int64_t>(gridDim.x) * 4;
+  for (int64_t r = gw; r < a.n_sel; r += nw) {
+    const int job = a.job_of[r];
+    bool zero = false;
+    for (int c = lane; c < M; c += 32) {
+      const float2 pp = a.job_out[static_cast<int64_t>(job) * M + c];
+      a.ph_patch2[r * M + c] = pp;
+      a.ph_res2[r * M + c] = 0.f;
+      const float2 h = a.ph[r * M + c];
+      // psdph = ph * conj(ph_patch2) in f64 (exact products of f32 values)
+      const double re = static_cast<double>(h.x) * pp.x + static_cast<double>(h.y) * pp.y;
+      const double im = static_cast<double>(h.y) * pp.x - static_cast<double>(h.x) * pp.y;
+      if (re == 0.0 && im == 0.0) zero = true;
+    }
+    if (__any_sync(0xffffffffu, zero)) {
+      if (lane == 0) {
+        a.K2[r] = __longlong_as_double(0x7ff8000000000000LL);
+        a.coh2[r] = __longlong_as_double(0x7ff8000000000000LL);
+        a.C2[r] = 0.0;
+      }
+      continue;
+    }
+    float mn = __int_as_float(0x7f800000), mx = -mn;
+    for (int k = lane; k < nf; k += 32) {
+      const int c = a.fit[k];
+      const float2 pp = a.job_out[static_cast<int64_t>(job) * M + c];
+      const float2 h = a.ph[r * M + c];
+      const double re = static_cast<double>(h.x) * pp.x + static_cast<double>(h.y) * pp.y;
+      const double im = static_cast<double>(h.y) * pp.x - static_cast<double>(h.x) * pp.y;
+      const double mg = hypot(re, im);
+      cpx[k] = make_float2(static_cast<float>(re / mg), static_cast<float>(im / mg));
+      bp[k] = a.bp[r * M + c];
+      mn = fminf(mn, bp[k]);
+      mx = fmaxf(mx, bp[k]);
+    }
+    mn = -warp_max(-mn);
+    mx = warp_max(mx);
+    double range = static_cast<double>(__fsub_rn(mx, mn));
+    if (range == 0.0) range = 1.0;
+    const float rf = static_cast<float>(range), qp = 0.785398163397448309615f;
+    float den = 0.f, dl = 0.f;
+    for (int k = lane; k < nf; k += 32) {
+      tp[k] = __fmul_rn(__fdiv_rn(bp[k], rf), qp);
+      const float ab = hypotf(cpx[k].x, cpx[k].y);
+      const float wb = __fmul_rn(ab, bp[k]);
+      den += ab;
+      dl += __fmul_rn(wb, wb);
+    }
+    double denom = static_cast<double>(warp_sum(den));
+    double den_lin = static_cast<double>(warp_sum(dl));
+    if (denom == 0.0) denom = 1.0;
+    if (den_lin == 0.0) den_lin = 1.0;
+    __syncwarp();
+    // coherence of every trial, columns summed in order (the reference adds
+    // the rows of its (columns, trials) product one after another)
+    float cmax = -1.f;
+    for (int t = lane; t < T; t += 32) {
+      const float tm = static_cast<float>(t - a.n_half);
+      float sx = 0.f, sy = 0.f;
+      for (int k = 0; k < nf; ++k) {
+        const float2 p = cmul_rn(s3_cis_neg(__fmul_rn(tp[k], tm)), cpx[k]);
+        sx = __fadd_rn(sx, p.x);
+        sy = __fadd_rn(sy, p.y);
+      }
+      ct[t] = __fdiv_rn(hypotf(sx, sy), static_cast<float>(denom));
+      cmax = fmaxf(cmax, ct[t]);
+    }
+    cmax = warp_max(cmax);
+    __syncwarp();
+    // candidates in trial order: local maxima within 2e-4 of the maximum
+    int n_cand = 0, first = -1, last = -1, coarse_best = -1, refined_best = -1;
+    S3Fit best_fit{0.f, 0.f, -1.f};
+    float coarse_best_v = -1.f;
+    for (int t0 = 0; t0 < T; t0 += 32) {
+      const int t = t0 + lane;
+      bool cand = false;
+      if (t < T) {
+        const float v = ct[t];
+        bool lm;
+        if (T == 1) lm = true;
+        else if (t == 0) lm = v >= ct[1];
+        else if (t == T - 1) lm = v >= ct[T - 2];
+        else lm = v >= ct[t - 1] && v >= ct[t + 1];
+        cand = lm && static_cast<double>(v) >= static_cast<double>(cmax) - 2.0e-4;
+      }
+      unsigned bal = __ballot_sync(0xffffffffu, cand);
+      while (bal) {
+        const int tt = t0 + __ffs(bal) - 1;
+        bal &= bal - 1;
+        if (first < 0) first = tt;
+        last = tt;
+        ++n_cand;
+        if (ct[tt] > coarse_best_v) {
+          coarse_best_v = ct[tt];
+          coarse_best = tt;
+        }
+        const S3Fit f = s3_refine(cpx, bp, nf, den_lin, (3.14159265358979323846 / 4.0) / range * (tt - a.n_half), lane);
+        if (static_cast<double>(f.coh) > static_cast<double>(best_fit.coh)) {
+          best_fit = f;
+          refined_best = tt;
+        }
+      }
+    }
+    int pick = refined_best;
+    if (n_cand == 2 && first == 0 && last == T - 1) pick = coarse_best;
+    if (pick < 0) pick = coarse_best >= 0 ? coarse_best : 0;  // refined coherences all NaN
+    S3Fit f = best_fit;
+    if (pick != refined_best)
+      f = s3_refine(cpx, bp, nf, den_lin, (3.14159265358979323846 / 4.0) / range * (pick - a.n_half), lane);
+    for (int k = lane; k < nf; k += 32) {
+      const float2 res = cmul_rn(cpx[k], s3_cis_neg(__fmul_rn(f.K, bp[k])));
+      a.ph_res2[r * M + a.fit[k]] = atan2f(res.y, res.x);
+    }
+    if (lane == 0) {
+      a.K2[r] = static_cast<double>(f.K);
+      a.C2[r] = static_cast<double>(f.C);
+      a.coh2[r] = static_cast<double>(f.coh);
+    }
+    __syncwarp();
+  }
+}
+
+cudaError_t launch_s3_fit(const S3FitArgs& a, int sm_count, cudaStream_t st) {
+  if (a.n_sel <= 0) return cudaSuccess;
+  const size_t sm = 4 * a.warp_smem;
+  cudaError_t e = cudaFuncSetAttribute(k_s3_fit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_s3_fit, 128, sm);
+  if (e != cudaSuccess) return e;
+  const int64_t blocks =
+      std::min<int64_t>((a.n_sel + 3) / 4, static_cast<int64_t>(sm_count) * std::max(per_sm, 1));
+  k_s3_fit<<<static_cast<unsigned>(blocks), 128, sm, st>>>(a);
+  return cudaGetLastError();
+}
+
 // ============================================================== batches ===
 // Many patches, each iteration one launch per step over every active patch.
 // Work units are numbered patch after patch (prefix tables); a unit finds its

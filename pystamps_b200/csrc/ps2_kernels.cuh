@@ -104,6 +104,37 @@ struct FinalizeArgs {
   int force_continue;        // iterate past the stop rule (timing runs)
 };
 
+// --------------------------------------------------------------- stage 3 --
+struct S3ClapArgs {
+  const float2* grid;      // stage-2 ph_grid [rows, cols, M]
+  int grid_cols, M;
+  const int32_t* jobs;     // [n_jobs][4]: patch origin row, col (0-based; -1: no patch), PS cell in the patch
+  int64_t n_jobs;
+  int ngroups;             // ceil(M / 4)
+  int slc_rad;             // slc_osf - 1
+  int alpha_is_one;
+  double alpha, beta;
+  const double* low_pass;  // [32 * 32]
+  double g7[7];
+  float2* job_out;         // [n_jobs, M] filtered value at the PS cell
+};
+
+struct S3FitArgs {
+  const float2* ph;        // [n_sel, M] selected rows
+  const float* bp;         // [n_sel, M]
+  const int32_t* job_of;   // [n_sel]
+  const float2* job_out;   // [n_jobs, M]
+  const int32_t* fit;      // [n_fit] columns used by topofit
+  int n_fit, M, n_half;
+  int64_t n_sel;
+  size_t warp_smem;        // bytes of shared memory per warp
+  float2* ph_patch2;       // [n_sel, M]
+  double* K2;
+  double* C2;
+  double* coh2;
+  float* ph_res2;          // [n_sel, M]
+};
+
 // --------------------------------------------------------------- batches --
 // One patch of a batch: the single-patch arguments of every step.
 struct PatchDev {
@@ -179,6 +210,8 @@ cudaError_t launch_reduce_ab(const double* part, int n, double* out, cudaStream_
 size_t topofit_smem_bytes(int L, int mpad);
 cudaError_t topofit_geometry(const TopoArgs& a, int grid_cap, int* L_out, int* mpad_out, int* blocks_out);
 cudaError_t launch_batch_reset(const BatchArgs& b, cudaStream_t st);
+cudaError_t launch_s3_clap(const S3ClapArgs& a, const Twiddles32f& tf, int sm_count, cudaStream_t st);
+cudaError_t launch_s3_fit(const S3FitArgs& a, int sm_count, cudaStream_t st);
 cudaError_t launch_batch_bin(const BatchArgs& b, int64_t total, int sm_count, cudaStream_t st);
 cudaError_t launch_batch_clap(const BatchArgs& b, int64_t total, const Twiddles32f& tf, int sm_count,
                               cudaStream_t st);

@@ -11,7 +11,7 @@ HEADER = ROOT / "include" / "ps2cuda.h"
 
 def declared_functions():
     text = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\**\s*(ps2_[a-z_0-9]+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\**\s*(ps[23]_[a-z_0-9]+)\s*\(", text, re.M)))
 
 
 def test_header_declares_the_context_and_kernel_entry_points():
@@ -50,7 +50,8 @@ def test_struct_layouts_match_header():
     from pystamps_b200 import _lib
 
     for struct, cls in (("ps2_patch_desc", _lib.PatchDesc), ("ps2_outputs", _lib.Outputs),
-                        ("ps2_iter_stats", _lib.IterStats)):
+                        ("ps2_iter_stats", _lib.IterStats), ("ps3_reestimate_desc", _lib.S3Desc),
+                        ("ps3_reestimate_out", _lib.S3Out)):
         assert _field_names(struct) == [f for f, _ in cls._fields_], struct
 
 
@@ -74,3 +75,15 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setenv("PS2CUDA_LIB", str(tmp_path / "nope.so"))
     with pytest.raises(_lib.BackendUnavailableError):
         _lib.lib()
+
+
+def test_stage3_reestimate_rejects_bad_descriptors_without_a_device(cuda_lib):
+    from pystamps_b200 import _lib
+
+    d = _lib.S3Desc()
+    o = _lib.S3Out()
+    d.n_sel, d.n_ifg, d.clap_win, d.n_fit = 1, 4, 24, 4
+    assert cuda_lib.ps3_reestimate(ctypes.byref(d), ctypes.byref(o), 0) == -4  # clap_win must be 32
+    d.clap_win, d.n_fit = 32, 0
+    assert cuda_lib.ps3_reestimate(ctypes.byref(d), ctypes.byref(o), 0) == -1
+    assert b"n_fit" in cuda_lib.ps2_last_error()
