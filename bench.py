@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-stage3", action="store_true")
     return ap.parse_args()
 
 
@@ -204,6 +205,44 @@ def run_reference(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+def stage3_leg(ctx, prep, rank: int, cpu: bool = True) -> dict:
+    """Stage-3 re-estimate (ps3_reestimate) of the PS whose converged stage-2
+    coherence exceeds 0.3, timed end to end through the public call (host
+    arrays in and out); the oracle re-estimates a bounded sample of the same
+    rows on the host cores for the CPU figure."""
+    from pystamps_b200 import stage3
+
+    pm = ctx.download(["coh_ps", "ph_grid"])
+    sel = np.where(pm["coh_ps"] > 0.3)[0]
+    gij = np.rint(prep.grid_ij).astype(np.int64)
+    bp = np.asarray(prep.bperp, dtype=np.float32)
+    bp = np.broadcast_to(bp, (prep.n_ps, prep.n_ifg)) if bp.ndim == 1 else bp
+    fit = np.arange(prep.n_ifg)
+    ntw = float(np.float32(prep.n_trial_wraps))
+    kw = dict(clap_alpha=prep.clap_alpha, clap_beta=prep.clap_beta, low_pass=prep.low_pass, n_trial_wraps=ntw)
+    stage3.reestimate(pm["ph_grid"], gij, sel[:1000], prep.ph_nm, bp, fit, **kw)  # warm-up
+    ts = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        stage3.reestimate(pm["ph_grid"], gij, sel, prep.ph_nm, bp, fit, **kw)
+        ts.append(time.perf_counter() - t0)
+    t = min(ts)
+    out = {"selected_ps": int(sel.size), "n_ifg": prep.n_ifg, "seconds": t, "ps_per_s": sel.size / t,
+           "cells": int(np.unique(gij[sel, 0] * 100000 + gij[sel, 1]).size),
+           "what": "stage3.reestimate: gather rows + ps3_reestimate (H2D, patch CLAP per PS cell, stage-3 topofit, D2H)"}
+    if cpu and rank == 0:
+        from oracle import oracle as O
+
+        k = min(2000, sel.size)
+        t0 = time.perf_counter()
+        O.s3_reestimate(pm["ph_grid"], gij, sel[:k], prep.ph_nm, bp, fit, alpha=prep.clap_alpha,
+                        beta=prep.clap_beta, low_pass=prep.low_pass, n_trial_wraps=ntw)
+        tc = time.perf_counter() - t0
+        out["cpu_baseline"] = {"ps_per_s": k / tc, "cores": ncores(), "kind": "port",
+                               "sample": f"oracle re-estimate of {k} of the {sel.size} selected PS"}
+    return out
+
+
 # ------------------------------------------------------------- GPU leg ------
 def run_ours(args, rank: int, world: int, dist):
     import torch
@@ -322,6 +361,10 @@ def run_ours(args, rank: int, world: int, dist):
             t = float(tt.item())
         e2e_vals.append(world * n * m * st["i_loop"] / t)
         iters.append(st["i_loop"])
+    # ---------------- stage-3 re-estimate on the converged patch ---------------
+    stage3 = None
+    if not args.no_stage3 and e2e_vals:
+        stage3 = stage3_leg(ectx, prep, rank, cpu=not args.no_cpu)
     ectx.close()
     e2e = None if not e2e_vals else {"value": statistics.median(e2e_vals), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "iterations_per_step": iters,
@@ -378,6 +421,7 @@ def run_ours(args, rank: int, world: int, dist):
             "roofline": roofline, "roofline_bin": bin_roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clocks, "fp64_gpu": fp64,
             "fp32_over_fp64": (value / fp64["value"]) if fp64 else None, "precision_vs_fp64": prec,
+            "stage3_reestimate": stage3,
         }
         print(json.dumps(line), flush=True)
 
