@@ -642,20 +642,16 @@ cudaError_t launch_overlap(const OverlapArgs& a, bool fp64, cudaStream_t st) {
 constexpr float kQuarterPiF = 3.14159265358979323846f / 4.0f;  // Rust std::f32::consts::PI / 4.0
 
 // e^{-j x} for the re-anchoring points, |x| < ~1e3: Cody-Waite argument
-// reduction by pi/2 with a two-constant split of pi/2 (Cody & Waite, "Software
-// Manual for the Elementary Functions", 1980), then the hardware sin/cos
-// approximations on |r| <= pi/4 and the quadrant rotation.
+// reduction by 2 pi with a two-constant split of 2 pi (Cody & Waite, "Software
+// Manual for the Elementary Functions", 1980) to |r| <= pi, then the hardware
+// sin/cos approximations (absolute error ~4e-7 on that range; a reduction to
+// pi/4 with a quadrant rotation buys no accuracy there and costs a conversion
+// and four selects per call).
 __device__ __forceinline__ float2 cis_neg_anchor(float x) {
-  const float k = rintf(x * 0.636619772367581343f);
-  float r = fmaf(-k, 1.57079637050628662109375f, x);
-  r = fmaf(-k, -4.37113900018624283e-8f, r);
-  const float sr = __sinf(r), cr = __cosf(r);
-  const int q = static_cast<int>(k) & 3;
-  const float sx0 = (q & 1) ? cr : sr;
-  const float cx0 = (q & 1) ? sr : cr;
-  const float sx = (q & 2) ? -sx0 : sx0;
-  const float cx = ((q + 1) & 2) ? -cx0 : cx0;
-  return make_float2(cx, -sx);
+  const float k = rintf(x * 0.159154943091895335769f);
+  float r = fmaf(-k, 6.28318548202514648438f, x);
+  r = fmaf(-k, -1.74845553146951715e-7f, r);
+  return make_float2(__cosf(r), -__sinf(r));
 }
 
 template <int L>
