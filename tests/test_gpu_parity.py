@@ -226,9 +226,10 @@ def _teacher_forced(S, oracle, patch, iterations=5):
             n_ties += int(tie.sum())
             good = ~tie & ~np.isnan(fr.K)
             np.testing.assert_array_equal(np.isnan(g["K_ps"]), np.isnan(fr.K))
-            assert np.abs(g["coh_ps"] - fr.coh)[good].max() <= 1e-5, it
-            dK = np.abs(g["K_ps"] - fr.K) / np.maximum(np.abs(fr.K), 1e-3)
-            assert dK[good].max() <= K_REL_TOL, it
+            if good.any():  # with very few interferograms every row can be a tie
+                assert np.abs(g["coh_ps"] - fr.coh)[good].max() <= 1e-5, it
+                dK = np.abs(g["K_ps"] - fr.K) / np.maximum(np.abs(fr.K), 1e-3)
+                assert dK[good].max() <= K_REL_TOL, it
             np.testing.assert_array_equal(g["N_opt"], fr.N_opt)
             prev = g
     return n_ties
