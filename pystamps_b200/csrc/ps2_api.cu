@@ -1620,38 +1620,98 @@ int ps2_batch_run(ps2_ctx* const* ctxs, int64_t n, ps2_iter_stats* last) {
   std::vector<int64_t> before(static_cast<size_t>(n));
   for (int64_t p = 0; p < n; ++p) before[p] = ctxs[p]->last.i_loop;
   const int lanes_of[4] = {4, 8, 16, 32};
-  int64_t launched = 0;
-  CK(cudaEventRecord(c0->evpool[0], st));
-  for (int64_t k = 0; k < cap_iter; ++k) {
+  int per_iter = 5;  // reset, bin, clap, overlap, finalize + one topofit per lane class
+  for (int cls = 0; cls < 4; ++cls) per_iter += plan.units[cls].empty() ? 0 : 1;
+  auto enqueue = [&]() -> int {
     CK(launch_batch_reset(b, st));
     CK(launch_batch_bin(b, plan.bin_prefix.back(), c0->sm_count, st));
     CK(launch_batch_clap(b, plan.clap_prefix.back(), c0->twf, c0->sm_count, st));
     CK(launch_batch_overlap(b, plan.ov_prefix.back(), c0->sm_count, st));
-    launched += 4;
     for (int cls = 0; cls < 4; ++cls) {
       if (plan.units[cls].empty()) continue;
       CK(launch_batch_topofit(b, lanes_of[cls], reinterpret_cast<const int32_t*>(base + o_cls[cls]),
                               static_cast<int>(plan.units[cls].size() / 2), plan.mpad_max[cls], c0->sm_count, st));
-      ++launched;
     }
     CK(launch_batch_finalize(b, st));
-    ++launched;
-    CK(cudaMemcpyAsync(c0->h_active, b.n_active, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    if (*c0->h_active == 0) break;
+    return PS2_OK;
+  };
+  // The loop as one graph launch: a WHILE conditional node whose body is one
+  // batched iteration followed by k_batch_continue (continue while any patch
+  // iterates). Eager launches with a host check per iteration if capture is
+  // refused or PS2_NO_GRAPH is set.
+  const char* ng = getenv("PS2_NO_GRAPH");
+  bool use_graph = !(ng != nullptr && ng[0] != '\0' && ng[0] != '0');
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  if (use_graph) {
+    bool ok = cudaGraphCreate(&graph, 0) == cudaSuccess;
+    cudaGraphConditionalHandle h{};
+    cudaGraphNodeParams gp{};
+    if (ok) ok = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+      gp.type = cudaGraphNodeTypeConditional;
+      gp.conditional.handle = h;
+      gp.conditional.type = cudaGraphCondTypeWhile;
+      gp.conditional.size = 1;
+      cudaGraphNode_t node;
+      ok = cudaGraphAddNode(&node, graph, nullptr, 0, &gp) == cudaSuccess;
+    }
+    if (ok) {
+      ok = cudaStreamBeginCaptureToGraph(st, gp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      if (ok) {
+        const int rc_e = enqueue();
+        const bool ok_c = rc_e == PS2_OK && launch_batch_continue(h, b.n_active, st) == cudaSuccess;
+        cudaGraph_t captured = nullptr;
+        const bool ok_end = cudaStreamEndCapture(st, &captured) == cudaSuccess;
+        ok = ok_c && ok_end;
+      }
+    }
+    if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (!ok) {
+      if (exec) cudaGraphExecDestroy(exec);
+      if (graph) cudaGraphDestroy(graph);
+      exec = nullptr;
+      graph = nullptr;
+      cudaGetLastError();
+      use_graph = false;
+    }
+  }
+  CK(cudaEventRecord(c0->evpool[0], st));
+  if (use_graph) {
+    const cudaError_t e1 = cudaGraphLaunch(exec, st);
+    const cudaError_t e2 = cudaStreamSynchronize(st);
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    CK(e1);
+    CK(e2);
+  } else {
+    for (int64_t k = 0; k < cap_iter; ++k) {
+      rc = enqueue();
+      if (rc) return rc;
+      CK(cudaMemcpyAsync(c0->h_active, b.n_active, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (*c0->h_active == 0) break;
+    }
   }
   CK(cudaEventRecord(c0->evpool[1], st));
   CK(cudaStreamSynchronize(st));
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, c0->evpool[0], c0->evpool[1]));
+  int64_t iterations = 0;
   for (int64_t p = 0; p < n; ++p) {
     ps2_ctx* c = ctxs[p];
     CK(cudaMemcpy(c->h_stats, c->stats.p, 8 * sizeof(double), cudaMemcpyDeviceToHost));
     fill_stats(c->h_stats, &c->last);
+    iterations = std::max<int64_t>(iterations, c->last.i_loop - before[p]);
+  }
+  const int64_t launched = iterations * (per_iter + (use_graph ? 1 : 0));
+  for (int64_t p = 0; p < n; ++p) {
+    ps2_ctx* c = ctxs[p];
     c->iters_done += c->last.i_loop - before[p];
     c->launches = launched;
     c->last_ms = ms;
-    c->last_run_graph = false;
+    c->last_run_graph = use_graph;
     for (int i = 0; i < 4; ++i) c->kernel_ms[i] = 0.0;
     if (last) last[p] = c->last;
   }

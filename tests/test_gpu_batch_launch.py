@@ -47,8 +47,9 @@ def test_batch_matches_each_patch_alone(cuda_lib):
         assert st["i_loop"] == a["stats"]["i_loop"] and st["stop"] == 1
         for key in KEYS:
             np.testing.assert_array_equal(t[key], a[key], err_msg=f"patch {k} {key}")
-    # per iteration: reset, bin, clap, overlap, topofit per lane class (2 here), finalize
-    assert n_launch == 7 * max(iters)
+    # per iteration: reset, bin, clap, overlap, topofit per lane class (2 here), finalize,
+    # and the graph's loop-condition kernel
+    assert n_launch == 8 * max(iters)
 
 
 def test_batch_rerun_after_reset_is_identical(cuda_lib):
@@ -84,3 +85,21 @@ def test_batch_rejects_bad_input(cuda_lib):
         arr = (ctypes.c_void_p * 2)(b.ctxs[0]._ctx.value, b.ctxs[0]._ctx.value)
         with pytest.raises(_lib.Stage2CudaError):
             _lib.check(_lib.lib().ps2_batch_run(arr, ctypes.c_int64(2), None))
+
+
+def test_batch_eager_loop_matches_graph_loop(cuda_lib, monkeypatch):
+    from pystamps_b200 import batch
+
+    preps = _patches()[:3]
+    with batch.Batch(preps) as b:
+        b.run()
+        graph = b.download(("K_ps", "coh_ps", "N_opt"))
+        b.reset()
+        monkeypatch.setenv("PS2_NO_GRAPH", "1")
+        b.run()
+        eager = b.download(("K_ps", "coh_ps", "N_opt"))
+        assert b.launch_count() == 7 * max(r["i_loop"] for r in eager)
+    for a, c in zip(graph, eager):
+        assert a["i_loop"] == c["i_loop"]
+        for k in ("K_ps", "coh_ps", "N_opt"):
+            np.testing.assert_array_equal(a[k], c[k])
