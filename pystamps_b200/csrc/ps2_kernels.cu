@@ -198,12 +198,30 @@ __device__ __forceinline__ void fft32(typename CT<R>::C (&x)[32], const typename
 }
 
 // ================================================================== CLAP ==
-template <typename R>
-struct ClapTile {
+// One warp's 32x32 working set (33-column rows avoid bank conflicts along
+// columns). PAD staggers consecutive tiles: 8 floats for 4 tiles per block, 4
+// for 8, so the block's interleaved loads (all tiles' ifgs of one cell at once)
+// hit distinct banks.
+template <typename R, int PAD>
+struct ClapTileT {
   R re[32][33];
   R im[32][33];
   R hs[32][33];
-  R pad[8];  // consecutive tiles start 8 banks apart (the 4-ifg loads hit 4 tiles at once)
+  R pad[PAD];
+};
+template <typename R>
+using ClapTile = ClapTileT<R, 8>;
+
+// warps per CLAP block and the matching tile stagger
+template <int NW>
+struct ClapShape;
+template <>
+struct ClapShape<4> {
+  static constexpr int kPad = 8;
+};
+template <>
+struct ClapShape<8> {
+  static constexpr int kPad = 4;
 };
 
 __device__ __forceinline__ uint32_t to_bits(float v) { return __float_as_uint(v); }
@@ -368,8 +386,8 @@ __device__ __noinline__ void fft_pass(R (*re)[33], R (*im)[33], const typename C
 // One window of one interferogram, computed by one warp in its tile.
 // On entry the tile holds the 24x24 window zero-padded to 32x32; on exit rows
 // and columns < n_win hold the filtered values times the pyramid weight / 1024.
-template <typename R>
-__device__ __forceinline__ void clap_window_warp(ClapTile<R>& T, const int lane, const ClapArgs& a,
+template <typename R, typename Tile>
+__device__ __forceinline__ void clap_window_warp(Tile& T, const int lane, const ClapArgs& a,
                                                  const typename CT<R>::C* twf, const typename CT<R>::C* twi,
                                                  const R* lp, const R* wt, const R (&g7)[7], const int rs,
                                                  const int cs) {
@@ -447,19 +465,26 @@ __device__ __forceinline__ void clap_consts(const ClapArgs& a, R* lp, R* wt) {
   for (int i = threadIdx.x; i < nw2; i += blockDim.x) wt[i] = static_cast<R>(a.wscaled[i]);
 }
 
-// One block-task of CLAP: window task / (Mp/4), interferograms 4 * (task % (Mp/4)) + warp.
-template <typename R>
-__device__ __forceinline__ void clap_task(const ClapArgs& a, const int64_t task, ClapTile<R>* tiles,
-                                          const typename CT<R>::C* twf, const typename CT<R>::C* twi, const R* lp,
-                                          const R* wt, const R (&g7)[7]) {
+// One block-task of CLAP: window task / ngroups, interferograms
+// NW * (task % ngroups) + warp, ngroups = ceil(Mp / NW).
+template <typename R, int NW>
+__device__ __forceinline__ int clap_groups(const ClapArgs& a) {
+  return (a.Mp + NW - 1) / NW;
+}
+
+template <typename R, int NW>
+__device__ __forceinline__ void clap_task(const ClapArgs& a, const int64_t task,
+                                          ClapTileT<R, ClapShape<NW>::kPad>* tiles, const typename CT<R>::C* twf,
+                                          const typename CT<R>::C* twi, const R* lp, const R* wt, const R (&g7)[7]) {
   using C = typename CT<R>::C;
+  constexpr int NT = 32 * NW;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nw = a.n_win, nw2 = nw * nw;
   const int n_inc = nw / 4 > 1 ? nw / 4 : 1;
-  const int ngroups = a.Mp / 4;
+  const int ngroups = clap_groups<R, NW>(a);
   const C* __restrict__ grid = static_cast<const C*>(a.grid);
   C* __restrict__ out = static_cast<C*>(a.win_out);
-  ClapTile<R>& T = tiles[warp];
+  auto& T = tiles[warp];
   {
     const int64_t wi = task / ngroups;
     const int g = static_cast<int>(task - wi * ngroups);
@@ -476,18 +501,18 @@ __device__ __forceinline__ void clap_task(const ClapArgs& a, const int64_t task,
       j1 = a.n_j - nw;
     }
     __syncthreads();
-    // zero the padding of the four tiles, load the windows (NaN -> 0)
-    for (int idx = tid; idx < 4 * 32 * 32; idx += 128) {
+    // zero the padding of the tiles, load the windows (NaN -> 0)
+    for (int idx = tid; idx < NW * 32 * 32; idx += NT) {
       const int q = idx >> 10, e = idx & 1023, r = e >> 5, cc = e & 31;
       if (r >= nw || cc >= nw) {
         tiles[q].re[r][cc] = R(0);
         tiles[q].im[r][cc] = R(0);
       }
     }
-    for (int idx = tid; idx < nw2 * 4; idx += 128) {
-      const int pix = idx >> 2, q = idx & 3;
+    for (int idx = tid; idx < nw2 * NW; idx += NT) {
+      const int pix = idx / NW, q = idx % NW;
       const int li = pix / nw, lj = pix - li * nw;
-      const int c = 4 * g + q;
+      const int c = NW * g + q;
       C v = mk(R(0), R(0));
       if (c < a.M) {
         v = grid[(static_cast<int64_t>(i1 + li) * a.n_j + (j1 + lj)) * a.Mp + c];
@@ -497,31 +522,32 @@ __device__ __forceinline__ void clap_task(const ClapArgs& a, const int64_t task,
       tiles[q].im[li][lj] = v.y;
     }
     __syncthreads();
-    if (4 * g + warp < a.M) clap_window_warp<R>(T, lane, a, twf, twi, lp, wt, g7, rs, cs);
+    if (NW * g + warp < a.M) clap_window_warp<R>(T, lane, a, twf, twi, lp, wt, g7, rs, cs);
     __syncthreads();
-    for (int idx = tid; idx < nw2 * 4; idx += 128) {
-      const int pix = idx >> 2, q = idx & 3;
+    for (int idx = tid; idx < nw2 * NW; idx += NT) {
+      const int pix = idx / NW, q = idx % NW;
       const int li = pix / nw, lj = pix - li * nw;
-      out[(wi * nw2 + pix) * a.Mp + 4 * g + q] = mk(tiles[q].re[li][lj], tiles[q].im[li][lj]);
+      const int c = NW * g + q;
+      if (c < a.Mp) out[(wi * nw2 + pix) * a.Mp + c] = mk(tiles[q].re[li][lj], tiles[q].im[li][lj]);
     }
   }
 }
 
-// shared-memory carve-up of a CLAP block: 4 tiles, low-pass, weights, twiddles
-template <typename R>
+// shared-memory carve-up of a CLAP block: NW tiles, low-pass, weights, twiddles
+template <typename R, int NW>
 struct ClapSmem {
-  ClapTile<R>* tiles;
+  ClapTileT<R, ClapShape<NW>::kPad>* tiles;
   R* lp;
   R* wt;
   typename CT<R>::C* twf;
   typename CT<R>::C* twi;
 };
 
-template <typename R>
-__device__ __forceinline__ ClapSmem<R> clap_smem(unsigned char* raw, const typename CT<R>::Tw& tw) {
-  ClapSmem<R> m;
-  m.tiles = reinterpret_cast<ClapTile<R>*>(raw);
-  m.lp = reinterpret_cast<R*>(m.tiles + 4);
+template <typename R, int NW>
+__device__ __forceinline__ ClapSmem<R, NW> clap_smem(unsigned char* raw, const typename CT<R>::Tw& tw) {
+  ClapSmem<R, NW> m;
+  m.tiles = reinterpret_cast<ClapTileT<R, ClapShape<NW>::kPad>*>(raw);
+  m.lp = reinterpret_cast<R*>(m.tiles + NW);
   m.wt = m.lp + 1024;
   m.twf = reinterpret_cast<typename CT<R>::C*>(m.wt + 1024);
   m.twi = m.twf + 16;
@@ -532,46 +558,44 @@ __device__ __forceinline__ ClapSmem<R> clap_smem(unsigned char* raw, const typen
   return m;
 }
 
-template <typename R>
-__global__ void __launch_bounds__(128) k_clap(ClapArgs a, typename CT<R>::Tw tw) {
+template <typename R, int NW>
+__global__ void __launch_bounds__(32 * NW) k_clap(ClapArgs a, typename CT<R>::Tw tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const ClapSmem<R> m = clap_smem<R>(smem_raw, tw);
+  const ClapSmem<R, NW> m = clap_smem<R, NW>(smem_raw, tw);
   clap_consts<R>(a, m.lp, m.wt);
   R g7[7];
 #pragma unroll
   for (int i = 0; i < 7; ++i) g7[i] = static_cast<R>(a.g7[i]);
-  const int64_t ntask = static_cast<int64_t>(a.nwi) * a.nwj * (a.Mp / 4);
+  const int64_t ntask = static_cast<int64_t>(a.nwi) * a.nwj * clap_groups<R, NW>(a);
   for (int64_t task = blockIdx.x; task < ntask; task += gridDim.x)
-    clap_task<R>(a, task, m.tiles, m.twf, m.twi, m.lp, m.wt, g7);
+    clap_task<R, NW>(a, task, m.tiles, m.twf, m.twi, m.lp, m.wt, g7);
 }
 
-template <typename R>
+template <typename R, int NW>
 static size_t clap_smem_bytes() {
-  return 4 * sizeof(ClapTile<R>) + (1024 + 1024) * sizeof(R) + 32 * 2 * sizeof(R);
+  return NW * sizeof(ClapTileT<R, ClapShape<NW>::kPad>) + (1024 + 1024) * sizeof(R) + 32 * 2 * sizeof(R);
 }
 
+template <typename R, int NW>
+static cudaError_t launch_clap_nw(const ClapArgs& a, const typename CT<R>::Tw& tw, int sm_count, cudaStream_t st) {
+  const int64_t ntask = static_cast<int64_t>(a.nwi) * a.nwj * ((a.Mp + NW - 1) / NW);
+  if (ntask <= 0) return cudaSuccess;
+  const size_t sm = clap_smem_bytes<R, NW>();
+  cudaError_t e = cudaFuncSetAttribute(k_clap<R, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clap<R, NW>, 32 * NW, sm);
+  if (e != cudaSuccess) return e;
+  const int64_t blocks = std::min<int64_t>(ntask, static_cast<int64_t>(sm_count) * (per_sm > 0 ? per_sm : 1));
+  k_clap<R, NW><<<static_cast<unsigned>(blocks), 32 * NW, sm, st>>>(a, tw);
+  return cudaGetLastError();
+}
+
+// FP32: 8 warps per block (16 resident warps per SM, shared memory bound);
+// FP64: 4 (its tiles are twice the size)
 cudaError_t launch_clap(const ClapArgs& a, bool fp64, const Twiddles32f& tf, const Twiddles32d& td, int sm_count,
                         cudaStream_t st) {
-  const int64_t ntask = static_cast<int64_t>(a.nwi) * a.nwj * (a.Mp / 4);
-  if (ntask <= 0) return cudaSuccess;
-  if (fp64) {
-    const size_t sm = clap_smem_bytes<double>();
-    cudaError_t e = cudaFuncSetAttribute(k_clap<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clap<double>, 128, sm);
-    int64_t blocks = std::min<int64_t>(ntask, static_cast<int64_t>(sm_count) * (per_sm > 0 ? per_sm : 1));
-    k_clap<double><<<static_cast<unsigned>(blocks), 128, sm, st>>>(a, td);
-  } else {
-    const size_t sm = clap_smem_bytes<float>();
-    cudaError_t e = cudaFuncSetAttribute(k_clap<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clap<float>, 128, sm);
-    int64_t blocks = std::min<int64_t>(ntask, static_cast<int64_t>(sm_count) * (per_sm > 0 ? per_sm : 1));
-    k_clap<float><<<static_cast<unsigned>(blocks), 128, sm, st>>>(a, tf);
-  }
-  return cudaGetLastError();
+  return fp64 ? launch_clap_nw<double, 4>(a, td, sm_count, st) : launch_clap_nw<float, 8>(a, tf, sm_count, st);
 }
 
 // Overlap-add as a gather: cell (i, j) sums the windows that cover it, in the
@@ -1973,7 +1997,7 @@ __global__ void __launch_bounds__(256) k_batch_bin(BatchArgs b) {
 
 __global__ void __launch_bounds__(128) k_batch_clap(BatchArgs b, Twiddles32f tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const ClapSmem<float> m = clap_smem<float>(smem_raw, tw);
+  const ClapSmem<float, 4> m = clap_smem<float, 4>(smem_raw, tw);
   float g7[7];
   int cur = -1;
   const int64_t total = b.clap_prefix[b.P];
@@ -1988,7 +2012,7 @@ __global__ void __launch_bounds__(128) k_batch_clap(BatchArgs b, Twiddles32f tw)
       for (int i = 0; i < 7; ++i) g7[i] = static_cast<float>(a.g7[i]);
       cur = p;
     }
-    clap_task<float>(a, u - b.clap_prefix[p], m.tiles, m.twf, m.twi, m.lp, m.wt, g7);
+    clap_task<float, 4>(a, u - b.clap_prefix[p], m.tiles, m.twf, m.twi, m.lp, m.wt, g7);
   }
 }
 
@@ -2046,7 +2070,7 @@ cudaError_t launch_batch_bin(const BatchArgs& b, int64_t total, int sm_count, cu
 cudaError_t launch_batch_clap(const BatchArgs& b, int64_t total, const Twiddles32f& tf, int sm_count,
                               cudaStream_t st) {
   if (total <= 0) return cudaSuccess;
-  const size_t sm = clap_smem_bytes<float>();
+  const size_t sm = clap_smem_bytes<float, 4>();
   cudaError_t e = cudaFuncSetAttribute(k_batch_clap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
