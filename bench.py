@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-stage3", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     return ap.parse_args()
 
 
@@ -203,6 +204,43 @@ def run_reference(args, rank: int, world: int):
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def adjoint_leg(prep, dev: int) -> dict:
+    """ps2_coherence_forward / _backward (the torch.autograd.Function's two
+    calls) on the workload, FP32, timed with CUDA events on the current
+    stream: ms per call and PS x ifg per second."""
+    import torch
+
+    from pystamps_b200 import autograd as AG
+
+    cmap = AG.CoherenceMap(prep, dev)
+    try:
+        d = torch.device("cuda", dev)
+        ph = torch.from_numpy(np.ascontiguousarray(prep.ph_nm, dtype=np.complex64)).to(d)
+        K = torch.zeros(prep.n_ps, dtype=torch.float32, device=d)
+        w = torch.from_numpy(np.asarray(prep.weight0, dtype=np.float32)).to(d)
+        g = torch.ones(prep.n_ps, dtype=torch.float32, device=d)
+        for _ in range(2):
+            cmap.forward(ph, K, w, prep.clap_alpha, prep.clap_beta)
+            cmap.backward(ph, K, w, prep.clap_alpha, prep.clap_beta, g)
+        out = {}
+        for name, fn in (("forward", lambda: cmap.forward(ph, K, w, prep.clap_alpha, prep.clap_beta)),
+                         ("backward", lambda: cmap.backward(ph, K, w, prep.clap_alpha, prep.clap_beta, g))):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(3):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / 3
+            out[name + "_ms"] = ms
+            out[name + "_ps_ifg_per_s"] = prep.n_ps * prep.n_ifg / (ms / 1e3)
+        out["what"] = "FP32 coherence map with K given: bin, CLAP, resample, coherence; backward recomputes the forward"
+        return out
+    finally:
+        cmap.close()
 
 
 def stage3_leg(ctx, prep, rank: int, cpu: bool = True) -> dict:
@@ -361,6 +399,10 @@ def run_ours(args, rank: int, world: int, dist):
             t = float(tt.item())
         e2e_vals.append(world * n * m * st["i_loop"] / t)
         iters.append(st["i_loop"])
+    # ---------------- adjoint of the coherence (forward + backward) ------------
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_leg(prep, dev)
     # ---------------- stage-3 re-estimate on the converged patch ---------------
     stage3 = None
     if not args.no_stage3 and e2e_vals:
@@ -421,7 +463,7 @@ def run_ours(args, rank: int, world: int, dist):
             "roofline": roofline, "roofline_bin": bin_roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clocks, "fp64_gpu": fp64,
             "fp32_over_fp64": (value / fp64["value"]) if fp64 else None, "precision_vs_fp64": prec,
-            "stage3_reestimate": stage3,
+            "stage3_reestimate": stage3, "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
 

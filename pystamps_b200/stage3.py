@@ -261,3 +261,75 @@ def select_ps(pm: dict, *, ph, bperp_mat, bperp, D_A, xy, master_ix: int, ifg_in
     return {"ix": ix0 + 1, "keep_ix": keep, "ph_patch2": r["ph_patch2"], "ph_res2": r["ph_res2"],
             "K_ps2": r["K_ps2"], "C_ps2": r["C_ps2"], "coh_ps2": r["coh_ps2"], "coh_thresh": thresh_all[ix0],
             "coh_thresh_coeffs": coeffs, "max_percent_rand": mpr}
+
+
+# --------------------------------------------------------------- MAT I/O ----
+SELECT_DEFAULTS = {"select_method": "PERCENT", "percent_rand": 1.0, "density_rand": 1.0, "gamma_stdev_reject": 0.0,
+                   "slc_osf": 1.0, "clap_win": 32.0, "clap_alpha": 1.0, "clap_beta": 0.3,
+                   "small_baseline_flag": "n"}
+
+
+def ifg_index_for_selection(n_ifg: int, master_ix: int, small_baseline: bool, drop=()) -> np.ndarray:
+    """_ifg_index_for_selection (ported.py:2755-2764): 1-based interferograms
+    kept for the selection, renumbered after the master column is removed."""
+    drop = {int(v) for v in np.asarray(drop).reshape(-1)}
+    ifg = [i for i in range(1, n_ifg + 1) if i not in drop]
+    if not small_baseline:
+        ifg = [i for i in ifg if i != master_ix]
+        ifg = [i - 1 if i > master_ix else i for i in ifg]
+    return np.asarray(ifg, dtype=np.float64)
+
+
+def stage3_select_ps(patch_dir, device: int = 0) -> str:
+    """Drop-in for ported.stage3_select_ps (ported.py:4328-4620): reads
+    ps1/ph1/bp1/da1/pm1 and the parms, selects with the re-estimate on the GPU,
+    writes select1.mat with the reference's variables and returns its summary
+    line."""
+    from scipy.io import loadmat, savemat
+
+    from .stage2 import _resolve_parms, _scalar
+
+    patch_dir = Path(patch_dir)
+    ps = loadmat(patch_dir / "ps1.mat")
+    pm_raw = loadmat(patch_dir / "pm1.mat")
+    n_ps = int(round(float(_scalar(ps, "n_ps", 0.0))))
+    if n_ps <= 0:
+        raise Stage3Error("ps1.mat missing valid n_ps")
+    parms = dict(SELECT_DEFAULTS)
+    pf = _resolve_parms(patch_dir)
+    drop = ()
+    if pf is not None:
+        raw = loadmat(pf)
+        for k, v in SELECT_DEFAULTS.items():
+            if k in raw:
+                parms[k] = _scalar(raw, k, v)
+        if "drop_ifg_index" in raw:
+            drop = np.asarray(raw["drop_ifg_index"]).reshape(-1)
+    ph = np.asarray(loadmat(patch_dir / "ph1.mat")["ph"])
+    if ph.shape[0] != n_ps and ph.shape[1] == n_ps:
+        ph = ph.T
+    bperp_mat = np.asarray(loadmat(patch_dir / "bp1.mat")["bperp_mat"], dtype=np.float64)
+    D_A = None
+    if (patch_dir / "da1.mat").exists():
+        D_A = np.asarray(loadmat(patch_dir / "da1.mat")["D_A"], dtype=np.float64).reshape(-1)
+    master_ix = int(round(float(_scalar(ps, "master_ix", 1.0))))
+    sb = str(parms["small_baseline_flag"]).lower() == "y"
+    n_ifg = int(round(float(_scalar(ps, "n_ifg", ph.shape[1]))))
+    ifg_index = ifg_index_for_selection(n_ifg, master_ix, sb, drop)
+    pm = {k: pm_raw[k] for k in ("coh_ps", "K_ps", "C_ps", "ph_patch", "ph_res", "ph_grid", "grid_ij", "Nr",
+                                 "coh_bins", "low_pass", "n_trial_wraps") if k in pm_raw}
+    out = select_ps(pm, ph=ph, bperp_mat=bperp_mat, bperp=ps["bperp"], D_A=D_A, xy=ps.get("xy"),
+                    master_ix=master_ix, ifg_index=ifg_index, parms=parms, device=device)
+    col = lambda v, dt: np.asarray(v, dtype=dt).reshape(-1, 1)  # noqa: E731
+    savemat(patch_dir / "select1.mat", {
+        "ix": col(out["ix"], np.float64), "keep_ix": col(out["keep_ix"], np.bool_),
+        "ph_patch2": out["ph_patch2"].astype(np.complex64), "ph_res2": out["ph_res2"],
+        "K_ps2": col(out["K_ps2"], np.float64), "C_ps2": col(out["C_ps2"], np.float64),
+        "coh_ps2": col(out["coh_ps2"], np.float64), "coh_thresh": col(out["coh_thresh"], np.float64),
+        "coh_thresh_coeffs": np.asarray(out["coh_thresh_coeffs"], dtype=np.float64),
+        "clap_alpha": float(parms["clap_alpha"]), "clap_beta": float(parms["clap_beta"]),
+        "n_win": float(parms["clap_win"]), "max_percent_rand": np.float32(out["max_percent_rand"]),
+        "gamma_stdev_reject": float(parms["gamma_stdev_reject"]),
+        "small_baseline_flag": str(parms["small_baseline_flag"]), "ifg_index": ifg_index.reshape(1, -1),
+    })
+    return f"Stage 3 selected {out['ix'].size} PS"

@@ -124,3 +124,30 @@ def test_reestimate_matches_oracle_on_a_larger_selection(cuda_lib, oracle):
     for i in first[:50]:
         same = np.where(cells == cells[i])[0]
         assert np.all(g["ph_patch2"][same] == g["ph_patch2"][i])
+
+
+def test_stage3_select_ps_on_a_patch_directory(cuda_lib, golden, tmp_path):
+    """MAT files in, select1.mat out, like the reference's stage3_select_ps."""
+    from scipy.io import loadmat, savemat
+
+    from pystamps_b200 import stage3
+
+    sel = golden("stage3_select.npz")
+    n = sel["ph"].shape[0]
+    savemat(tmp_path / "ps1.mat", {"n_ps": float(n), "n_ifg": float(sel["ph"].shape[1]), "master_ix": 1.0,
+                                   "bperp": sel["bperp"].reshape(1, -1), "xy": sel["xy"]})
+    savemat(tmp_path / "ph1.mat", {"ph": sel["ph"]})
+    savemat(tmp_path / "bp1.mat", {"bperp_mat": sel["bperp_mat"]})
+    savemat(tmp_path / "da1.mat", {"D_A": sel["D_A"].reshape(-1, 1)})
+    savemat(tmp_path / "parms.mat", {"select_method": "DENSITY", "density_rand": 20.0, "slc_osf": 1.0,
+                                     "gamma_stdev_reject": 0.0, "clap_alpha": 1.0, "clap_beta": 0.3,
+                                     "clap_win": 32.0, "small_baseline_flag": "n"})
+    savemat(tmp_path / "pm1.mat", {k[3:]: sel[k] for k in sel.files if k.startswith("pm_")})
+    msg = stage3.stage3_select_ps(tmp_path)
+    out = loadmat(tmp_path / "select1.mat")
+    assert msg == f"Stage 3 selected {sel['sel_ix'].size} PS"
+    np.testing.assert_array_equal(out["ix"].ravel(), sel["sel_ix"].ravel())
+    np.testing.assert_array_equal(out["ifg_index"].ravel(), sel["sel_ifg_index"].ravel())
+    assert int((out["keep_ix"].ravel().astype(bool) != sel["sel_keep_ix"].ravel().astype(bool)).sum()) <= 3
+    np.testing.assert_allclose(out["coh_thresh"].ravel(), sel["sel_coh_thresh"].ravel(), rtol=1e-6)
+    assert float(out["max_percent_rand"].ravel()[0]) == pytest.approx(float(sel["sel_max_percent_rand"].ravel()[0]))
