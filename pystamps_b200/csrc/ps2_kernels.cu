@@ -254,12 +254,16 @@ __device__ __forceinline__ unsigned long long warp_max_u(unsigned long long v) {
 }
 
 // Median of the 1,024 non-negative values held 32 per lane (median(),
-// native_stage2.rs:1173-1184: mean of the 512th and 513th smallest). Exact
-// order statistic by bisection on the IEEE bit pattern, which orders
-// non-negative floats like their values.
+// native_stage2.rs:1173-1184: mean of the 512th and 513th smallest), exact.
+// Bisection on the IEEE bit pattern (which orders non-negative floats like
+// their values) narrows a bracket [lo, hi] holding the 512th smallest until it
+// holds at most 32 of the values; those are copied to `scratch` (32 slots of
+// the warp's shared memory) and ranked among themselves. v0, v1 = the 512th
+// and 513th smallest.
 template <typename R>
-__device__ __forceinline__ R warp_median1024(const R (&o)[32]) {
+__device__ __forceinline__ void warp_median_pair(const R (&o)[32], R* scratch, R& v0, R& v1) {
   using U = typename CT<R>::U;
+  const int lane = threadIdx.x & 31;
   U lo = to_bits(o[0]), hi = lo;
 #pragma unroll
   for (int i = 1; i < 32; ++i) {
@@ -269,69 +273,92 @@ __device__ __forceinline__ R warp_median1024(const R (&o)[32]) {
   }
   lo = warp_min_u(lo);
   hi = warp_max_u(hi);
-  const int kth = 511;
-  while (lo < hi) {
+  int cnt_lo = 0, cnt_hi = 1024;  // values below lo, values up to hi
+  while (lo < hi && cnt_hi - cnt_lo > 32) {
     const U mid = lo + ((hi - lo) >> 1);
-    int cnt = 0;
+    unsigned cnt = 0;
 #pragma unroll
-    for (int i = 0; i < 32; ++i) cnt += (to_bits(o[i]) <= mid) ? 1 : 0;
-    cnt = warp_sum(cnt);
-    if (cnt >= kth + 1)
+    for (int i = 0; i < 32; ++i) cnt += (to_bits(o[i]) <= mid) ? 1u : 0u;
+    cnt = __reduce_add_sync(kFull, cnt);
+    if (cnt >= 512u) {
       hi = mid;
-    else
+      cnt_hi = static_cast<int>(cnt);
+    } else {
       lo = mid + 1;
+      cnt_lo = static_cast<int>(cnt);
+    }
   }
-  int cle = 0;
-  U nxt = ~U(0);
+  const int r0 = 511 - cnt_lo;  // rank of the 512th smallest inside the bracket
+  if (lo == hi) {
+    v0 = from_bits(lo);
+    if (cnt_hi >= 513) {
+      v1 = v0;
+    } else {
+      U nxt = ~U(0);
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        const U u = to_bits(o[i]);
+        if (u > hi) nxt = min(nxt, u);
+      }
+      v1 = from_bits(warp_min_u(nxt));
+    }
+    return;
+  }
+  // copy the bracket's values to scratch (exclusive prefix over lanes)
+  int mine = 0;
 #pragma unroll
   for (int i = 0; i < 32; ++i) {
     const U u = to_bits(o[i]);
-    cle += (u <= lo) ? 1 : 0;
-    if (u > lo) nxt = min(nxt, u);
+    mine += (u >= lo && u <= hi) ? 1 : 0;
   }
-  cle = warp_sum(cle);
-  nxt = warp_min_u(nxt);
-  const R v0 = from_bits(lo);
-  const R v1 = (cle >= kth + 2) ? v0 : from_bits(nxt);
+  int incl = mine;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int t = __shfl_up_sync(kFull, incl, d);
+    if (lane >= d) incl += t;
+  }
+  int off = incl - mine;
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    const U u = to_bits(o[i]);
+    if (u >= lo && u <= hi) scratch[off++] = o[i];
+  }
+  __syncwarp();
+  const int nb = cnt_hi - cnt_lo;
+  const R x = lane < nb ? scratch[lane] : R(0);
+  int rank = 0;
+  for (int j = 0; j < nb; ++j) {
+    const R y = scratch[j];
+    rank += (y < x || (y == x && j < lane)) ? 1 : 0;
+  }
+  const unsigned m0 = __ballot_sync(kFull, lane < nb && rank == r0);
+  v0 = __shfl_sync(kFull, x, __ffs(m0) - 1);
+  if (r0 + 1 < nb) {
+    const unsigned m1 = __ballot_sync(kFull, lane < nb && rank == r0 + 1);
+    v1 = __shfl_sync(kFull, x, __ffs(m1) - 1);
+  } else {
+    U nxt = ~U(0);
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      const U u = to_bits(o[i]);
+      if (u > hi) nxt = min(nxt, u);
+    }
+    v1 = from_bits(warp_min_u(nxt));
+  }
+  __syncwarp();
+}
+
+template <typename R>
+__device__ __forceinline__ R warp_median1024(const R (&o)[32], R* scratch) {
+  R v0, v1;
+  warp_median_pair<R>(o, scratch, v0, v1);
   return (v0 + v1) * R(0.5);
 }
 
 template <typename R>
-__device__ __forceinline__ R warp_median1024_pair(const R (&o)[32], R& v0_out, R& v1_out) {
-  using U = typename CT<R>::U;
-  U lo = to_bits(o[0]), hi = lo;
-#pragma unroll
-  for (int i = 1; i < 32; ++i) {
-    const U u = to_bits(o[i]);
-    lo = min(lo, u);
-    hi = max(hi, u);
-  }
-  lo = warp_min_u(lo);
-  hi = warp_max_u(hi);
-  const int kth = 511;
-  while (lo < hi) {
-    const U mid = lo + ((hi - lo) >> 1);
-    int cnt = 0;
-#pragma unroll
-    for (int i = 0; i < 32; ++i) cnt += (to_bits(o[i]) <= mid) ? 1 : 0;
-    cnt = warp_sum(cnt);
-    if (cnt >= kth + 1)
-      hi = mid;
-    else
-      lo = mid + 1;
-  }
-  int cle = 0;
-  U nxt = ~U(0);
-#pragma unroll
-  for (int i = 0; i < 32; ++i) {
-    const U u = to_bits(o[i]);
-    cle += (u <= lo) ? 1 : 0;
-    if (u > lo) nxt = min(nxt, u);
-  }
-  cle = warp_sum(cle);
-  nxt = warp_min_u(nxt);
-  v0_out = from_bits(lo);
-  v1_out = (cle >= kth + 2) ? v0_out : from_bits(nxt);
+__device__ __forceinline__ R warp_median1024_pair(const R (&o)[32], R* scratch, R& v0_out, R& v1_out) {
+  warp_median_pair<R>(o, scratch, v0_out, v1_out);
   return (v0_out + v1_out) * R(0.5);
 }
 
@@ -427,7 +454,7 @@ __device__ __forceinline__ void clap_window_warp(Tile& T, const int lane, const 
     }
     o[k] = acc;
   }
-  const R med = warp_median1024<R>(o);
+  const R med = warp_median1024<R>(o, &T.hs[0][0]);
   // H <- max((H/med)^alpha - 1, 0); spectrum *= H*beta + low_pass
   const R beta = static_cast<R>(a.beta);
   const R alpha = static_cast<R>(a.alpha);
@@ -1661,7 +1688,7 @@ __device__ __forceinline__ float2 s3_patch_point(ClapTile<float>& T, const int l
       if (sk + d >= 0 && sk + d < 32) acc += t[(k + d) & 31] * g7[d + 3];
     o[k] = acc;
   }
-  const float med = warp_median1024<float>(o);
+  const float med = warp_median1024<float>(o, &T.hs[0][0]);
   const float beta = static_cast<float>(a.beta), alpha = static_cast<float>(a.alpha);
   const float inv_med = med != 0.f ? 1.f / med : 1.f;
   float2 acc = make_float2(0.f, 0.f);
@@ -2445,7 +2472,7 @@ __global__ void __launch_bounds__(128) k_clap_bwd(ClapBwdArgs b, typename CT<R>:
         o[k] = acc;
       }
       R v0, v1;
-      const R med = warp_median1024_pair<R>(o, v0, v1);
+      const R med = warp_median1024_pair<R>(o, &T.hs[0][0], v0, v1);
       // g_Y = FFT2(g_y) (adjoint of the unnormalised inverse FFT)
       if (lane < nw) fft_pass<R>(T.gre, T.gim, twf, lane, true);
       __syncwarp();
