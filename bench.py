@@ -244,10 +244,14 @@ def adjoint_leg(prep, dev: int) -> dict:
 
 
 def stage3_leg(ctx, prep, rank: int, cpu: bool = True) -> dict:
-    """Stage-3 re-estimate (ps3_reestimate) of the PS whose converged stage-2
-    coherence exceeds 0.3, timed end to end through the public call (host
-    arrays in and out); the oracle re-estimates a bounded sample of the same
+    """Stage-3 re-estimate of the PS whose converged stage-2 coherence
+    exceeds 0.3: through ps2_stage3_reestimate on the context that ran stage 2
+    (selection in, results out to host memory, or kept on the device), and
+    through ps3_reestimate (every input from host memory, the reference's
+    stage-3 interface); the oracle re-estimates a bounded sample of the same
     rows on the host cores for the CPU figure."""
+    import torch
+
     from pystamps_b200 import stage3
 
     pm = ctx.download(["coh_ps", "ph_grid"])
@@ -256,18 +260,30 @@ def stage3_leg(ctx, prep, rank: int, cpu: bool = True) -> dict:
     bp = np.asarray(prep.bperp, dtype=np.float32)
     bp = np.broadcast_to(bp, (prep.n_ps, prep.n_ifg)) if bp.ndim == 1 else bp
     fit = np.arange(prep.n_ifg)
-    ntw = float(np.float32(prep.n_trial_wraps))
+    ntw = float(prep.n_trial_wraps)
     kw = dict(clap_alpha=prep.clap_alpha, clap_beta=prep.clap_beta, low_pass=prep.low_pass, n_trial_wraps=ntw)
-    stage3.reestimate(pm["ph_grid"], gij, sel[:1000], prep.ph_nm, bp, fit, **kw)  # warm-up
-    ts = []
-    for _ in range(2):
-        t0 = time.perf_counter()
-        stage3.reestimate(pm["ph_grid"], gij, sel, prep.ph_nm, bp, fit, **kw)
-        ts.append(time.perf_counter() - t0)
-    t = min(ts)
-    out = {"selected_ps": int(sel.size), "n_ifg": prep.n_ifg, "seconds": t, "ps_per_s": sel.size / t,
+
+    def best(fn, reps=2):
+        fn()  # warm-up
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return min(ts)
+
+    t_res = best(lambda: stage3.reestimate_resident(ctx, sel, fit))
+    t_dev = best(lambda: stage3.reestimate_resident(ctx, sel, fit, on_device=True))
+    t_host = best(lambda: stage3.reestimate(pm["ph_grid"], gij, sel, prep.ph_nm, bp, fit, **kw))
+    out = {"selected_ps": int(sel.size), "n_ifg": prep.n_ifg, "seconds": t_res, "ps_per_s": sel.size / t_res,
            "cells": int(np.unique(gij[sel, 0] * 100000 + gij[sel, 1]).size),
-           "what": "stage3.reestimate: gather rows + ps3_reestimate (H2D, patch CLAP per PS cell, stage-3 topofit, D2H)"}
+           "what": "stage3.reestimate_resident: selection H2D, patch CLAP per PS cell + stage-3 topofit on the "
+                   "stage-2 context's resident grid/phases/bperp, results D2H",
+           "outputs_on_device_seconds": t_dev,
+           "host_entry_seconds": t_host,
+           "host_entry_what": "stage3.reestimate: gather rows + ps3_reestimate (grid, phases, bperp H2D; results D2H)"}
     if cpu and rank == 0:
         from oracle import oracle as O
 

@@ -237,6 +237,18 @@ typedef struct ps3_reestimate_out {
 
 int ps3_reestimate(const ps3_reestimate_desc* desc, ps3_reestimate_out* out, int device);
 
+/* The same re-estimate from a context that ran stage 2 (ps2_run_to_convergence
+ * or ps2_batch_run): the patch's phases, bperp, cells, low-pass, CLAP
+ * parameters, trial count and last binned grid are read where they already
+ * are in device memory, so only the selection goes in and the results come
+ * out. sel: 0-based rows in the caller's order; fit_ifg: 0-based columns.
+ * outputs_on_device != 0: the out pointers are device pointers on the
+ * context's device. The window is 32 x 32 (parms clap_win, the only stage-3
+ * window this library runs) with the context's 32 x 32 low-pass filter.
+ * Synchronous; FP32 contexts. */
+int ps2_stage3_reestimate(ps2_ctx* ctx, const int64_t* sel, int64_t n_sel, const int64_t* fit_ifg, int64_t n_fit,
+                          int64_t slc_osf, ps3_reestimate_out* out, int outputs_on_device);
+
 /* ---- differentiable coherence (adjoints) ------------------------------------
  * The gamma map with K given, as a function of the input phases, K and the
  * CLAP parameters, on the loaded patch's geometry (cells, bperp, low-pass,

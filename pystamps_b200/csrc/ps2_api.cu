@@ -234,6 +234,10 @@ struct ps2_ctx {
   DevBuf ad_ph, ad_K, ad_w, ad_coh, ad_grid, ad_win, ad_filt, ad_gfilt, ad_gph, ad_gK, ad_gf, ad_part;
   int ad_blocks = 0, ad_blocks64 = 0;
   cudaEvent_t ad_ev = nullptr;
+  // stage-3 re-estimate from the loaded patch (ps2_stage3_reestimate): for
+  // each row in the caller's order, its cell-sorted position and its cell
+  std::vector<int32_t> h_sorted_pos, h_cell;
+  int64_t gmax_i = 0, gmax_j = 0;
   // batches led by this context (ps2_batch_run): per-patch arguments and tables
   DevBuf bt;
   int* h_active = nullptr;  // pinned [1]
@@ -618,14 +622,23 @@ int ps2_load_patch(ps2_ctx* c, const ps2_patch_desc* d) {
     start[gl[r] + 1] += 1;
   }
   for (int64_t g = 0; g < G; ++g) start[g + 1] += start[g];
+  c->h_sorted_pos.resize(static_cast<size_t>(N));
+  c->h_cell.resize(static_cast<size_t>(N));
+  c->gmax_i = 0;
+  c->gmax_j = 0;
   {
     std::vector<int32_t> fillp(start.begin(), start.end() - 1);
     for (int64_t r = 0; r < N; ++r) {
       const int32_t s = fillp[gl[r]]++;
       perm[s] = static_cast<int32_t>(r);
       cell_of[s] = static_cast<int32_t>(gl[r]);
+      c->h_sorted_pos[r] = s;
+      c->h_cell[r] = static_cast<int32_t>(gl[r]);
+      c->gmax_i = std::max<int64_t>(c->gmax_i, gl[r] / c->n_j + 1);
+      c->gmax_j = std::max<int64_t>(c->gmax_j, gl[r] % c->n_j + 1);
     }
   }
+
   const size_t R = rsz(c), Cz = csz(c);
   CK(c->perm.alloc(sizeof(int32_t) * N));
   CK(cudaMemcpyAsync(c->perm.p, perm.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, c->st));
@@ -1721,6 +1734,44 @@ int ps2_batch_run(ps2_ctx* const* ctxs, int64_t n, ps2_iter_stats* last) {
 }  // extern "C"
 
 // ======================================================= stage-3 re-estimate ==
+namespace {
+
+// One patch per distinct PS cell (ported.py:4496-4516): jobs[4 k..4 k+3] =
+// patch origin row, col (0-based; -1 when the 32-cell patch does not fit) and
+// the PS cell inside the patch; job_of[r] = the job of selected row r.
+template <typename CellOf>
+int s3_plan_jobs(int64_t n, int64_t n_i, int64_t n_j, int64_t nw, CellOf cell_of, std::vector<int32_t>* job_of,
+                 std::vector<int32_t>* jobs, const char* who) {
+  const int64_t half = nw / 2;
+  std::vector<int32_t> cell_job(static_cast<size_t>(n_i * n_j), -1);
+  job_of->assign(static_cast<size_t>(n), 0);
+  jobs->clear();
+  for (int64_t r = 0; r < n; ++r) {
+    int64_t pi = 0, pj = 0;
+    cell_of(r, &pi, &pj);
+    if (pi < 1 || pi > n_i || pj < 1 || pj > n_j)
+      return set_err(PS2_ERR_INVALID_ARG, "%s: grid_ij of row %lld = (%lld, %lld) outside 1..%lld x 1..%lld", who,
+                     (long long)r, (long long)pi, (long long)pj, (long long)n_i, (long long)n_j);
+    int32_t& j = cell_job[(pi - 1) * n_j + (pj - 1)];
+    if (j < 0) {
+      j = static_cast<int32_t>(jobs->size() / 4);
+      int64_t i_min = std::max<int64_t>(pi - half, 1), i_max = i_min + nw - 1;
+      if (i_max > n_i) i_min = i_min - i_max + n_i;
+      int64_t j_min = std::max<int64_t>(pj - half, 1), j_max = j_min + nw - 1;
+      if (j_max > n_j) j_min = j_min - j_max + n_j;
+      const bool ok = i_min >= 1 && j_min >= 1;
+      jobs->push_back(ok ? static_cast<int32_t>(i_min - 1) : -1);
+      jobs->push_back(ok ? static_cast<int32_t>(j_min - 1) : -1);
+      jobs->push_back(static_cast<int32_t>(pi - i_min));
+      jobs->push_back(static_cast<int32_t>(pj - j_min));
+    }
+    (*job_of)[r] = j;
+  }
+  return PS2_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int ps3_reestimate(const ps3_reestimate_desc* d, ps3_reestimate_out* o, int device) {
@@ -1749,29 +1800,13 @@ int ps3_reestimate(const ps3_reestimate_desc* d, ps3_reestimate_out* o, int devi
                      (long long)d->fit_ifg[k], (long long)d->n_ifg - 1);
   if (d->n_sel == 0) return PS2_OK;
   CK(cudaSetDevice(device));
-  const int64_t M = d->n_ifg, n = d->n_sel, n_i = d->n_i, n_j = d->n_j, half = d->clap_win / 2, nw = d->clap_win;
-  // one patch per distinct PS cell (ported.py:4496-4516)
-  std::vector<int32_t> cell_job(static_cast<size_t>(n_i * n_j), -1), job_of(n), jobs;
-  for (int64_t r = 0; r < n; ++r) {
-    const int64_t pi = d->grid_ij[2 * r], pj = d->grid_ij[2 * r + 1];
-    if (pi < 1 || pi > n_i || pj < 1 || pj > n_j)
-      return set_err(PS2_ERR_INVALID_ARG, "ps3_reestimate: grid_ij of row %lld = (%lld, %lld) outside 1..%lld x 1..%lld",
-                     (long long)r, (long long)pi, (long long)pj, (long long)n_i, (long long)n_j);
-    int32_t& j = cell_job[(pi - 1) * n_j + (pj - 1)];
-    if (j < 0) {
-      j = static_cast<int32_t>(jobs.size() / 4);
-      int64_t i_min = std::max<int64_t>(pi - half, 1), i_max = i_min + nw - 1;
-      if (i_max > n_i) i_min = i_min - i_max + n_i;
-      int64_t j_min = std::max<int64_t>(pj - half, 1), j_max = j_min + nw - 1;
-      if (j_max > n_j) j_min = j_min - j_max + n_j;
-      const bool ok = i_min >= 1 && j_min >= 1;
-      jobs.push_back(ok ? static_cast<int32_t>(i_min - 1) : -1);
-      jobs.push_back(ok ? static_cast<int32_t>(j_min - 1) : -1);
-      jobs.push_back(static_cast<int32_t>(pi - i_min));
-      jobs.push_back(static_cast<int32_t>(pj - j_min));
-    }
-    job_of[r] = j;
-  }
+  const int64_t M = d->n_ifg, n = d->n_sel, n_i = d->n_i, n_j = d->n_j;
+  std::vector<int32_t> job_of, jobs;
+  int rc = s3_plan_jobs(n, n_i, n_j, d->clap_win, [&](int64_t r, int64_t* pi, int64_t* pj) {
+    *pi = d->grid_ij[2 * r];
+    *pj = d->grid_ij[2 * r + 1];
+  }, &job_of, &jobs, "ps3_reestimate");
+  if (rc) return rc;
   const int64_t n_jobs = static_cast<int64_t>(jobs.size() / 4);
   std::vector<int32_t> fit(d->fit_ifg, d->fit_ifg + d->n_fit);
   cudaDeviceProp prop;
@@ -1811,6 +1846,7 @@ int ps3_reestimate(const ps3_reestimate_desc* d, ps3_reestimate_out* o, int devi
   ca.grid = grid.as<float2>();
   ca.grid_cols = static_cast<int>(d->grid_cols);
   ca.M = static_cast<int>(M);
+  ca.grid_stride = static_cast<int>(M);
   ca.jobs = djobs.as<int32_t>();
   ca.n_jobs = n_jobs;
   ca.ngroups = static_cast<int>((M + 3) / 4);
@@ -1849,6 +1885,120 @@ int ps3_reestimate(const ps3_reestimate_desc* d, ps3_reestimate_out* o, int devi
   CK(cudaMemcpyAsync(o->C_ps2, C2.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(o->coh_ps2, coh2.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  return PS2_OK;
+}
+
+
+int ps2_stage3_reestimate(ps2_ctx* c, const int64_t* sel, int64_t n_sel, const int64_t* fit_ifg, int64_t n_fit,
+                          int64_t slc_osf, ps3_reestimate_out* o, int outputs_on_device) {
+  if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "ps2_stage3_reestimate: no patch loaded");
+  if (c->fp64) return set_err(PS2_ERR_UNSUPPORTED, "ps2_stage3_reestimate: the context is FP64 (stage 3 is FP32)");
+  if (!o || (n_sel > 0 && (!sel || !fit_ifg)))
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_stage3_reestimate: NULL argument");
+  if (n_sel < 0) return set_err(PS2_ERR_INVALID_ARG, "ps2_stage3_reestimate: n_sel < 0");
+  if (n_fit <= 0 || n_fit > c->M || n_fit > 1024)
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_stage3_reestimate: n_fit %lld out of range", (long long)n_fit);
+  if (slc_osf < 1) return set_err(PS2_ERR_INVALID_ARG, "ps2_stage3_reestimate: slc_osf must be >= 1");
+  if (c->iters_done <= 0) return set_err(PS2_ERR_INVALID_ARG, "ps2_stage3_reestimate: stage 2 has not run");
+  if (n_sel > 0 && (!o->ph_patch2 || !o->K_ps2 || !o->C_ps2 || !o->coh_ps2 || !o->ph_res2))
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_stage3_reestimate: an output array is NULL");
+  for (int64_t k = 0; k < n_fit; ++k)
+    if (fit_ifg[k] < 0 || fit_ifg[k] >= c->M)
+      return set_err(PS2_ERR_INVALID_ARG, "ps2_stage3_reestimate: fit_ifg[%lld] = %lld outside 0..%d", (long long)k,
+                     (long long)fit_ifg[k], c->M - 1);
+  for (int64_t r = 0; r < n_sel; ++r)
+    if (sel[r] < 0 || sel[r] >= c->N)
+      return set_err(PS2_ERR_INVALID_ARG, "ps2_stage3_reestimate: sel[%lld] = %lld outside 0..%lld", (long long)r,
+                     (long long)sel[r], (long long)c->N - 1);
+  if (n_sel == 0) return PS2_OK;
+  CK(cudaSetDevice(c->device));
+  const int64_t M = c->M, n = n_sel;
+  std::vector<int32_t> job_of, jobs, rows(static_cast<size_t>(n));
+  const int64_t nj_grid = c->n_j;
+  int rc = s3_plan_jobs(n, c->gmax_i, c->gmax_j, 32, [&](int64_t r, int64_t* pi, int64_t* pj) {
+    const int64_t g = c->h_cell[sel[r]];
+    *pi = g / nj_grid + 1;
+    *pj = g % nj_grid + 1;
+  }, &job_of, &jobs, "ps2_stage3_reestimate");
+  if (rc) return rc;
+  for (int64_t r = 0; r < n; ++r) rows[r] = c->h_sorted_pos[sel[r]];
+  const int64_t n_jobs = static_cast<int64_t>(jobs.size() / 4);
+  std::vector<int32_t> fit(fit_ifg, fit_ifg + n_fit);
+  const int n_half = c->n_half;  // the stage-2 trial count (pm1.n_trial_wraps)
+  const size_t warp_smem = (static_cast<size_t>(n_fit) * 16 + static_cast<size_t>(2 * n_half + 1) * 4 + 15) & ~size_t(15);
+  if (4 * warp_smem > 200 * 1024)
+    return set_err(PS2_ERR_UNSUPPORTED, "ps2_stage3_reestimate: %lld fit interferograms x %d trials exceed shared memory",
+                   (long long)n_fit, 2 * n_half + 1);
+  cudaStream_t st = c->st;
+  DevBuf djobs, djob_of, drow, dfit, jout, pp2, K2, C2, coh2, res2;
+  CK(djobs.alloc(sizeof(int32_t) * jobs.size()));
+  CK(cudaMemcpyAsync(djobs.p, jobs.data(), sizeof(int32_t) * jobs.size(), cudaMemcpyHostToDevice, st));
+  CK(djob_of.alloc(sizeof(int32_t) * n));
+  CK(cudaMemcpyAsync(djob_of.p, job_of.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+  CK(drow.alloc(sizeof(int32_t) * n));
+  CK(cudaMemcpyAsync(drow.p, rows.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+  CK(dfit.alloc(sizeof(int32_t) * fit.size()));
+  CK(cudaMemcpyAsync(dfit.p, fit.data(), sizeof(int32_t) * fit.size(), cudaMemcpyHostToDevice, st));
+  CK(jout.alloc(sizeof(float2) * n_jobs * M));
+  float2* o_pp = reinterpret_cast<float2*>(o->ph_patch2);
+  float* o_res = o->ph_res2;
+  double *o_K = o->K_ps2, *o_C = o->C_ps2, *o_coh = o->coh_ps2;
+  if (!outputs_on_device) {
+    CK(pp2.alloc(sizeof(float2) * n * M));
+    CK(res2.alloc(sizeof(float) * n * M));
+    CK(K2.alloc(sizeof(double) * n));
+    CK(C2.alloc(sizeof(double) * n));
+    CK(coh2.alloc(sizeof(double) * n));
+    o_pp = pp2.as<float2>();
+    o_res = res2.as<float>();
+    o_K = K2.as<double>();
+    o_C = C2.as<double>();
+    o_coh = coh2.as<double>();
+  }
+  S3ClapArgs ca{};
+  ca.grid = c->grid.as<float2>();  // the last iteration's binned grid (pm1.ph_grid)
+  ca.grid_cols = c->n_j;
+  ca.M = static_cast<int>(M);
+  ca.grid_stride = c->Mp;
+  ca.jobs = djobs.as<int32_t>();
+  ca.n_jobs = n_jobs;
+  ca.ngroups = static_cast<int>((M + 3) / 4);
+  ca.slc_rad = static_cast<int>(slc_osf - 1);
+  ca.alpha = c->alpha;
+  ca.beta = c->beta;
+  ca.alpha_is_one = c->alpha == 1.0 ? 1 : 0;
+  ca.low_pass = c->low_pass.as<double>();
+  gauss7(ca.g7, nullptr);
+  ca.job_out = jout.as<float2>();
+  CK(launch_s3_clap(ca, c->twf, c->sm_count, st));
+  S3FitArgs fa{};
+  fa.ph = c->ph_nm.as<float2>();
+  fa.bp = c->bp.as<float>();
+  fa.row = drow.as<int32_t>();
+  fa.bp_row_inv = c->bp_row_inv;
+  fa.job_of = djob_of.as<int32_t>();
+  fa.job_out = jout.as<float2>();
+  fa.fit = dfit.as<int32_t>();
+  fa.n_fit = static_cast<int>(n_fit);
+  fa.M = static_cast<int>(M);
+  fa.n_half = n_half;
+  fa.n_sel = n;
+  fa.warp_smem = warp_smem;
+  fa.ph_patch2 = o_pp;
+  fa.K2 = o_K;
+  fa.C2 = o_C;
+  fa.coh2 = o_coh;
+  fa.ph_res2 = o_res;
+  CK(launch_s3_fit(fa, c->sm_count, st));
+  if (!outputs_on_device) {
+    CK(cudaMemcpyAsync(o->ph_patch2, pp2.p, sizeof(float2) * n * M, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(o->ph_res2, res2.p, sizeof(float) * n * M, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(o->K_ps2, K2.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(o->C_ps2, C2.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(o->coh_ps2, coh2.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  c->launches = 2;
   return PS2_OK;
 }
 

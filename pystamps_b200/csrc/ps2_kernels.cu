@@ -1745,7 +1745,7 @@ __global__ void __launch_bounds__(128) k_s3_clap(S3ClapArgs a, Twiddles32f tw) {
       const int c = 4 * g + q;
       float2 v = make_float2(0.f, 0.f);
       if (c < M) {
-        v = a.grid[(static_cast<int64_t>(i0 + li) * a.grid_cols + (j0 + lj)) * M + c];
+        v = a.grid[(static_cast<int64_t>(i0 + li) * a.grid_cols + (j0 + lj)) * a.grid_stride + c];
         if (isnan(v.x) || isnan(v.y)) v = make_float2(0.f, 0.f);
         const bool own = li == bi && lj == bj;
         const bool osf = c == 0 && abs(li - bi) <= a.slc_rad && abs(lj - bj) <= a.slc_rad;
@@ -1841,12 +1841,13 @@ __global__ void __launch_bounds__(128) k_s3_fit(S3FitArgs a) {
   const int64_t nw = static_cast<int64_t>(gridDim.x) * 4;
   for (int64_t r = gw; r < a.n_sel; r += nw) {
     const int job = a.job_of[r];
+    const int64_t row = a.row ? static_cast<int64_t>(a.row[r]) : r;  // row of ph / bp
     bool zero = false;
     for (int c = lane; c < M; c += 32) {
       const float2 pp = a.job_out[static_cast<int64_t>(job) * M + c];
       a.ph_patch2[r * M + c] = pp;
       a.ph_res2[r * M + c] = 0.f;
-      const float2 h = a.ph[r * M + c];
+      const float2 h = a.ph[row * M + c];
       // psdph = ph * conj(ph_patch2) in f64 (exact products of f32 values)
       const double re = static_cast<double>(h.x) * pp.x + static_cast<double>(h.y) * pp.y;
       const double im = static_cast<double>(h.y) * pp.x - static_cast<double>(h.x) * pp.y;
@@ -1864,12 +1865,12 @@ __global__ void __launch_bounds__(128) k_s3_fit(S3FitArgs a) {
     for (int k = lane; k < nf; k += 32) {
       const int c = a.fit[k];
       const float2 pp = a.job_out[static_cast<int64_t>(job) * M + c];
-      const float2 h = a.ph[r * M + c];
+      const float2 h = a.ph[row * M + c];
       const double re = static_cast<double>(h.x) * pp.x + static_cast<double>(h.y) * pp.y;
       const double im = static_cast<double>(h.y) * pp.x - static_cast<double>(h.x) * pp.y;
       const double mg = hypot(re, im);
       cpx[k] = make_float2(static_cast<float>(re / mg), static_cast<float>(im / mg));
-      bp[k] = a.bp[r * M + c];
+      bp[k] = a.bp_row_inv ? a.bp[c] : a.bp[row * M + c];
       mn = fminf(mn, bp[k]);
       mx = fmaxf(mx, bp[k]);
     }

@@ -106,8 +106,8 @@ struct FinalizeArgs {
 
 // --------------------------------------------------------------- stage 3 --
 struct S3ClapArgs {
-  const float2* grid;      // stage-2 ph_grid [rows, cols, M]
-  int grid_cols, M;
+  const float2* grid;      // stage-2 ph_grid [rows, cols, grid_stride]
+  int grid_cols, M, grid_stride;
   const int32_t* jobs;     // [n_jobs][4]: patch origin row, col (0-based; -1: no patch), PS cell in the patch
   int64_t n_jobs;
   int ngroups;             // ceil(M / 4)
@@ -120,8 +120,10 @@ struct S3ClapArgs {
 };
 
 struct S3FitArgs {
-  const float2* ph;        // [n_sel, M] selected rows
-  const float* bp;         // [n_sel, M]
+  const float2* ph;        // [*, M] rows of the selected PS
+  const float* bp;         // [*, M], or [M] when bp_row_inv
+  const int32_t* row;      // [n_sel] row of each selected PS in ph / bp (NULL: row r)
+  int bp_row_inv;
   const int32_t* job_of;   // [n_sel]
   const float2* job_out;   // [n_jobs, M]
   const int32_t* fit;      // [n_fit] columns used by topofit

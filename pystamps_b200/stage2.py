@@ -255,6 +255,7 @@ class Stage2Context:
         self._lib = lib()
         self._ctx = ctypes.c_void_p()
         check(self._lib.ps2_create(ctypes.byref(self._ctx), ctypes.c_int(device)))
+        self.device = int(device)
         self.prepared: PreparedPatch | None = None
         self.precision = PRECISION_FP32
         self._keep = []

@@ -193,6 +193,48 @@ def reestimate(ph_grid, grid_ij, sel, ph_work, bperp_mat, fit_ifg, *, clap_alpha
     return out
 
 
+def reestimate_resident(ctx, sel, fit_ifg, *, slc_osf: int = 1, on_device: bool = False) -> dict:
+    """The stage-3 re-estimate of rows `sel` (0-based) of a patch that a
+    Stage2Context (FP32) has just run through stage 2: the phases, bperp,
+    cells, CLAP parameters, trial count and last binned grid (pm1.ph_grid)
+    are read where they already are in device memory (ps2_stage3_reestimate),
+    so only the selection goes to the device. The phases are the context's
+    amplitude-normalised ones; psdph / |psdph| (ported.py:4529-4535) does not
+    depend on the amplitude, so the results match `reestimate` on the raw
+    phases up to the FP32 rounding of that normalisation.
+
+    on_device=True returns torch CUDA tensors on the context's device."""
+    sel = np.ascontiguousarray(np.asarray(sel, dtype=np.int64).reshape(-1))
+    fit = np.ascontiguousarray(np.asarray(fit_ifg, dtype=np.int64).reshape(-1))
+    p = ctx.prepared
+    if p is None:
+        raise Stage3Error("the context holds no patch")
+    n, m = sel.size, p.n_ifg
+    o = _lib.S3Out()
+    if on_device:
+        import torch
+
+        dev = torch.device("cuda", ctx.device)
+        out = {"ph_patch2": torch.zeros((n, m), dtype=torch.complex64, device=dev),
+               "K_ps2": torch.empty(n, dtype=torch.float64, device=dev),
+               "C_ps2": torch.empty(n, dtype=torch.float64, device=dev),
+               "coh_ps2": torch.empty(n, dtype=torch.float64, device=dev),
+               "ph_res2": torch.zeros((n, m), dtype=torch.float32, device=dev)}
+        addr = {k: v.data_ptr() for k, v in out.items()}
+        torch.cuda.current_stream(dev).synchronize()  # the allocations' fills precede the library's stream
+    else:
+        out = {"ph_patch2": np.zeros((n, m), np.complex64), "K_ps2": np.empty(n), "C_ps2": np.empty(n),
+               "coh_ps2": np.empty(n), "ph_res2": np.zeros((n, m), np.float32)}
+        addr = {k: ptr(v) for k, v in out.items()}
+    o.ph_patch2, o.K_ps2, o.C_ps2 = addr["ph_patch2"], addr["K_ps2"], addr["C_ps2"]
+    o.coh_ps2, o.ph_res2 = addr["coh_ps2"], addr["ph_res2"]
+    vp = ctypes.c_void_p
+    check(_lib.lib().ps2_stage3_reestimate(ctx._ctx, vp(ptr(sel)), ctypes.c_int64(n), vp(ptr(fit)), ctypes.c_int64(fit.size),
+                                           ctypes.c_int64(int(slc_osf)), ctypes.byref(o),
+                                           ctypes.c_int(1 if on_device else 0)))
+    return out
+
+
 def bootstrap_coh_std(ph_res, sel, fit_ifg) -> np.ndarray:
     """Spread of the residual coherence over 100 bootstrap draws per PS
     (ported.py:4408-4422, numpy default_rng(0), draws in PS order)."""

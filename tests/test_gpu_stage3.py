@@ -151,3 +151,57 @@ def test_stage3_select_ps_on_a_patch_directory(cuda_lib, golden, tmp_path):
     assert int((out["keep_ix"].ravel().astype(bool) != sel["sel_keep_ix"].ravel().astype(bool)).sum()) <= 3
     np.testing.assert_allclose(out["coh_thresh"].ravel(), sel["sel_coh_thresh"].ravel(), rtol=1e-6)
     assert float(out["max_percent_rand"].ravel()[0]) == pytest.approx(float(sel["sel_max_percent_rand"].ravel()[0]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("row_variant,slc_osf", [(True, 1), (False, 2)])
+def test_resident_reestimate_matches_host_entry(cuda_lib, row_variant, slc_osf):
+    """ps2_stage3_reestimate on the context that ran stage 2 gives the same
+    bits as ps3_reestimate on the downloaded grid and the context's phases."""
+    import torch
+
+    from pystamps_b200 import stage2 as S
+    from pystamps_b200 import stage3, synth
+
+    patch = synth.make_workload("A", row_variant=row_variant)
+    prep = S.prepare_patch(patch)
+    assert prep.row_invariant == (not row_variant)
+    rng = np.random.default_rng(11)
+    sel_rows = rng.choice(prep.n_ps, 2500, replace=False)  # unsorted: any row order
+    fit = np.sort(rng.choice(prep.n_ifg, prep.n_ifg - 3, replace=False))
+    gij = np.rint(prep.grid_ij).astype(np.int64)
+    bp = np.asarray(prep.bperp, dtype=np.float64)
+    bp = np.broadcast_to(bp, (prep.n_ps, prep.n_ifg)) if bp.ndim == 1 else bp
+    with S.Stage2Context() as c:
+        c.load(prep, "fp32")
+        c.run()
+        pm = c.download(["ph_grid"])
+        r = stage3.reestimate_resident(c, sel_rows, fit, slc_osf=slc_osf)
+        rd = stage3.reestimate_resident(c, sel_rows, fit, slc_osf=slc_osf, on_device=True)
+        with pytest.raises(Exception, match="outside"):
+            stage3.reestimate_resident(c, np.array([prep.n_ps]), fit)
+        with pytest.raises(Exception, match="outside"):
+            stage3.reestimate_resident(c, sel_rows[:4], np.array([prep.n_ifg]))
+    h = stage3.reestimate(pm["ph_grid"], gij, sel_rows, prep.ph_nm, bp, fit, clap_alpha=prep.clap_alpha,
+                          clap_beta=prep.clap_beta, low_pass=prep.low_pass, n_trial_wraps=prep.n_trial_wraps,
+                          slc_osf=slc_osf)
+    for k in ("ph_patch2", "ph_res2", "K_ps2", "C_ps2", "coh_ps2"):
+        np.testing.assert_array_equal(r[k], h[k], err_msg=k)
+        np.testing.assert_array_equal(rd[k].cpu().numpy(), h[k], err_msg=k)
+    assert torch.isfinite(rd["coh_ps2"]).any()
+
+
+@pytest.mark.gpu
+def test_resident_reestimate_rejects_fp64_and_unrun_contexts(cuda_lib):
+    from pystamps_b200 import stage2 as S
+    from pystamps_b200 import stage3, synth
+
+    prep = S.prepare_patch(synth.make_patch(1500, 12, 26, 41, seed=3, n_rand=2000, gamma_max_iterations=2))
+    with S.Stage2Context() as c:
+        c.load(prep, "fp32")
+        with pytest.raises(Exception, match="has not run"):
+            stage3.reestimate_resident(c, np.arange(10), np.arange(prep.n_ifg))
+        c.load(prep, "fp64")
+        c.run()
+        with pytest.raises(Exception, match="FP64"):
+            stage3.reestimate_resident(c, np.arange(10), np.arange(prep.n_ifg))
