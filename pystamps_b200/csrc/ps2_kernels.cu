@@ -764,62 +764,6 @@ __device__ __forceinline__ int group_transpose_reduce(float2 (&v)[W], const int 
   return cnt;
 }
 
-template <int W>
-__device__ __forceinline__ void accumulate_column(float2 (&S)[W], const float2 z, const float2 rot, const float th,
-                                                  const int m0) {
-  // th here is bp * (pi/4)/range; the anchor angle is th * m
-  float2 u = cmul(z, cis_neg_anchor(th * static_cast<float>(m0)));
-#pragma unroll
-  for (int k = 0; k < W; ++k) {
-    if (k > 0 && (k & 15) == 0) u = cmul(z, cis_neg_anchor(th * static_cast<float>(m0 + k)));
-    S[k].x += u.x;
-    S[k].y += u.y;
-    if (k + 1 < W) u = cmul(u, rot);
-  }
-}
-
-template <int W>
-__device__ __forceinline__ void accumulate_two_columns(float2 (&S)[W], const float2 z0, const float2 r0,
-                                                       const float t0, const float2 z1, const float2 r1,
-                                                       const float t1, const int m0) {
-  float2 u0 = cmul(z0, cis_neg_anchor(t0 * static_cast<float>(m0)));
-  float2 u1 = cmul(z1, cis_neg_anchor(t1 * static_cast<float>(m0)));
-#pragma unroll
-  for (int k = 0; k < W; ++k) {
-    if (k > 0 && (k & 15) == 0) {
-      u0 = cmul(z0, cis_neg_anchor(t0 * static_cast<float>(m0 + k)));
-      u1 = cmul(z1, cis_neg_anchor(t1 * static_cast<float>(m0 + k)));
-    }
-    S[k].x += u0.x + u1.x;
-    S[k].y += u0.y + u1.y;
-    if (k + 1 < W) {
-      u0 = cmul(u0, r0);
-      u1 = cmul(u1, r1);
-    }
-  }
-}
-
-template <int W>
-__device__ __forceinline__ void accumulate_four_columns(float2 (&S)[W], const float2 (&z)[4], const float2 (&r)[4],
-                                                        const float (&t)[4], const int m0) {
-  float2 u[4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) u[i] = cmul(z[i], cis_neg_anchor(t[i] * static_cast<float>(m0)));
-#pragma unroll
-  for (int k = 0; k < W; ++k) {
-    if (k > 0 && (k & 15) == 0) {
-#pragma unroll
-      for (int i = 0; i < 4; ++i) u[i] = cmul(z[i], cis_neg_anchor(t[i] * static_cast<float>(m0 + k)));
-    }
-    S[k].x += (u[0].x + u[1].x) + (u[2].x + u[3].x);
-    S[k].y += (u[0].y + u[1].y) + (u[2].y + u[3].y);
-    if (k + 1 < W) {
-#pragma unroll
-      for (int i = 0; i < 4; ++i) u[i] = cmul(u[i], r[i]);
-    }
-  }
-}
-
 // Per-PS column store: z (psdph), e^{-j theta} (the per-trial rotation, theta =
 // bp/range*pi/4 as the reference rounds it) and bp. Anchor angles are formed as
 // bp * ((pi/4)/range) * m.
@@ -827,48 +771,103 @@ struct ColumnSmem {
   float *zx, *zy, *rx, *ry, *bp;
 };
 
+// Trials +m and -m from one rotation chain, two columns per packed FP32x2
+// instruction. For a column z = (x, y) and w = e^{-j m theta}:
+//   z w       = (x w.x - y w.y, x w.y + y w.x)               trial +m
+//   z conj(w) = (x w.x + y w.y, y w.x - x w.y) = z e^{+j m theta}   trial -m
+// so the four sums  sum x w.x, sum x w.y, sum y w.y, sum y w.x  give both
+// trials. A lane holds its columns in pairs (c0, c1) = (gl + L k, gl + L (k+1)):
+// Wx = (w0.x, w1.x), Wy = (w0.y, w1.y) and the accumulators are FP32x2 pairs
+// (one column of the pair in each half), added together once per block. One
+// |m| step is then 4 packed instructions for the rotation
+//   Wx <- Wx Rx - Wy Ry,  Wy <- Wx Ry + Wy Rx      (R = e^{-j theta})
+// and 4 for the sums, i.e. 1 instruction per (trial, column). w is re-anchored
+// exactly (cis_neg_anchor of theta * m) at the first |m| of every block, so a
+// chain is at most W - 1 rotations long.
+struct PackedCols {
+  float2 x, y, rx, ry, nry, wx, wy;
+};
+
+__device__ __forceinline__ PackedCols load_packed_cols(const ColumnSmem& cs, const int c0, const int c1,
+                                                       const float qr, const int m0) {
+  PackedCols p;
+  p.x = make_float2(cs.zx[c0], cs.zx[c1]);
+  p.y = make_float2(cs.zy[c0], cs.zy[c1]);
+  p.rx = make_float2(cs.rx[c0], cs.rx[c1]);
+  p.ry = make_float2(cs.ry[c0], cs.ry[c1]);
+  p.nry = make_float2(-p.ry.x, -p.ry.y);
+  const float2 w0 = cis_neg_anchor(cs.bp[c0] * qr * static_cast<float>(m0));
+  const float2 w1 = cis_neg_anchor(cs.bp[c1] * qr * static_cast<float>(m0));
+  p.wx = make_float2(w0.x, w1.x);
+  p.wy = make_float2(w0.y, w1.y);
+  return p;
+}
+
+template <int W>
+__device__ __forceinline__ void accumulate_packed(float2 (&Axx)[W], float2 (&Axy)[W], float2 (&Ayy)[W],
+                                                  float2 (&Ayx)[W], PackedCols& p, const int k) {
+  Axx[k] = __ffma2_rn(p.x, p.wx, Axx[k]);
+  Axy[k] = __ffma2_rn(p.x, p.wy, Axy[k]);
+  Ayy[k] = __ffma2_rn(p.y, p.wy, Ayy[k]);
+  Ayx[k] = __ffma2_rn(p.y, p.wx, Ayx[k]);
+  if (k + 1 < W) {
+    const float2 t = __fmul2_rn(p.wy, p.nry);
+    const float2 u = __fmul2_rn(p.wy, p.rx);
+    const float2 wx = p.wx;
+    p.wx = __ffma2_rn(wx, p.rx, t);
+    p.wy = __ffma2_rn(wx, p.ry, u);
+  }
+}
+
+// One block of W trial pairs |m| = m0 .. m0+W-1 (m0 >= 1): trial indices
+// n_half + m and n_half - m. ncl (columns per lane) is even. The running best
+// keeps the first maximum in trial order (argmax_first_f32, :1526-1536)
+// although the trials arrive out of order.
 template <int W, int L>
-__device__ __forceinline__ void sweep_block(const ColumnSmem& cs, const float qr, const int ncl, const int gl,
-                                            const int m0, const int t0, const int T, float& best_sq, int& best_t) {
-  float2 S[W];
+__device__ __forceinline__ void sweep_pairs(const ColumnSmem& cs, const float qr, const int ncl, const int gl,
+                                            const int m0, const int n_half, float& best_sq, int& best_t) {
+  float2 Axx[W], Axy[W], Ayy[W], Ayx[W];
 #pragma unroll
-  for (int k = 0; k < W; ++k) S[k] = make_float2(0.f, 0.f);
+  for (int k = 0; k < W; ++k) {
+    Axx[k] = make_float2(0.f, 0.f);
+    Axy[k] = make_float2(0.f, 0.f);
+    Ayy[k] = make_float2(0.f, 0.f);
+    Ayx[k] = make_float2(0.f, 0.f);
+  }
   int k = 0;
   for (; k + 3 < ncl; k += 4) {
-    float2 z[4], r[4];
-    float t[4];
+    PackedCols p0 = load_packed_cols(cs, gl + L * k, gl + L * (k + 1), qr, m0);
+    PackedCols p1 = load_packed_cols(cs, gl + L * (k + 2), gl + L * (k + 3), qr, m0);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int c = gl + L * (k + i);
-      z[i] = make_float2(cs.zx[c], cs.zy[c]);
-      r[i] = make_float2(cs.rx[c], cs.ry[c]);
-      t[i] = cs.bp[c] * qr;
+    for (int j = 0; j < W; ++j) {
+      accumulate_packed<W>(Axx, Axy, Ayy, Ayx, p0, j);
+      accumulate_packed<W>(Axx, Axy, Ayy, Ayx, p1, j);
     }
-    accumulate_four_columns<W>(S, z, r, t, m0);
-  }
-  for (; k + 1 < ncl; k += 2) {
-    const int c0 = gl + L * k, c1 = c0 + L;
-    accumulate_two_columns<W>(S, make_float2(cs.zx[c0], cs.zy[c0]), make_float2(cs.rx[c0], cs.ry[c0]),
-                              cs.bp[c0] * qr, make_float2(cs.zx[c1], cs.zy[c1]), make_float2(cs.rx[c1], cs.ry[c1]),
-                              cs.bp[c1] * qr, m0);
   }
   if (k < ncl) {
-    const int c0 = gl + L * k;
-    accumulate_column<W>(S, make_float2(cs.zx[c0], cs.zy[c0]), make_float2(cs.rx[c0], cs.ry[c0]), cs.bp[c0] * qr,
-                         m0);
+    PackedCols p0 = load_packed_cols(cs, gl + L * k, gl + L * (k + 1), qr, m0);
+#pragma unroll
+    for (int j = 0; j < W; ++j) accumulate_packed<W>(Axx, Axy, Ayy, Ayx, p0, j);
+  }
+  float2 S[2 * W];
+#pragma unroll
+  for (int j = 0; j < W; ++j) {
+    const float xx = Axx[j].x + Axx[j].y, xy = Axy[j].x + Axy[j].y;
+    const float yy = Ayy[j].x + Ayy[j].y, yx = Ayx[j].x + Ayx[j].y;
+    S[j] = make_float2(xx - yy, xy + yx);
+    S[W + j] = make_float2(xx + yy, yx - xy);
   }
   int base;
-  const int cnt = group_transpose_reduce<W, L>(S, gl, base);
+  const int cnt = group_transpose_reduce<2 * W, L>(S, gl, base);
 #pragma unroll
-  for (int j = 0; j < (W / L > 1 ? W / L : 1); ++j) {
+  for (int j = 0; j < (2 * W / L > 1 ? 2 * W / L : 1); ++j) {
     if (j < cnt) {
-      const int t = t0 + base + j;
-      if (t < T) {
-        const float sq = S[j].x * S[j].x + S[j].y * S[j].y;
-        if (sq > best_sq) {
-          best_sq = sq;
-          best_t = t;
-        }
+      const int idx = base + j;
+      const int t = idx < W ? n_half + m0 + idx : n_half - (m0 + idx - W);
+      const float sq = S[j].x * S[j].x + S[j].y * S[j].y;
+      if (sq > best_sq || (sq == best_sq && t < best_t)) {
+        best_sq = sq;
+        best_t = t;
       }
     }
   }
@@ -902,7 +901,6 @@ __device__ __forceinline__ void topofit_vblock(const TopoArgs& a, const int mpad
   float2* __restrict__ ph_patch = static_cast<float2*>(a.ph_patch);
   const int64_t M = a.M;
   const int ncl = mpad / L;
-  const int T = 2 * a.n_half + 1;
   const unsigned gmask = (L == 32) ? kFull : (((1u << L) - 1u) << (g * L));
   double rms_acc = 0.0;
   int inv_acc = 0;
@@ -979,27 +977,29 @@ __device__ __forceinline__ void topofit_vblock(const TopoArgs& a, const int mpad
     }
     const float qr = kQuarterPiF / range;
     __syncwarp();
-    // trial sweep over m = -n .. n (all groups run it; invalid ones discard it)
-    float best_sq = -1.f;
-    int best_t = 0;
-    int t0 = 0;
-    for (; T - t0 >= 16; t0 += 16) sweep_block<16, L>(cs, qr, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
-    if (T - t0 >= 8) {
-      sweep_block<8, L>(cs, qr, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
-      t0 += 8;
+    // trial sweep over m = -n .. n (all groups run it; invalid ones discard it):
+    // m = 0 is the plain column sum, then the pairs +-m
+    float best_sq, s0x = 0.f, s0y = 0.f;
+    for (int k = 0; k < ncl; ++k) {
+      const int c = gl + L * k;
+      s0x += cs.zx[c];
+      s0y += cs.zy[c];
     }
-    if (T - t0 >= 4) {
-      sweep_block<4, L>(cs, qr, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
-      t0 += 4;
+    s0x = group_sum<L>(s0x);
+    s0y = group_sum<L>(s0y);
+    best_sq = s0x * s0x + s0y * s0y;
+    int best_t = a.n_half;
+    int m0 = 1;
+    for (; a.n_half - m0 + 1 >= 8; m0 += 8) sweep_pairs<8, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
+    if (a.n_half - m0 + 1 >= 4) {
+      sweep_pairs<4, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
+      m0 += 4;
     }
-    if (T - t0 >= 2) {
-      sweep_block<2, L>(cs, qr, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
-      t0 += 2;
+    if (a.n_half - m0 + 1 >= 2) {
+      sweep_pairs<2, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
+      m0 += 2;
     }
-    if (T - t0 >= 1) {
-      sweep_block<1, L>(cs, qr, ncl, gl, t0 - a.n_half, t0, T, best_sq, best_t);
-      t0 += 1;
-    }
+    if (a.n_half - m0 + 1 >= 1) sweep_pairs<1, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
     // first maximum over the group (argmax_first_f32, :1526-1536)
 #pragma unroll
     for (int o = L / 2; o > 0; o >>= 1) {
@@ -1298,7 +1298,9 @@ size_t topofit_smem_bytes(int L, int mpad) {
   return static_cast<size_t>(4 * (32 / L)) * stride * sizeof(float);
 }
 
-int topofit_mpad(int L, int M) { return ((M + L - 1) / L) * L; }
+// Columns per PS padded to a multiple of 2L (zero columns): each lane holds an
+// even number of columns, the packed pairs of the trial sweep.
+int topofit_mpad(int L, int M) { return ((M + 2 * L - 1) / (2 * L)) * (2 * L); }
 
 template <int L>
 static cudaError_t topofit_geometry_l(const TopoArgs& a, int grid_cap, size_t* smem, int* blocks_out) {
@@ -2055,7 +2057,7 @@ __global__ void __launch_bounds__(256) k_batch_overlap(BatchArgs b) {
 }
 
 template <int L>
-__global__ void __launch_bounds__(128) k_batch_topofit(BatchArgs b, const int32_t* __restrict__ units, int n_units) {
+__global__ void __launch_bounds__(128, 4) k_batch_topofit(BatchArgs b, const int32_t* __restrict__ units, int n_units) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int sh_hist[kCohBins];
   __shared__ double sh_rms[4];
