@@ -16,11 +16,14 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <mutex>
 
 #include "ps2_device.cuh"
 #include "ps2_kernels.cuh"
 
 namespace ps2 {
+
+cudaError_t kernel_attributes_once(size_t dynamic_smem);
 
 template <typename R>
 struct CT;
@@ -82,48 +85,55 @@ __device__ __forceinline__ void bin_task(const BinArgs& a, const int64_t task, c
     const int chunk = static_cast<int>(task - cell * a.nchunk);
     const int c = chunk * 32 + lane;
     const bool active = c < a.M;
-    const bool write_w = a.mode == 1 && chunk == 0 && lane == 0;
+    const bool write_w = a.mode == 1 && chunk == 0;
     const int s0 = a.cell_start[cell], s1 = a.cell_start[cell + 1];
     R ax = R(0), ay = R(0);
-    // rows are taken four at a time with every load issued before the
-    // arithmetic; the sum itself stays sequential in row order
-    for (int sb = s0; sb < s1; sb += 4) {
-      R wv[4], kv[4], bv[4];
-      float2 v[4];
+    // rows in batches of 32: lane l evaluates the weight and reads K of row
+    // sb + l once, the batch's rows take them by shuffle; inside a batch rows go
+    // four at a time with every load issued before the arithmetic, and the sum
+    // itself stays sequential in row order
+    for (int sb = s0; sb < s1; sb += 32) {
+      const int sl = sb + lane;
+      R wl = R(0), kl = R(0);
+      if (sl < s1) {
+        wl = bin_weight<R>(a, W, coh, sl);
+        if (a.mode != 3) kl = K[sl];
+        if (write_w) W[sl] = wl;
+      }
+      const int nb = min(32, s1 - sb);
+      for (int j0 = 0; j0 < nb; j0 += 4) {
+        R wv[4], kv[4], bv[4];
+        float2 v[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int s = sb + i;
-        wv[i] = R(0);
-        kv[i] = R(0);
-        bv[i] = R(0);
-        v[i] = make_float2(0.f, 0.f);
-        if (s < s1) {
-          wv[i] = bin_weight<R>(a, W, coh, s);
-          if (a.mode != 3) kv[i] = K[s];
-          if (active) {
+        for (int i = 0; i < 4; ++i) {
+          const int s = sb + j0 + i;
+          wv[i] = __shfl_sync(kFull, wl, (j0 + i) & 31);
+          kv[i] = __shfl_sync(kFull, kl, (j0 + i) & 31);
+          bv[i] = R(0);
+          v[i] = make_float2(0.f, 0.f);
+          if (s < s1 && active) {
             v[i] = ph[static_cast<int64_t>(s) * M + c];
             if (a.mode != 3)
               bv[i] = a.bp_row_inv ? static_cast<R>(bp[c]) : static_cast<R>(bp[static_cast<int64_t>(s) * M + c]);
           }
         }
-      }
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int s = sb + i;
-        if (s >= s1) break;
-        if (write_w) W[s] = wv[i];
-        if (!active) continue;
-        if (a.mode == 3) {
-          // accumulate_grid alone: ph_nm holds ph_weight, no ramp and no weight
-          ax = add_rn(ax, static_cast<R>(v[i].x));
-          ay = add_rn(ay, static_cast<R>(v[i].y));
-        } else {
-          const R phs = -(bv[i] * kv[i]);
-          R sn, cs;
-          sincos_r(phs, &sn, &cs);
-          const C r = cmul_rn(mk(static_cast<R>(v[i].x), static_cast<R>(v[i].y)), mk(cs, sn));
-          ax = add_rn(ax, mul_rn(r.x, wv[i]));
-          ay = add_rn(ay, mul_rn(r.y, wv[i]));
+        for (int i = 0; i < 4; ++i) {
+          const int s = sb + j0 + i;
+          if (s >= s1) break;
+          if (!active) continue;
+          if (a.mode == 3) {
+            // accumulate_grid alone: ph_nm holds ph_weight, no ramp and no weight
+            ax = add_rn(ax, static_cast<R>(v[i].x));
+            ay = add_rn(ay, static_cast<R>(v[i].y));
+          } else {
+            const R phs = -(bv[i] * kv[i]);
+            R sn, cs;
+            sincos_r(phs, &sn, &cs);
+            const C r = cmul_rn(mk(static_cast<R>(v[i].x), static_cast<R>(v[i].y)), mk(cs, sn));
+            ax = add_rn(ax, mul_rn(r.x, wv[i]));
+            ay = add_rn(ay, mul_rn(r.y, wv[i]));
+          }
         }
       }
     }
@@ -492,6 +502,107 @@ __device__ __forceinline__ void clap_consts(const ClapArgs& a, R* lp, R* wt) {
   for (int i = threadIdx.x; i < nw2; i += blockDim.x) wt[i] = static_cast<R>(a.wscaled[i]);
 }
 
+// Window loads and stores of a CLAP block: NW interferograms of one window,
+// pixel (li, lj) of interferogram NW*g + q in tiles[q]. FP32 moves two
+// interferograms (16 bytes) per access; each thread issues U accesses before
+// it touches shared memory. Pixel -> (row, column) uses pix * inv_nw >> 16
+// (inv_nw = ceil(65536 / nw)), exact for pix < 1024 and nw <= 32.
+template <typename R>
+struct ClapIo;
+template <>
+struct ClapIo<float> {
+  static constexpr int kPer = 2;  // interferograms per access
+  static constexpr int kU = 8;    // accesses in flight per thread
+};
+template <>
+struct ClapIo<double> {
+  static constexpr int kPer = 1;
+  static constexpr int kU = 4;
+};
+
+// Interferograms c and c + 1 (columns >= M read as zero; only columns < M
+// are dereferenced).
+__device__ __forceinline__ void clap_fetch(const float2* p, const int c, const int M, float (&v)[4]) {
+  if (c + 1 < M) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    v[0] = q.x;
+    v[1] = q.y;
+    v[2] = q.z;
+    v[3] = q.w;
+  } else {
+    const float2 q = c < M ? *p : make_float2(0.f, 0.f);
+    v[0] = q.x;
+    v[1] = q.y;
+    v[2] = 0.f;
+    v[3] = 0.f;
+  }
+}
+__device__ __forceinline__ void clap_fetch(const double2* p, const int c, const int M, double (&v)[2]) {
+  const double2 q = c < M ? *p : make_double2(0.0, 0.0);
+  v[0] = q.x;
+  v[1] = q.y;
+}
+
+template <typename R, int NW, typename Tile>
+__device__ __forceinline__ void clap_load_tiles(const ClapArgs& a, Tile* tiles, const typename CT<R>::C* grid,
+                                                const int i1, const int j1, const int g, const int nw, const int nw2,
+                                                const uint32_t inv_nw, const int tid) {
+  constexpr int NT = 32 * NW, PER = ClapIo<R>::kPer, U = ClapIo<R>::kU, NQ = NW / PER;
+  const int n_items = nw2 * NQ;
+  for (int b0 = 0; b0 < n_items; b0 += NT * U) {
+    R v[U][2 * PER];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = b0 + u * NT + tid;
+#pragma unroll
+      for (int e = 0; e < 2 * PER; ++e) v[u][e] = R(0);
+      if (idx < n_items) {
+        const int pix = idx / NQ, q0 = (idx % NQ) * PER;
+        const int li = static_cast<int>((static_cast<uint32_t>(pix) * inv_nw) >> 16), lj = pix - li * nw;
+        const int c = NW * g + q0;
+        clap_fetch(grid + (static_cast<int64_t>(i1 + li) * a.n_j + (j1 + lj)) * a.Mp + c, c, a.M, v[u]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = b0 + u * NT + tid;
+      if (idx < n_items) {
+        const int pix = idx / NQ, q0 = (idx % NQ) * PER;
+        const int li = static_cast<int>((static_cast<uint32_t>(pix) * inv_nw) >> 16), lj = pix - li * nw;
+#pragma unroll
+        for (int e = 0; e < PER; ++e) {
+          R x = v[u][2 * e], y = v[u][2 * e + 1];
+          if (isnan(x) || isnan(y)) x = y = R(0);  // NaN -> 0 (clap_filter_one_ifg)
+          tiles[q0 + e].re[li][lj] = x;
+          tiles[q0 + e].im[li][lj] = y;
+        }
+      }
+    }
+  }
+}
+
+template <typename R, int NW, typename Tile>
+__device__ __forceinline__ void clap_store_tiles(const ClapArgs& a, const Tile* tiles, typename CT<R>::C* out,
+                                                 const int64_t wi, const int g, const int nw, const int nw2,
+                                                 const uint32_t inv_nw, const int tid) {
+  constexpr int NT = 32 * NW, PER = ClapIo<R>::kPer, NQ = NW / PER;
+  const int n_items = nw2 * NQ;
+  for (int idx = tid; idx < n_items; idx += NT) {
+    const int pix = idx / NQ, q0 = (idx % NQ) * PER;
+    const int li = static_cast<int>((static_cast<uint32_t>(pix) * inv_nw) >> 16), lj = pix - li * nw;
+    const int c = NW * g + q0;
+    if (c >= a.Mp) continue;
+    typename CT<R>::C* dst = out + (wi * nw2 + pix) * a.Mp + c;
+    if constexpr (PER == 2) {
+      // Mp is a multiple of 4 and c even: c + 1 < Mp, 16-byte aligned
+      *reinterpret_cast<float4*>(dst) = make_float4(tiles[q0].re[li][lj], tiles[q0].im[li][lj],
+                                                    tiles[q0 + 1].re[li][lj], tiles[q0 + 1].im[li][lj]);
+    } else {
+      *dst = mk(tiles[q0].re[li][lj], tiles[q0].im[li][lj]);
+    }
+  }
+}
+
 // One block-task of CLAP: window task / ngroups, interferograms
 // NW * (task % ngroups) + warp, ngroups = ceil(Mp / NW).
 template <typename R, int NW>
@@ -528,35 +639,22 @@ __device__ __forceinline__ void clap_task(const ClapArgs& a, const int64_t task,
       j1 = a.n_j - nw;
     }
     __syncthreads();
-    // zero the padding of the tiles, load the windows (NaN -> 0)
-    for (int idx = tid; idx < NW * 32 * 32; idx += NT) {
-      const int q = idx >> 10, e = idx & 1023, r = e >> 5, cc = e & 31;
-      if (r >= nw || cc >= nw) {
-        tiles[q].re[r][cc] = R(0);
-        tiles[q].im[r][cc] = R(0);
+    // zero the padding of the tiles (none for a 32-pixel window)
+    if (nw < 32) {
+      for (int idx = tid; idx < NW * 32 * 32; idx += NT) {
+        const int q = idx >> 10, e = idx & 1023, r = e >> 5, cc = e & 31;
+        if (r >= nw || cc >= nw) {
+          tiles[q].re[r][cc] = R(0);
+          tiles[q].im[r][cc] = R(0);
+        }
       }
     }
-    for (int idx = tid; idx < nw2 * NW; idx += NT) {
-      const int pix = idx / NW, q = idx % NW;
-      const int li = pix / nw, lj = pix - li * nw;
-      const int c = NW * g + q;
-      C v = mk(R(0), R(0));
-      if (c < a.M) {
-        v = grid[(static_cast<int64_t>(i1 + li) * a.n_j + (j1 + lj)) * a.Mp + c];
-        if (isnan(v.x) || isnan(v.y)) v = mk(R(0), R(0));
-      }
-      tiles[q].re[li][lj] = v.x;
-      tiles[q].im[li][lj] = v.y;
-    }
+    const uint32_t inv_nw = (65536u + static_cast<uint32_t>(nw) - 1u) / static_cast<uint32_t>(nw);
+    clap_load_tiles<R, NW>(a, tiles, grid, i1, j1, g, nw, nw2, inv_nw, tid);
     __syncthreads();
     if (NW * g + warp < a.M) clap_window_warp<R>(T, lane, a, twf, twi, lp, wt, g7, rs, cs);
     __syncthreads();
-    for (int idx = tid; idx < nw2 * NW; idx += NT) {
-      const int pix = idx / NW, q = idx % NW;
-      const int li = pix / nw, lj = pix - li * nw;
-      const int c = NW * g + q;
-      if (c < a.Mp) out[(wi * nw2 + pix) * a.Mp + c] = mk(tiles[q].re[li][lj], tiles[q].im[li][lj]);
-    }
+    clap_store_tiles<R, NW>(a, tiles, out, wi, g, nw, nw2, inv_nw, tid);
   }
 }
 
@@ -608,7 +706,7 @@ static cudaError_t launch_clap_nw(const ClapArgs& a, const typename CT<R>::Tw& t
   const int64_t ntask = static_cast<int64_t>(a.nwi) * a.nwj * ((a.Mp + NW - 1) / NW);
   if (ntask <= 0) return cudaSuccess;
   const size_t sm = clap_smem_bytes<R, NW>();
-  cudaError_t e = cudaFuncSetAttribute(k_clap<R, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = kernel_attributes_once(sm);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clap<R, NW>, 32 * NW, sm);
@@ -1306,7 +1404,7 @@ template <int L>
 static cudaError_t topofit_geometry_l(const TopoArgs& a, int grid_cap, size_t* smem, int* blocks_out) {
   const int mpad = topofit_mpad(L, a.M);
   const size_t sm = topofit_smem_bytes(L, mpad);
-  cudaError_t e = cudaFuncSetAttribute(k_topofit_f32<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = kernel_attributes_once(sm);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_topofit_f32<L>, 128, sm);
@@ -1358,7 +1456,7 @@ cudaError_t launch_topofit(const TopoArgs& a, bool fp64, int grid_blocks, cudaSt
     int64_t need = (a.N + 7) / 8;
     const int blocks = static_cast<int>(std::min<int64_t>(need, grid_blocks));
     const size_t sm = static_cast<size_t>(8) * a.M * (sizeof(double2) + sizeof(double));
-    cudaError_t e = cudaFuncSetAttribute(k_topofit_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = kernel_attributes_once(sm);
     if (e != cudaSuccess) return e;
     k_topofit_f64<<<blocks, 256, sm, st>>>(a);
     return cudaGetLastError();
@@ -1635,7 +1733,7 @@ cudaError_t launch_random_hist(const double* rnd, int64_t n_rand, const double* 
                                const int64_t* ib, int small_baseline, int n_half, double cutoff0, double dbin,
                                int32_t* hist, int sm_count, cudaStream_t st) {
   const size_t sm = static_cast<size_t>(8) * 3 * m * sizeof(double);
-  cudaError_t e = cudaFuncSetAttribute(k_random_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = kernel_attributes_once(sm);
   if (e != cudaSuccess) return e;
   int64_t blocks = (n_rand + 7) / 8;
   if (blocks > static_cast<int64_t>(sm_count) * 8) blocks = static_cast<int64_t>(sm_count) * 8;
@@ -1770,7 +1868,7 @@ cudaError_t launch_s3_clap(const S3ClapArgs& a, const Twiddles32f& tf, int sm_co
   const int64_t ntask = a.n_jobs * a.ngroups;
   if (ntask <= 0) return cudaSuccess;
   const size_t sm = s3_clap_smem();
-  cudaError_t e = cudaFuncSetAttribute(k_s3_clap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = kernel_attributes_once(sm);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_s3_clap, 128, sm);
@@ -1966,7 +2064,7 @@ __global__ void __launch_bounds__(128) k_s3_fit(S3FitArgs a) {
 cudaError_t launch_s3_fit(const S3FitArgs& a, int sm_count, cudaStream_t st) {
   if (a.n_sel <= 0) return cudaSuccess;
   const size_t sm = 4 * a.warp_smem;
-  cudaError_t e = cudaFuncSetAttribute(k_s3_fit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = kernel_attributes_once(sm);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_s3_fit, 128, sm);
@@ -2101,7 +2199,7 @@ cudaError_t launch_batch_clap(const BatchArgs& b, int64_t total, const Twiddles3
                               cudaStream_t st) {
   if (total <= 0) return cudaSuccess;
   const size_t sm = clap_smem_bytes<float, 4>();
-  cudaError_t e = cudaFuncSetAttribute(k_batch_clap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = kernel_attributes_once(sm);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_clap, 128, sm);
@@ -2121,7 +2219,7 @@ template <int L>
 static cudaError_t batch_topofit_l(const BatchArgs& b, const int32_t* units, int n_units, int mpad_max, int sm_count,
                                    cudaStream_t st) {
   const size_t sm = topofit_smem_bytes(L, mpad_max);
-  cudaError_t e = cudaFuncSetAttribute(k_batch_topofit<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = kernel_attributes_once(sm);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_topofit<L>, 128, sm);
@@ -2630,8 +2728,7 @@ static size_t clap_bwd_smem() {
 template <typename R>
 static int clap_bwd_blocks(int sm_count) {
   const size_t sm = clap_bwd_smem<R>();
-  if (cudaFuncSetAttribute(k_clap_bwd<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
-    return 0;
+  if (kernel_attributes_once(sm) != cudaSuccess) return 0;
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clap_bwd<R>, 128, sm) != cudaSuccess) return 0;
   return sm_count * std::max(per_sm, 1);
@@ -2807,6 +2904,68 @@ cudaError_t launch_ph_weight(const BinArgs& a, int64_t N, bool fp64, const int32
   else
     k_ph_weight<float><<<148 * 8, 256, 0, st>>>(a, perm, N, static_cast<float2*>(out_orig));
   return cudaGetLastError();
+}
+
+
+// ====================================================== kernel attributes ==
+// Every kernel that may take more than 48 KB of dynamic shared memory is opted
+// in to the device's per-block maximum once per device and process, before its
+// first launch; a launch then only checks its request against that limit.
+// Kernel attributes are thereby never changed while another host thread
+// captures, instantiates or launches a graph that holds the same kernel
+// (contexts run concurrently from several threads).
+namespace {
+template <typename F>
+cudaError_t opt_in_smem(F* f, int optin) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, f);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              optin - static_cast<int>(fa.sharedSizeBytes));
+}
+
+constexpr int kMaxDevices = 64;
+std::once_flag g_attr_once[kMaxDevices];
+cudaError_t g_attr_result[kMaxDevices];
+int g_attr_optin[kMaxDevices];
+}  // namespace
+
+cudaError_t kernel_attributes_once(size_t dynamic_smem) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::call_once(g_attr_once[dev], [dev] {
+    int optin = 0;
+    const cudaError_t r = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const cudaError_t steps[] = {
+        r,
+        r == cudaSuccess ? opt_in_smem(k_clap<float, 8>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<double, 4>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_topofit_f32<4>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_topofit_f32<8>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_topofit_f32<16>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_topofit_f32<32>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_topofit_f64, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_random_hist, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_s3_clap, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_s3_fit, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_batch_clap, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_batch_topofit<4>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_batch_topofit<8>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_batch_topofit<16>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_batch_topofit<32>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap_bwd<float>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap_bwd<double>, optin) : r,
+    };
+    cudaError_t first = cudaSuccess;
+    for (const cudaError_t x : steps)
+      if (first == cudaSuccess && x != cudaSuccess) first = x;
+    g_attr_result[dev] = first;
+    g_attr_optin[dev] = optin;
+  });
+  if (g_attr_result[dev] != cudaSuccess) return g_attr_result[dev];
+  return dynamic_smem <= static_cast<size_t>(g_attr_optin[dev]) ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 }  // namespace ps2
