@@ -338,6 +338,7 @@ TopoArgs topo_args(ps2_ctx* c, void* K_out, void* C_out, void* coh_io) {
   t.Mp = c->Mp;
   t.n_half = c->n_half;
   t.zero_mode = 0;
+  t.filt_unit = c->fp64 ? 0 : 1;  // the loop's k_overlap stores f/|f| in FP32
   t.K_out = K_out;
   t.C_out = C_out;
   t.coh_io = coh_io;
@@ -418,7 +419,9 @@ int enqueue_iteration(ps2_ctx* c, bool later, bool force_continue, cudaEvent_t* 
   ++launched;
   if (ev) CK(cudaEventRecord(ev[1], c->st));
   CK(launch_clap(clap_args(c, c->grid.p, c->win.p), fp64, c->twf, c->twd, c->sm_count, c->st));
-  CK(launch_overlap(overlap_args(c, c->win.p, c->filt.p), fp64, c->st));
+  OverlapArgs ov = overlap_args(c, c->win.p, c->filt.p);
+  ov.normalize = fp64 ? 0 : 1;
+  CK(launch_overlap(ov, fp64, c->st));
   launched += 2;
   if (ev) CK(cudaEventRecord(ev[2], c->st));
   // K[1] keeps the K this iteration binned with (pm1's ph_weight needs it);
@@ -1576,6 +1579,7 @@ int ps2_batch_run(ps2_ctx* const* ctxs, int64_t n, ps2_iter_stats* last) {
     d.bin = bin_args(c, 0, c->K[0].p);
     d.clap = clap_args(c, c->grid.p, c->win.p);
     d.ov = overlap_args(c, c->win.p, c->filt.p);
+    d.ov.normalize = 1;
     d.topo = topo_args(c, c->K[0].p, c->C.p, c->coh.p);
     d.fin = finalize_args(c, false);
     d.K1 = c->K[1].as<float>();

@@ -753,7 +753,16 @@ __device__ __forceinline__ void overlap_elem(const OverlapArgs& a, const int64_t
         }
       }
     }
-    filt[idx] = mk(static_cast<R>(sx), static_cast<R>(sy));
+    C f = mk(static_cast<R>(sx), static_cast<R>(sy));
+    if constexpr (sizeof(R) == 4) {
+      if (a.normalize) {
+        // normalize_complex_unit_magnitude (:1186-1205) once per cell instead of
+        // once per PS of the cell in the topofit; the same expression, the same bits
+        const float mag = hypotf(f.x, f.y);
+        if (mag != 0.f) f = make_float2(f.x / mag, f.y / mag);
+      }
+    }
+    filt[idx] = f;
   }
 }
 
@@ -1040,8 +1049,10 @@ __device__ __forceinline__ void topofit_vblock(const TopoArgs& a, const int mpad
           } else {
             // extract_patch_phase + normalize_complex_unit_magnitude (:1186-1205)
             float2 f = fv[i];
-            const float mag = hypotf(f.x, f.y);
-            if (mag != 0.f) f = make_float2(f.x / mag, f.y / mag);
+            if (!a.filt_unit) {
+              const float mag = hypotf(f.x, f.y);
+              if (mag != 0.f) f = make_float2(f.x / mag, f.y / mag);
+            }
             if (ph_patch) ph_patch[s * M + c] = f;
             v = cmul_rn(conjf2(f), pv[i]);  // psdph (:687-689)
           }

@@ -52,6 +52,7 @@ struct OverlapArgs {
   const void* win_out;  // complex [W, n_win*n_win, Mp]
   void* filt;           // complex [G, Mp]
   int n_i, n_j, M, Mp, n_win, n_inc, nwi, nwj;
+  int normalize;        // 1 (FP32 stage-2 loop): store f/|f|, the unit patch phase the topofit reads
 };
 
 // --------------------------------------------------------------- topofit --
@@ -80,6 +81,7 @@ struct TopoArgs {
   void* ph_patch;         // complex [N, M]
   int accumulate_stats;   // 1: rms partials / histogram / invalid count
   int lanes;              // lanes per PS in the FP32 kernel (4, 8, 16, 32); 0: from n_ifg
+  int filt_unit;          // 1: filt already holds f/|f| (k_overlap with normalize), FP32 kernel
 };
 
 // -------------------------------------------------------------- finalize --
