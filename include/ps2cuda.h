@@ -249,6 +249,38 @@ int ps3_reestimate(const ps3_reestimate_desc* desc, ps3_reestimate_out* out, int
 int ps2_stage3_reestimate(ps2_ctx* ctx, const int64_t* sel, int64_t n_sel, const int64_t* fit_ifg, int64_t n_fit,
                           int64_t slc_osf, ps3_reestimate_out* out, int outputs_on_device);
 
+/* ---- one patch over several GPUs ------------------------------------------
+ * A patch split by rows into contiguous cell ranges, one range per rank (one
+ * GPU each): every rank loads a context with its rows only (ps2_load_patch of
+ * the sub-patch: same n_i, n_j, low-pass, Nr and parameters, rows in their
+ * original relative order) and iterates with
+ *   ps2_shard_bin(ctx, d_grid)          bin this rank's rows; copy the context's
+ *                                       grid (complex [n_i*n_j, Mp], Mp = M
+ *                                       rounded up to 4; complex128 for FP64)
+ *                                       to the device buffer d_grid
+ *   <sum d_grid over the ranks>         cells are disjoint: the sum is the grid
+ *                                       of the whole patch, bit for bit
+ *   ps2_shard_filter(ctx, d_grid, lo, hi)  copy the summed grid in; CLAP of the
+ *                                       windows meeting rows of cells lo..hi-1
+ *                                       and overlap-add of cells lo..hi-1
+ *   ps2_shard_fit(ctx, stats)           topofit of this rank's rows; stats (host,
+ *                                       PS2_SHARD_STATS doubles) = coherence
+ *                                       histogram [100], sum of squared changes,
+ *                                       invalid rows
+ *   <sum stats over the ranks>
+ *   ps2_shard_finalize(ctx, stats, n_total, &it)  the stop rule and the P-square
+ *                                       update from the summed statistics (the
+ *                                       same on every rank); loop while !it.stop
+ * Each call is synchronous on the context's stream. The reference iterates one
+ * patch on one host (native_stage2.rs:261-406); this split has no counterpart.
+ * Per-PS results equal a single-context run; the convergence RMS sums rank
+ * totals, so it can differ from it in the last bits. */
+#define PS2_SHARD_STATS (PS2_COH_BINS + 2)
+int ps2_shard_bin(ps2_ctx* ctx, void* d_grid);
+int ps2_shard_filter(ps2_ctx* ctx, const void* d_grid, int64_t cell_lo, int64_t cell_hi);
+int ps2_shard_fit(ps2_ctx* ctx, double* stats);
+int ps2_shard_finalize(ps2_ctx* ctx, const double* stats, int64_t n_total, ps2_iter_stats* out);
+
 /* ---- differentiable coherence (adjoints) ------------------------------------
  * The gamma map with K given, as a function of the input phases, K and the
  * CLAP parameters, on the loaded patch's geometry (cells, bperp, low-pass,

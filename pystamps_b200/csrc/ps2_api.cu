@@ -2006,4 +2006,127 @@ int ps2_stage3_reestimate(ps2_ctx* c, const int64_t* sel, int64_t n_sel, const i
   return PS2_OK;
 }
 
+
+// ------------------------------------------------ one patch over several GPUs
+// A patch whose rows are split by contiguous cell ranges: each rank's context
+// holds its rows and the full grid. One iteration is
+//   ps2_shard_bin      -> sum the ranks' grids (disjoint cells)
+//   ps2_shard_filter   (CLAP windows over the rank's rows of cells, overlap-add
+//                       of its cells)
+//   ps2_shard_fit      -> sum the ranks' statistics
+//   ps2_shard_finalize (the same finalize on every rank)
+// which is enqueue_iteration with the two exchanges cut in.
+
+int ps2_shard_bin(ps2_ctx* c, void* d_grid) {
+  if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "ps2_shard_bin: no patch loaded");
+  if (!d_grid) return set_err(PS2_ERR_INVALID_ARG, "ps2_shard_bin: NULL grid");
+  CK(cudaSetDevice(c->device));
+  const bool fp64 = c->fp64, later = c->iters_done > 0;
+  if (!c->psquare && later) {
+    TopoArgs t = topo_args(c, nullptr, nullptr, nullptr);
+    t.ph_res = c->ph_res.p;
+    CK(launch_snr_weight(t, c->amp.as<float>(), c->w.p, fp64, c->sm_count, c->st));
+  }
+  CK(cudaMemsetAsync(c->hist.p, 0, sizeof(int32_t) * PS2_COH_BINS, c->st));
+  CK(cudaMemsetAsync(c->n_invalid.p, 0, sizeof(int32_t), c->st));
+  CK(cudaMemsetAsync(c->rms_partial.p, 0, sizeof(double) * c->topo_blocks, c->st));
+  CK(launch_bin(bin_args(c, (later && c->psquare) ? 1 : 0, c->K[0].p), fp64, c->sm_count, c->st));
+  CK(cudaMemcpyAsync(d_grid, c->grid.p, csz(c) * c->G * c->Mp, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return PS2_OK;
+}
+
+int ps2_shard_filter(ps2_ctx* c, const void* d_grid, int64_t cell_lo, int64_t cell_hi) {
+  if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "ps2_shard_filter: no patch loaded");
+  if (!d_grid) return set_err(PS2_ERR_INVALID_ARG, "ps2_shard_filter: NULL grid");
+  if (cell_lo < 0 || cell_hi > c->G || cell_lo > cell_hi)
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_shard_filter: cells [%lld, %lld) outside 0..%lld", (long long)cell_lo,
+                   (long long)cell_hi, (long long)c->G);
+  CK(cudaSetDevice(c->device));
+  const bool fp64 = c->fp64;
+  CK(cudaMemcpyAsync(c->grid.p, d_grid, csz(c) * c->G * c->Mp, cudaMemcpyDeviceToDevice, c->st));
+  if (cell_hi > cell_lo && static_cast<int64_t>(c->nwi) * c->nwj > 0) {
+    // windows whose rows of cells meet rows cell_lo / n_j .. (cell_hi - 1) / n_j
+    // (clap_windows, native_stage2.rs:957-995: window ix1 covers rows
+    // min(ix1 * n_inc, n_i - n_win) .. + n_win - 1)
+    const int64_t r_lo = cell_lo / c->n_j, r_hi = (cell_hi - 1) / c->n_j;
+    int64_t ix_lo = -1, ix_hi = -1;
+    for (int64_t ix = 0; ix < c->nwi; ++ix) {
+      const int64_t i1 = std::min<int64_t>(ix * c->n_inc, c->n_i - c->n_win);
+      if (i1 <= r_hi && i1 + c->n_win - 1 >= r_lo) {
+        if (ix_lo < 0) ix_lo = ix;
+        ix_hi = ix;
+      }
+    }
+    if (ix_lo >= 0) {
+      ClapArgs ca = clap_args(c, c->grid.p, c->win.p);
+      ca.w_lo = ix_lo * c->nwj;
+      ca.w_n = (ix_hi - ix_lo + 1) * c->nwj;
+      CK(launch_clap(ca, fp64, c->twf, c->twd, c->sm_count, c->st));
+    }
+  }
+  if (cell_hi > cell_lo) {
+    OverlapArgs ov = overlap_args(c, c->win.p, c->filt.p);
+    ov.normalize = fp64 ? 0 : 1;
+    ov.cell_lo = cell_lo;
+    ov.cell_n = cell_hi - cell_lo;
+    CK(launch_overlap(ov, fp64, c->st));
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return PS2_OK;
+}
+
+int ps2_shard_fit(ps2_ctx* c, double* stats) {
+  if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "ps2_shard_fit: no patch loaded");
+  if (!stats) return set_err(PS2_ERR_INVALID_ARG, "ps2_shard_fit: NULL statistics");
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpyAsync(c->K[1].p, c->K[0].p, rsz(c) * c->N, cudaMemcpyDeviceToDevice, c->st));
+  TopoArgs t = topo_args(c, c->K[0].p, c->C.p, c->coh.p);
+  if (!c->psquare) t.ph_res = c->ph_res.p;
+  CK(launch_topofit(t, c->fp64, c->topo_blocks, c->st));
+  std::vector<int32_t> hist(PS2_COH_BINS);
+  std::vector<double> part(static_cast<size_t>(c->topo_blocks));
+  int32_t inv = 0;
+  CK(cudaMemcpyAsync(hist.data(), c->hist.p, sizeof(int32_t) * PS2_COH_BINS, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(part.data(), c->rms_partial.p, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(&inv, c->n_invalid.p, sizeof(int32_t), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  double sum = 0.0;
+  for (const double v : part) sum += v;
+  for (int i = 0; i < PS2_COH_BINS; ++i) stats[i] = static_cast<double>(hist[i]);
+  stats[PS2_COH_BINS] = sum;
+  stats[PS2_COH_BINS + 1] = static_cast<double>(inv);
+  return PS2_OK;
+}
+
+int ps2_shard_finalize(ps2_ctx* c, const double* stats, int64_t n_total, ps2_iter_stats* out) {
+  if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "ps2_shard_finalize: no patch loaded");
+  if (!stats) return set_err(PS2_ERR_INVALID_ARG, "ps2_shard_finalize: NULL statistics");
+  if (n_total < c->N) return set_err(PS2_ERR_INVALID_ARG, "ps2_shard_finalize: n_total %lld < this shard's %lld rows",
+                                     (long long)n_total, (long long)c->N);
+  CK(cudaSetDevice(c->device));
+  std::vector<int32_t> hist(PS2_COH_BINS);
+  for (int i = 0; i < PS2_COH_BINS; ++i) {
+    const double v = stats[i];
+    if (!(v >= 0.0) || v > 2147483647.0)
+      return set_err(PS2_ERR_INVALID_ARG, "ps2_shard_finalize: histogram bin %d = %g", i, v);
+    hist[i] = static_cast<int32_t>(v);
+  }
+  const int32_t inv = static_cast<int32_t>(stats[PS2_COH_BINS + 1]);
+  const double sum = stats[PS2_COH_BINS];
+  CK(cudaMemcpyAsync(c->hist.p, hist.data(), sizeof(int32_t) * PS2_COH_BINS, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemsetAsync(c->rms_partial.p, 0, sizeof(double) * c->topo_blocks, c->st));
+  CK(cudaMemcpyAsync(c->rms_partial.p, &sum, sizeof(double), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->n_invalid.p, &inv, sizeof(int32_t), cudaMemcpyHostToDevice, c->st));
+  FinalizeArgs f = finalize_args(c, false);
+  f.N = n_total;
+  CK(launch_finalize(f, c->st));
+  CK(cudaMemcpyAsync(c->h_stats, c->stats.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  fill_stats(c->h_stats, &c->last);
+  c->iters_done += 1;
+  if (out) *out = c->last;
+  return PS2_OK;
+}
+
 }  // extern "C"

@@ -624,7 +624,7 @@ __device__ __forceinline__ void clap_task(const ClapArgs& a, const int64_t task,
   C* __restrict__ out = static_cast<C*>(a.win_out);
   auto& T = tiles[warp];
   {
-    const int64_t wi = task / ngroups;
+    const int64_t wi = a.w_lo + task / ngroups;
     const int g = static_cast<int>(task - wi * ngroups);
     const int ix1 = static_cast<int>(wi / a.nwj), ix2 = static_cast<int>(wi - static_cast<int64_t>(ix1) * a.nwj);
     // clap_windows (native_stage2.rs:957-995)
@@ -691,7 +691,8 @@ __global__ void __launch_bounds__(32 * NW) k_clap(ClapArgs a, typename CT<R>::Tw
   R g7[7];
 #pragma unroll
   for (int i = 0; i < 7; ++i) g7[i] = static_cast<R>(a.g7[i]);
-  const int64_t ntask = static_cast<int64_t>(a.nwi) * a.nwj * clap_groups<R, NW>(a);
+  const int64_t nwin = a.w_n > 0 ? a.w_n : static_cast<int64_t>(a.nwi) * a.nwj;
+  const int64_t ntask = nwin * clap_groups<R, NW>(a);
   for (int64_t task = blockIdx.x; task < ntask; task += gridDim.x)
     clap_task<R, NW>(a, task, m.tiles, m.twf, m.twi, m.lp, m.wt, g7);
 }
@@ -703,7 +704,8 @@ static size_t clap_smem_bytes() {
 
 template <typename R, int NW>
 static cudaError_t launch_clap_nw(const ClapArgs& a, const typename CT<R>::Tw& tw, int sm_count, cudaStream_t st) {
-  const int64_t ntask = static_cast<int64_t>(a.nwi) * a.nwj * ((a.Mp + NW - 1) / NW);
+  const int64_t nwin = a.w_n > 0 ? a.w_n : static_cast<int64_t>(a.nwi) * a.nwj;
+  const int64_t ntask = nwin * ((a.Mp + NW - 1) / NW);
   if (ntask <= 0) return cudaSuccess;
   const size_t sm = clap_smem_bytes<R, NW>();
   cudaError_t e = kernel_attributes_once(sm);
@@ -768,14 +770,16 @@ __device__ __forceinline__ void overlap_elem(const OverlapArgs& a, const int64_t
 
 template <typename R>
 __global__ void __launch_bounds__(256) k_overlap(OverlapArgs a) {
-  const int64_t total = static_cast<int64_t>(a.n_i) * a.n_j * a.Mp;
+  const int64_t cells = a.cell_n > 0 ? a.cell_n : static_cast<int64_t>(a.n_i) * a.n_j;
+  const int64_t total = cells * a.Mp, base = a.cell_lo * a.Mp;
   for (int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
        idx += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    overlap_elem<R>(a, idx);
+    overlap_elem<R>(a, base + idx);
 }
 
 cudaError_t launch_overlap(const OverlapArgs& a, bool fp64, cudaStream_t st) {
-  const int64_t total = static_cast<int64_t>(a.n_i) * a.n_j * a.Mp;
+  const int64_t cells = a.cell_n > 0 ? a.cell_n : static_cast<int64_t>(a.n_i) * a.n_j;
+  const int64_t total = cells * a.Mp;
   int64_t blocks = (total + 255) / 256;
   if (blocks > 148 * 32) blocks = 148 * 32;
   if (blocks < 1) blocks = 1;

@@ -46,6 +46,7 @@ struct ClapArgs {
   const double* wscaled;   // [n_win*n_win] pyramid weight / 1024 (device)
   double g7[7];            // 7-tap Gaussian of the |H| smoothing
   void* win_out;           // complex [W, n_win*n_win, Mp]
+  int64_t w_lo, w_n;       // windows w_lo .. w_lo + w_n - 1 (w_n = 0: all windows)
 };
 
 struct OverlapArgs {
@@ -53,6 +54,7 @@ struct OverlapArgs {
   void* filt;           // complex [G, Mp]
   int n_i, n_j, M, Mp, n_win, n_inc, nwi, nwj;
   int normalize;        // 1 (FP32 stage-2 loop): store f/|f|, the unit patch phase the topofit reads
+  int64_t cell_lo, cell_n;  // cells cell_lo .. cell_lo + cell_n - 1 (cell_n = 0: all cells)
 };
 
 // --------------------------------------------------------------- topofit --
