@@ -85,55 +85,48 @@ __device__ __forceinline__ void bin_task(const BinArgs& a, const int64_t task, c
     const int chunk = static_cast<int>(task - cell * a.nchunk);
     const int c = chunk * 32 + lane;
     const bool active = c < a.M;
-    const bool write_w = a.mode == 1 && chunk == 0;
+    const bool write_w = a.mode == 1 && chunk == 0 && lane == 0;
     const int s0 = a.cell_start[cell], s1 = a.cell_start[cell + 1];
     R ax = R(0), ay = R(0);
-    // rows in batches of 32: lane l evaluates the weight and reads K of row
-    // sb + l once, the batch's rows take them by shuffle; inside a batch rows go
-    // four at a time with every load issued before the arithmetic, and the sum
-    // itself stays sequential in row order
-    for (int sb = s0; sb < s1; sb += 32) {
-      const int sl = sb + lane;
-      R wl = R(0), kl = R(0);
-      if (sl < s1) {
-        wl = bin_weight<R>(a, W, coh, sl);
-        if (a.mode != 3) kl = K[sl];
-        if (write_w) W[sl] = wl;
-      }
-      const int nb = min(32, s1 - sb);
-      for (int j0 = 0; j0 < nb; j0 += 4) {
-        R wv[4], kv[4], bv[4];
-        float2 v[4];
+    // rows are taken four at a time with every load issued before the
+    // arithmetic; the sum itself stays sequential in row order
+    for (int sb = s0; sb < s1; sb += 4) {
+      R wv[4], kv[4], bv[4];
+      float2 v[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int s = sb + j0 + i;
-          wv[i] = __shfl_sync(kFull, wl, (j0 + i) & 31);
-          kv[i] = __shfl_sync(kFull, kl, (j0 + i) & 31);
-          bv[i] = R(0);
-          v[i] = make_float2(0.f, 0.f);
-          if (s < s1 && active) {
+      for (int i = 0; i < 4; ++i) {
+        const int s = sb + i;
+        wv[i] = R(0);
+        kv[i] = R(0);
+        bv[i] = R(0);
+        v[i] = make_float2(0.f, 0.f);
+        if (s < s1) {
+          wv[i] = bin_weight<R>(a, W, coh, s);
+          if (a.mode != 3) kv[i] = K[s];
+          if (active) {
             v[i] = ph[static_cast<int64_t>(s) * M + c];
             if (a.mode != 3)
               bv[i] = a.bp_row_inv ? static_cast<R>(bp[c]) : static_cast<R>(bp[static_cast<int64_t>(s) * M + c]);
           }
         }
+      }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int s = sb + j0 + i;
-          if (s >= s1) break;
-          if (!active) continue;
-          if (a.mode == 3) {
-            // accumulate_grid alone: ph_nm holds ph_weight, no ramp and no weight
-            ax = add_rn(ax, static_cast<R>(v[i].x));
-            ay = add_rn(ay, static_cast<R>(v[i].y));
-          } else {
-            const R phs = -(bv[i] * kv[i]);
-            R sn, cs;
-            sincos_r(phs, &sn, &cs);
-            const C r = cmul_rn(mk(static_cast<R>(v[i].x), static_cast<R>(v[i].y)), mk(cs, sn));
-            ax = add_rn(ax, mul_rn(r.x, wv[i]));
-            ay = add_rn(ay, mul_rn(r.y, wv[i]));
-          }
+      for (int i = 0; i < 4; ++i) {
+        const int s = sb + i;
+        if (s >= s1) break;
+        if (write_w) W[s] = wv[i];
+        if (!active) continue;
+        if (a.mode == 3) {
+          // accumulate_grid alone: ph_nm holds ph_weight, no ramp and no weight
+          ax = add_rn(ax, static_cast<R>(v[i].x));
+          ay = add_rn(ay, static_cast<R>(v[i].y));
+        } else {
+          const R phs = -(bv[i] * kv[i]);
+          R sn, cs;
+          sincos_r(phs, &sn, &cs);
+          const C r = cmul_rn(mk(static_cast<R>(v[i].x), static_cast<R>(v[i].y)), mk(cs, sn));
+          ax = add_rn(ax, mul_rn(r.x, wv[i]));
+          ay = add_rn(ay, mul_rn(r.y, wv[i]));
         }
       }
     }
@@ -221,6 +214,10 @@ struct ClapTileT {
 };
 template <typename R>
 using ClapTile = ClapTileT<R, 8>;
+
+// Row stride of the pyramid-weight table in shared memory: lane l reads row l,
+// so rows 33 words apart put the 32 lanes on 32 different banks.
+constexpr int kWtStride = 33;
 
 // warps per CLAP block and the matching tile stagger
 template <int NW>
@@ -485,7 +482,7 @@ __device__ __forceinline__ void clap_window_warp(Tile& T, const int lane, const 
     fft_pass<R>(T.re, T.im, twi, lane, true);
     const bool row_zero = lane < rs;
     for (int l = 0; l < a.n_win; ++l) {
-      const R wv = (row_zero || l < cs) ? R(0) : wt[(lane - rs) * a.n_win + (l - cs)];
+      const R wv = (row_zero || l < cs) ? R(0) : wt[(lane - rs) * kWtStride + (l - cs)];
       T.re[lane][l] *= wv;
       T.im[lane][l] *= wv;
     }
@@ -499,7 +496,8 @@ template <typename R>
 __device__ __forceinline__ void clap_consts(const ClapArgs& a, R* lp, R* wt) {
   const int nw2 = a.n_win * a.n_win;
   for (int i = threadIdx.x; i < 1024; i += blockDim.x) lp[i] = static_cast<R>(a.low_pass[i]);
-  for (int i = threadIdx.x; i < nw2; i += blockDim.x) wt[i] = static_cast<R>(a.wscaled[i]);
+  for (int i = threadIdx.x; i < nw2; i += blockDim.x)
+    wt[(i / a.n_win) * kWtStride + i % a.n_win] = static_cast<R>(a.wscaled[i]);
 }
 
 // Window loads and stores of a CLAP block: NW interferograms of one window,
@@ -674,7 +672,7 @@ __device__ __forceinline__ ClapSmem<R, NW> clap_smem(unsigned char* raw, const t
   m.tiles = reinterpret_cast<ClapTileT<R, ClapShape<NW>::kPad>*>(raw);
   m.lp = reinterpret_cast<R*>(m.tiles + NW);
   m.wt = m.lp + 1024;
-  m.twf = reinterpret_cast<typename CT<R>::C*>(m.wt + 1024);
+  m.twf = reinterpret_cast<typename CT<R>::C*>(m.wt + 32 * kWtStride);
   m.twi = m.twf + 16;
   if (threadIdx.x < 16) {
     m.twf[threadIdx.x] = tw.w[threadIdx.x];
@@ -699,7 +697,7 @@ __global__ void __launch_bounds__(32 * NW) k_clap(ClapArgs a, typename CT<R>::Tw
 
 template <typename R, int NW>
 static size_t clap_smem_bytes() {
-  return NW * sizeof(ClapTileT<R, ClapShape<NW>::kPad>) + (1024 + 1024) * sizeof(R) + 32 * 2 * sizeof(R);
+  return NW * sizeof(ClapTileT<R, ClapShape<NW>::kPad>) + (1024 + 32 * kWtStride) * sizeof(R) + 32 * 2 * sizeof(R);
 }
 
 template <typename R, int NW>
