@@ -41,9 +41,10 @@ METRIC = "Stage-2 PSÃ—ifg/s per gamma iter, FP32 vs plain FP64 GPU at max|Î”Î³|â
 UNIT = "PS*ifg/s"
 FP32_LANES_PER_SM = 128
 # DRAM bytes (read + write) per PS x ifg of one k_topofit_f32 launch, from the ncu
-# capture at 250,000 PS x 60 ifg in profiles/kernels_precision_250k_ps_60_ifg.md
-# (195.5 MB per launch); the reported traffic scales it by N x M.
-TOPOFIT_TRAFFIC_BYTES_PER_PS_IFG = 195.5e6 / (250_000 * 60)
+# capture of the full-scale shape at 250,000 PS x 150 ifg (256x256 grid) in
+# profiles/kernels_full_scale_shape_250k_ps_150_ifg.md (536.6 MB per launch); the
+# reported traffic scales it by N x M.
+TOPOFIT_TRAFFIC_BYTES_PER_PS_IFG = 536.6e6 / (250_000 * 150)
 
 
 def parse():
@@ -355,7 +356,7 @@ def run_ours(args, rank: int, world: int, dist):
         "kernel": "k_topofit_f32", "bound": "fp32", "achieved": achieved, "peak": fp32_peak_tflops,
         "unit": "TFLOP/s", "frac": achieved / fp32_peak_tflops,
         "traffic": TOPOFIT_TRAFFIC_BYTES_PER_PS_IFG * n * m,
-        "traffic_source": "ncu dram__bytes_read+write at 250k PS x 60 ifg scaled by PS x ifg",
+        "traffic_source": "ncu dram__bytes_read+write at 250k PS x 150 ifg (256x256 grid) scaled by PS x ifg",
         "algorithmic": f"(8*T+32) flop per PS x ifg, T={T}: {flops:.3e} flop per launch",
         "peak_source": f"nominal FP32 FMA rate {sms} SM x {FP32_LANES_PER_SM} lanes x 2 x {sm_max:.0f} MHz "
                        "(MEASURED_PEAKS.json has no FP32 figure)",
@@ -364,7 +365,9 @@ def run_ours(args, rank: int, world: int, dist):
     bin_roof = {"kernel": "k_bin", "bound": "hbm", "achieved": bin_bytes / (bin_ms / 1e3) / 1e9,
                 "peak": float(peaks.get("hbm_gbs", 6650.0)), "unit": "GB/s",
                 "frac": bin_bytes / (bin_ms / 1e3) / 1e9 / float(peaks.get("hbm_gbs", 6650.0)),
-                "algorithmic": "12 B per PS x ifg (ph_nm c64 + bperp f32) + 8 B per cell x ifg"}
+                "algorithmic": "12 B per PS x ifg (ph_nm c64 + bperp f32) + 8 B per cell x ifg",
+                "peak_source": ("fallback 6.65 TB/s (MEASURED_PEAKS.json absent)" if peaks.get("fallback")
+                                else "measured copy bandwidth, MEASURED_PEAKS.json hbm_gbs")}
     ctx.close()
 
     # ---------------- plain FP64 GPU path ------------------------------------

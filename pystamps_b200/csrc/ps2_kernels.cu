@@ -88,13 +88,13 @@ __device__ __forceinline__ void bin_task(const BinArgs& a, const int64_t task, c
     const bool write_w = a.mode == 1 && chunk == 0 && lane == 0;
     const int s0 = a.cell_start[cell], s1 = a.cell_start[cell + 1];
     R ax = R(0), ay = R(0);
-    // rows are taken four at a time with every load issued before the
+    // rows are taken eight at a time with every load issued before the
     // arithmetic; the sum itself stays sequential in row order
-    for (int sb = s0; sb < s1; sb += 4) {
-      R wv[4], kv[4], bv[4];
-      float2 v[4];
+    for (int sb = s0; sb < s1; sb += 8) {
+      R wv[8], kv[8], bv[8];
+      float2 v[8];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
+      for (int i = 0; i < 8; ++i) {
         const int s = sb + i;
         wv[i] = R(0);
         kv[i] = R(0);
@@ -111,7 +111,7 @@ __device__ __forceinline__ void bin_task(const BinArgs& a, const int64_t task, c
         }
       }
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
+      for (int i = 0; i < 8; ++i) {
         const int s = sb + i;
         if (s >= s1) break;
         if (write_w) W[s] = wv[i];
