@@ -238,6 +238,11 @@ struct ps2_ctx {
   // each row in the caller's order, its cell-sorted position and its cell
   std::vector<int32_t> h_sorted_pos, h_cell;
   int64_t gmax_i = 0, gmax_j = 0;
+  // ps2_load_patch: the phase and bperp rows go up on this copy stream while the
+  // host sorts the rows by cell
+  cudaStream_t cst = nullptr;
+  cudaEvent_t ev_ph = nullptr, ev_bp = nullptr;
+  DevBuf stage_bp;
   // batches led by this context (ps2_batch_run): per-patch arguments and tables
   DevBuf bt;
   int* h_active = nullptr;  // pinned [1]
@@ -556,6 +561,10 @@ void ps2_destroy(ps2_ctx* c) {
   drop_loop_graph(c);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
   if (c->ad_ev) cudaEventDestroy(c->ad_ev);
+  c->stage_bp.release();
+  if (c->ev_ph) cudaEventDestroy(c->ev_ph);
+  if (c->ev_bp) cudaEventDestroy(c->ev_bp);
+  if (c->cst) cudaStreamDestroy(c->cst);
   c->bt.release();
   if (c->h_active) cudaFreeHost(c->h_active);
   if (c->h_stats) cudaFreeHost(c->h_stats);
@@ -611,6 +620,28 @@ int ps2_load_patch(ps2_ctx* c, const ps2_patch_desc* d) {
   const bool dev = d->pointers_on_device != 0;
   const int64_t N = c->N, M = c->M, G = c->G;
 
+  // The phase rows (and per-row bperp) start up the copy stream first, so the
+  // transfer overlaps the host's cell sort; the gathers below wait for them.
+  // Every return from here on waits for these copies (the caller's buffers are
+  // not kept past the call).
+  if (!c->cst) CK(cudaStreamCreateWithFlags(&c->cst, cudaStreamNonBlocking));
+  if (!c->ev_ph) CK(cudaEventCreateWithFlags(&c->ev_ph, cudaEventDisableTiming));
+  if (!c->ev_bp) CK(cudaEventCreateWithFlags(&c->ev_bp, cudaEventDisableTiming));
+  CK(cudaStreamSynchronize(c->st));
+  struct CopyJoin {
+    cudaStream_t s;
+    ~CopyJoin() { cudaStreamSynchronize(s); }
+  } join{c->cst};
+  const cudaMemcpyKind kind = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  CK(c->stage.alloc(sizeof(float) * 2 * N * M));
+  CK(cudaMemcpyAsync(c->stage.p, d->ph_nm, sizeof(float) * 2 * N * M, kind, c->cst));
+  CK(cudaEventRecord(c->ev_ph, c->cst));
+  if (!c->bp_row_inv) {
+    CK(c->stage_bp.alloc(sizeof(float) * N * M));
+    CK(cudaMemcpyAsync(c->stage_bp.p, d->bperp, sizeof(float) * N * M, kind, c->cst));
+    CK(cudaEventRecord(c->ev_bp, c->cst));
+  }
+
   // stable counting sort of rows by cell (host)
   std::vector<int64_t> gl(N);
   if (dev)
@@ -637,9 +668,13 @@ int ps2_load_patch(ps2_ctx* c, const ps2_patch_desc* d) {
       cell_of[s] = static_cast<int32_t>(gl[r]);
       c->h_sorted_pos[r] = s;
       c->h_cell[r] = static_cast<int32_t>(gl[r]);
-      c->gmax_i = std::max<int64_t>(c->gmax_i, gl[r] / c->n_j + 1);
-      c->gmax_j = std::max<int64_t>(c->gmax_j, gl[r] % c->n_j + 1);
     }
+  }
+  // largest 1-based grid row and column holding a PS (from the occupied cells)
+  for (int64_t g = 0; g < G; ++g) {
+    if (start[g + 1] == start[g]) continue;
+    c->gmax_i = std::max<int64_t>(c->gmax_i, g / c->n_j + 1);
+    c->gmax_j = std::max<int64_t>(c->gmax_j, g % c->n_j + 1);
   }
 
   const size_t R = rsz(c), Cz = csz(c);
@@ -650,21 +685,16 @@ int ps2_load_patch(ps2_ctx* c, const ps2_patch_desc* d) {
   CK(c->cell_of.alloc(sizeof(int32_t) * N));
   CK(cudaMemcpyAsync(c->cell_of.p, cell_of.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, c->st));
   // row data, gathered into cell order on the device
-  {
-    rc = copy_in(c, c->stage, d->ph_nm, sizeof(float) * 2 * N * M, dev);
-    if (rc) return rc;
-    CK(c->ph_nm.alloc(sizeof(float) * 2 * N * M));
-    CK(launch_gather_rows(c->stage.p, c->ph_nm.p, c->perm.as<int32_t>(), N, sizeof(float) * 2 * M, c->st));
-  }
+  CK(c->ph_nm.alloc(sizeof(float) * 2 * N * M));
+  CK(cudaStreamWaitEvent(c->st, c->ev_ph, 0));
+  CK(launch_gather_rows(c->stage.p, c->ph_nm.p, c->perm.as<int32_t>(), N, sizeof(float) * 2 * M, c->st));
   if (c->bp_row_inv) {
     rc = copy_in(c, c->bp, d->bperp, sizeof(float) * M, dev);
     if (rc) return rc;
   } else {
-    // the staging buffer is free again once the ph_nm gather (same stream) ran
-    rc = copy_in(c, c->stage, d->bperp, sizeof(float) * N * M, dev);
-    if (rc) return rc;
     CK(c->bp.alloc(sizeof(float) * N * M));
-    CK(launch_gather_rows(c->stage.p, c->bp.p, c->perm.as<int32_t>(), N, sizeof(float) * M, c->st));
+    CK(cudaStreamWaitEvent(c->st, c->ev_bp, 0));
+    CK(launch_gather_rows(c->stage_bp.p, c->bp.p, c->perm.as<int32_t>(), N, sizeof(float) * M, c->st));
   }
   if (!c->psquare) {
     rc = copy_in(c, c->stage, d->amp, sizeof(float) * N * M, dev);
