@@ -370,12 +370,13 @@ __device__ __forceinline__ R warp_median1024_pair(const R (&o)[32], R* scratch, 
 }
 
 // One 32-point FFT per lane over a row (rows = true, lane = row) or a column
-// (lane = column) of the tile, in place. Not inlined: the window code calls it
-// four times and one copy keeps the kernel inside the instruction cache.
+// (lane = column) of the tile, in place. The direction is a template parameter
+// (every shared-memory access then has one address form); not inlined: the
+// window code calls it four times and two copies keep the kernel inside the
+// instruction cache.
 // tw holds e^{-2 pi i k/32} (forward) or its conjugate (inverse), k < 16.
-template <typename R>
-__device__ __noinline__ void fft_pass(R (*re)[33], R (*im)[33], const typename CT<R>::C* tw, const int lane,
-                                      const bool rows) {
+template <typename R, bool rows>
+__device__ __noinline__ void fft_pass_t(R (*re)[33], R (*im)[33], const typename CT<R>::C* tw, const int lane) {
   using C = typename CT<R>::C;
   C x[32];
 #pragma unroll
@@ -415,6 +416,15 @@ __device__ __noinline__ void fft_pass(R (*re)[33], R (*im)[33], const typename C
       im[k][lane] = x[k].y;
     }
   }
+}
+
+template <typename R>
+__device__ __forceinline__ void fft_pass(R (*re)[33], R (*im)[33], const typename CT<R>::C* tw, const int lane,
+                                         const bool rows) {
+  if (rows)
+    fft_pass_t<R, true>(re, im, tw, lane);
+  else
+    fft_pass_t<R, false>(re, im, tw, lane);
 }
 
 // One window of one interferogram, computed by one warp in its tile.
