@@ -54,11 +54,11 @@ __device__ __forceinline__ float2 mk(float a, float b) { return make_float2(a, b
 __device__ __forceinline__ double2 mk(double a, double b) { return make_double2(a, b); }
 
 // ============================================================= binning ====
-template <typename R>
+template <typename R, int MODE>
 __device__ __forceinline__ R bin_weight(const BinArgs& a, const R* __restrict__ W, const R* __restrict__ coh,
                                         const int s) {
-  if (a.mode == 3) return R(1);
-  if (a.mode != 1) return W[s];
+  if (MODE == 3) return R(1);
+  if (MODE != 1) return W[s];
   // psquare_weighting lookup (native_stage2.rs:1674-1682)
   const double v = __dmul_rn(static_cast<double>(coh[s]), 1000.0);
   double r = v >= 0.0 ? floor(__dadd_rn(v, 0.5)) : ceil(__dsub_rn(v, 0.5));
@@ -70,8 +70,8 @@ __device__ __forceinline__ R bin_weight(const BinArgs& a, const R* __restrict__ 
 
 // One warp-task of the binning: cell `task / nchunk`, interferograms
 // 32 * (task % nchunk) + lane.
-template <typename R>
-__device__ __forceinline__ void bin_task(const BinArgs& a, const int64_t task, const int lane) {
+template <typename R, int MODE, bool ROWINV>
+__device__ __forceinline__ void bin_task_t(const BinArgs& a, const int64_t task, const int lane) {
   using C = typename CT<R>::C;
   const float2* __restrict__ ph = static_cast<const float2*>(a.ph_nm);
   const R* __restrict__ K = static_cast<const R*>(a.K);
@@ -85,7 +85,7 @@ __device__ __forceinline__ void bin_task(const BinArgs& a, const int64_t task, c
     const int chunk = static_cast<int>(task - cell * a.nchunk);
     const int c = chunk * 32 + lane;
     const bool active = c < a.M;
-    const bool write_w = a.mode == 1 && chunk == 0 && lane == 0;
+    const bool write_w = MODE == 1 && chunk == 0 && lane == 0;
     const int s0 = a.cell_start[cell], s1 = a.cell_start[cell + 1];
     R ax = R(0), ay = R(0);
     // rows are taken eight at a time with every load issued before the
@@ -101,12 +101,12 @@ __device__ __forceinline__ void bin_task(const BinArgs& a, const int64_t task, c
         bv[i] = R(0);
         v[i] = make_float2(0.f, 0.f);
         if (s < s1) {
-          wv[i] = bin_weight<R>(a, W, coh, s);
-          if (a.mode != 3) kv[i] = K[s];
+          wv[i] = bin_weight<R, MODE>(a, W, coh, s);
+          if (MODE != 3) kv[i] = K[s];
           if (active) {
             v[i] = ph[static_cast<int64_t>(s) * M + c];
-            if (a.mode != 3)
-              bv[i] = a.bp_row_inv ? static_cast<R>(bp[c]) : static_cast<R>(bp[static_cast<int64_t>(s) * M + c]);
+            if (MODE != 3)
+              bv[i] = ROWINV ? static_cast<R>(bp[c]) : static_cast<R>(bp[static_cast<int64_t>(s) * M + c]);
           }
         }
       }
@@ -116,7 +116,7 @@ __device__ __forceinline__ void bin_task(const BinArgs& a, const int64_t task, c
         if (s >= s1) break;
         if (write_w) W[s] = wv[i];
         if (!active) continue;
-        if (a.mode == 3) {
+        if (MODE == 3) {
           // accumulate_grid alone: ph_nm holds ph_weight, no ramp and no weight
           ax = add_rn(ax, static_cast<R>(v[i].x));
           ay = add_rn(ay, static_cast<R>(v[i].y));
@@ -132,6 +132,18 @@ __device__ __forceinline__ void bin_task(const BinArgs& a, const int64_t task, c
     }
     if (c < a.Mp) grid[cell * a.Mp + c] = active ? mk(ax, ay) : mk(R(0), R(0));
   }
+}
+
+// The weighting mode and the row invariance of bperp are compile-time in the
+// task body (no per-element branches on them).
+template <typename R>
+__device__ __forceinline__ void bin_task(const BinArgs& a, const int64_t task, const int lane) {
+  if (a.mode == 3)
+    bin_task_t<R, 3, false>(a, task, lane);
+  else if (a.mode == 1)
+    a.bp_row_inv ? bin_task_t<R, 1, true>(a, task, lane) : bin_task_t<R, 1, false>(a, task, lane);
+  else
+    a.bp_row_inv ? bin_task_t<R, 0, true>(a, task, lane) : bin_task_t<R, 0, false>(a, task, lane);
 }
 
 template <typename R>
@@ -996,9 +1008,9 @@ __device__ __forceinline__ void sweep_pairs(const ColumnSmem& cs, const float qr
 // groups s0 = (vb * 4 + warp) * G + k * nvb * 4 * G. The batched kernel runs
 // the same virtual blocks, so a patch's per-block rms partials, and with them
 // its stop decisions, are the same as when it runs alone.
-template <int L>
-__device__ __forceinline__ void topofit_vblock(const TopoArgs& a, const int mpad, const int vb, const int nvb,
-                                               unsigned char* smem_raw, int* sh_hist, double* sh_rms, int* sh_inv) {
+template <int L, bool LOOP, bool ROWINV>
+__device__ __forceinline__ void topofit_vblock_t(const TopoArgs& a, const int mpad, const int vb, const int nvb,
+                                                 unsigned char* smem_raw, int* sh_hist, double* sh_rms, int* sh_inv) {
   constexpr int G = 32 / L;
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   const int g = lane / L, gl = lane % L;
@@ -1027,7 +1039,7 @@ __device__ __forceinline__ void topofit_vblock(const TopoArgs& a, const int mpad
   for (int64_t s0 = (static_cast<int64_t>(vb) * 4 + wib) * G; s0 < a.N; s0 += step) {
     const int64_t s = s0 + g;
     const bool active = s < a.N;
-    const int64_t cell = (active && !cpx) ? a.cell_of[s] : 0;
+    const int64_t cell = (active && LOOP) ? a.cell_of[s] : 0;
     bool zero = false, nonzero = false;
     float mn = __int_as_float(0x7f800000), mx = -mn;
     // four columns per round with their global loads issued first
@@ -1041,13 +1053,13 @@ __device__ __forceinline__ void topofit_vblock(const TopoArgs& a, const int mpad
         pv[i] = make_float2(0.f, 0.f);
         bv[i] = 0.f;
         if (active && k0c + i < ncl && c < a.M) {
-          if (cpx) {
+          if (!LOOP) {
             pv[i] = cpx[s * M + c];
           } else {
             fv[i] = filt[cell * a.Mp + c];
             pv[i] = ph_nm[s * M + c];
           }
-          bv[i] = a.bp_row_inv ? a.bp[c] : a.bp[s * M + c];
+          bv[i] = ROWINV ? a.bp[c] : a.bp[s * M + c];
         }
       }
 #pragma unroll
@@ -1056,7 +1068,7 @@ __device__ __forceinline__ void topofit_vblock(const TopoArgs& a, const int mpad
         if (k0c + i >= ncl) break;
         float2 v = make_float2(0.f, 0.f);
         if (active && c < a.M) {
-          if (cpx) {
+          if (!LOOP) {
             v = pv[i];
           } else {
             // extract_patch_phase + normalize_complex_unit_magnitude (:1186-1205)
@@ -1216,6 +1228,19 @@ __device__ __forceinline__ void topofit_vblock(const TopoArgs& a, const int mpad
   }
   for (int i = tid; i < kCohBins; i += blockDim.x)
     if (sh_hist[i]) atomicAdd(&a.hist[i], sh_hist[i]);
+}
+
+// The input form (loop: ph_nm + filtered grid; standalone: psdph rows) and the
+// row invariance of bperp are compile-time in the body.
+template <int L>
+__device__ __forceinline__ void topofit_vblock(const TopoArgs& a, const int mpad, const int vb, const int nvb,
+                                               unsigned char* smem_raw, int* sh_hist, double* sh_rms, int* sh_inv) {
+  if (a.cpx)
+    a.bp_row_inv ? topofit_vblock_t<L, false, true>(a, mpad, vb, nvb, smem_raw, sh_hist, sh_rms, sh_inv)
+                 : topofit_vblock_t<L, false, false>(a, mpad, vb, nvb, smem_raw, sh_hist, sh_rms, sh_inv);
+  else
+    a.bp_row_inv ? topofit_vblock_t<L, true, true>(a, mpad, vb, nvb, smem_raw, sh_hist, sh_rms, sh_inv)
+                 : topofit_vblock_t<L, true, false>(a, mpad, vb, nvb, smem_raw, sh_hist, sh_rms, sh_inv);
 }
 
 template <int L>
