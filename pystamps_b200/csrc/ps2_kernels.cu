@@ -463,13 +463,16 @@ __device__ __forceinline__ void clap_window_warp(Tile& T, const int lane, const 
   // 0 <= ((k+16) mod 32) + d < 32.
   R t[32];
   const int sj = (lane + 16) & 31;
+  // this lane's taps: zero where the neighbour lies across the seam (adding
+  // x * 0 leaves the sum unchanged, so this equals skipping the tap)
+  R gl7[7];
+#pragma unroll
+  for (int d = -3; d <= 3; ++d) gl7[d + 3] = (sj + d >= 0 && sj + d < 32) ? g7[d + 3] : R(0);
 #pragma unroll
   for (int k = 0; k < 32; ++k) {
     R acc = R(0);
 #pragma unroll
-    for (int d = -3; d <= 3; ++d) {
-      if (sj + d >= 0 && sj + d < 32) acc += T.hs[k][(lane + d) & 31] * g7[d + 3];
-    }
+    for (int d = -3; d <= 3; ++d) acc += T.hs[k][(lane + d) & 31] * gl7[d + 3];
     t[k] = acc;
   }
   R o[32];
