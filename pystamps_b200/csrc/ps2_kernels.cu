@@ -1247,7 +1247,7 @@ __device__ __forceinline__ void topofit_vblock(const TopoArgs& a, const int mpad
 }
 
 template <int L>
-__global__ void __launch_bounds__(128) k_topofit_f32(TopoArgs a, int mpad) {
+__global__ void __launch_bounds__(128, 4) k_topofit_f32(TopoArgs a, int mpad) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int sh_hist[kCohBins];
   __shared__ double sh_rms[4];
@@ -2215,7 +2215,11 @@ __global__ void __launch_bounds__(128, 4) k_batch_topofit(BatchArgs b, const int
     const int p = units[2 * u], vb = units[2 * u + 1];
     if (!b.active[p]) continue;
     const PatchDev& d = b.patch[p];
-    topofit_vblock<L>(d.topo, d.mpad, vb, d.nvb, smem_raw, sh_hist, sh_rms, sh_inv);
+    // batches hold loaded contexts: always the loop form
+    if (d.topo.bp_row_inv)
+      topofit_vblock_t<L, true, true>(d.topo, d.mpad, vb, d.nvb, smem_raw, sh_hist, sh_rms, sh_inv);
+    else
+      topofit_vblock_t<L, true, false>(d.topo, d.mpad, vb, d.nvb, smem_raw, sh_hist, sh_rms, sh_inv);
   }
 }
 
