@@ -387,12 +387,15 @@ __device__ __forceinline__ R warp_median1024_pair(const R (&o)[32], R* scratch, 
 // window code calls it four times and two copies keep the kernel inside the
 // instruction cache.
 // tw holds e^{-2 pi i k/32} (forward) or its conjugate (inverse), k < 16.
-template <typename R, bool rows>
+template <typename R, bool rows, int NZ = 32>
 __device__ __noinline__ void fft_pass_t(R (*re)[33], R (*im)[33], const typename CT<R>::C* tw, const int lane) {
   using C = typename CT<R>::C;
   C x[32];
+  // entries NZ..31 of the row / column are zero (the window's padding) and are
+  // not read
 #pragma unroll
-  for (int k = 0; k < 32; ++k) x[k] = rows ? mk(re[lane][k], im[lane][k]) : mk(re[k][lane], im[k][lane]);
+  for (int k = 0; k < 32; ++k)
+    x[k] = k >= NZ ? mk(R(0), R(0)) : (rows ? mk(re[lane][k], im[lane][k]) : mk(re[k][lane], im[k][lane]));
 #pragma unroll
   for (int i = 0; i < 32; ++i) {
     const int r = ((i & 1) << 4) | ((i & 2) << 2) | (i & 4) | ((i & 8) >> 2) | ((i & 16) >> 4);
@@ -442,15 +445,22 @@ __device__ __forceinline__ void fft_pass(R (*re)[33], R (*im)[33], const typenam
 // One window of one interferogram, computed by one warp in its tile.
 // On entry the tile holds the 24x24 window zero-padded to 32x32; on exit rows
 // and columns < n_win hold the filtered values times the pyramid weight / 1024.
-template <typename R, typename Tile>
+template <typename R, int NWIN, typename Tile>
 __device__ __forceinline__ void clap_window_warp(Tile& T, const int lane, const ClapArgs& a,
                                                  const typename CT<R>::C* twf, const typename CT<R>::C* twi,
                                                  const R* lp, const R* wt, const R (&g7)[7], const int rs,
                                                  const int cs) {
   // forward FFT along rows (rows >= n_win are zero and stay zero), then columns
-  if (lane < a.n_win) fft_pass<R>(T.re, T.im, twf, lane, true);
-  __syncwarp();
-  fft_pass<R>(T.re, T.im, twf, lane, false);
+  if constexpr (NWIN > 0) {
+    // a compile-time window: the padding is zero by construction, never stored
+    if (lane < NWIN) fft_pass_t<R, true, NWIN>(T.re, T.im, twf, lane);
+    __syncwarp();
+    fft_pass_t<R, false, NWIN>(T.re, T.im, twf, lane);
+  } else {
+    if (lane < a.n_win) fft_pass<R>(T.re, T.im, twf, lane, true);
+    __syncwarp();
+    fft_pass<R>(T.re, T.im, twf, lane, false);
+  }
 #pragma unroll
   for (int k = 0; k < 32; ++k) {
     const R xr = T.re[k][lane], xi = T.im[k][lane];
@@ -503,10 +513,11 @@ __device__ __forceinline__ void clap_window_warp(Tile& T, const int lane, const 
   // inverse FFT along columns, then rows; keep the n_win x n_win corner, weighted
   fft_pass<R>(T.re, T.im, twi, lane, false);
   __syncwarp();
-  if (lane < a.n_win) {
+  const int nwv = NWIN > 0 ? NWIN : a.n_win;
+  if (lane < nwv) {
     fft_pass<R>(T.re, T.im, twi, lane, true);
     const bool row_zero = lane < rs;
-    for (int l = 0; l < a.n_win; ++l) {
+    for (int l = 0; l < nwv; ++l) {
       const R wv = (row_zero || l < cs) ? R(0) : wt[(lane - rs) * kWtStride + (l - cs)];
       T.re[lane][l] *= wv;
       T.im[lane][l] *= wv;
@@ -633,14 +644,14 @@ __device__ __forceinline__ int clap_groups(const ClapArgs& a) {
   return (a.Mp + NW - 1) / NW;
 }
 
-template <typename R, int NW>
+template <typename R, int NW, int NWIN = 0>
 __device__ __forceinline__ void clap_task(const ClapArgs& a, const int64_t task,
                                           ClapTileT<R, ClapShape<NW>::kPad>* tiles, const typename CT<R>::C* twf,
                                           const typename CT<R>::C* twi, const R* lp, const R* wt, const R (&g7)[7]) {
   using C = typename CT<R>::C;
   constexpr int NT = 32 * NW;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int nw = a.n_win, nw2 = nw * nw;
+  const int nw = NWIN > 0 ? NWIN : a.n_win, nw2 = nw * nw;
   const int n_inc = nw / 4 > 1 ? nw / 4 : 1;
   const int ngroups = clap_groups<R, NW>(a);
   const C* __restrict__ grid = static_cast<const C*>(a.grid);
@@ -663,7 +674,7 @@ __device__ __forceinline__ void clap_task(const ClapArgs& a, const int64_t task,
     }
     __syncthreads();
     // zero the padding of the tiles (none for a 32-pixel window)
-    if (nw < 32) {
+    if (NWIN == 0 && nw < 32) {
       for (int idx = tid; idx < NW * 32 * 32; idx += NT) {
         const int q = idx >> 10, e = idx & 1023, r = e >> 5, cc = e & 31;
         if (r >= nw || cc >= nw) {
@@ -675,7 +686,7 @@ __device__ __forceinline__ void clap_task(const ClapArgs& a, const int64_t task,
     const uint32_t inv_nw = (65536u + static_cast<uint32_t>(nw) - 1u) / static_cast<uint32_t>(nw);
     clap_load_tiles<R, NW>(a, tiles, grid, i1, j1, g, nw, nw2, inv_nw, tid);
     __syncthreads();
-    if (NW * g + warp < a.M) clap_window_warp<R>(T, lane, a, twf, twi, lp, wt, g7, rs, cs);
+    if (NW * g + warp < a.M) clap_window_warp<R, NWIN>(T, lane, a, twf, twi, lp, wt, g7, rs, cs);
     __syncthreads();
     clap_store_tiles<R, NW>(a, tiles, out, wi, g, nw, nw2, inv_nw, tid);
   }
@@ -706,7 +717,7 @@ __device__ __forceinline__ ClapSmem<R, NW> clap_smem(unsigned char* raw, const t
   return m;
 }
 
-template <typename R, int NW>
+template <typename R, int NW, int NWIN>
 __global__ void __launch_bounds__(32 * NW) k_clap(ClapArgs a, typename CT<R>::Tw tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const ClapSmem<R, NW> m = clap_smem<R, NW>(smem_raw, tw);
@@ -717,7 +728,7 @@ __global__ void __launch_bounds__(32 * NW) k_clap(ClapArgs a, typename CT<R>::Tw
   const int64_t nwin = a.w_n > 0 ? a.w_n : static_cast<int64_t>(a.nwi) * a.nwj;
   const int64_t ntask = nwin * clap_groups<R, NW>(a);
   for (int64_t task = blockIdx.x; task < ntask; task += gridDim.x)
-    clap_task<R, NW>(a, task, m.tiles, m.twf, m.twi, m.lp, m.wt, g7);
+    clap_task<R, NW, NWIN>(a, task, m.tiles, m.twf, m.twi, m.lp, m.wt, g7);
 }
 
 template <typename R, int NW>
@@ -725,8 +736,8 @@ static size_t clap_smem_bytes() {
   return NW * sizeof(ClapTileT<R, ClapShape<NW>::kPad>) + (1024 + 32 * kWtStride) * sizeof(R) + 32 * 2 * sizeof(R);
 }
 
-template <typename R, int NW>
-static cudaError_t launch_clap_nw(const ClapArgs& a, const typename CT<R>::Tw& tw, int sm_count, cudaStream_t st) {
+template <typename R, int NW, int NWIN>
+static cudaError_t launch_clap_nwin(const ClapArgs& a, const typename CT<R>::Tw& tw, int sm_count, cudaStream_t st) {
   const int64_t nwin = a.w_n > 0 ? a.w_n : static_cast<int64_t>(a.nwi) * a.nwj;
   const int64_t ntask = nwin * ((a.Mp + NW - 1) / NW);
   if (ntask <= 0) return cudaSuccess;
@@ -734,11 +745,17 @@ static cudaError_t launch_clap_nw(const ClapArgs& a, const typename CT<R>::Tw& t
   cudaError_t e = kernel_attributes_once(sm);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clap<R, NW>, 32 * NW, sm);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clap<R, NW, NWIN>, 32 * NW, sm);
   if (e != cudaSuccess) return e;
   const int64_t blocks = std::min<int64_t>(ntask, static_cast<int64_t>(sm_count) * (per_sm > 0 ? per_sm : 1));
-  k_clap<R, NW><<<static_cast<unsigned>(blocks), 32 * NW, sm, st>>>(a, tw);
+  k_clap<R, NW, NWIN><<<static_cast<unsigned>(blocks), 32 * NW, sm, st>>>(a, tw);
   return cudaGetLastError();
+}
+
+// the 24-pixel window (clap_win 32 x 0.75) as a compile-time shape, others at run time
+template <typename R, int NW>
+static cudaError_t launch_clap_nw(const ClapArgs& a, const typename CT<R>::Tw& tw, int sm_count, cudaStream_t st) {
+  return a.n_win == 24 ? launch_clap_nwin<R, NW, 24>(a, tw, sm_count, st) : launch_clap_nwin<R, NW, 0>(a, tw, sm_count, st);
 }
 
 // FP32: 8 warps per block (16 resident warps per SM, shared memory bound);
@@ -2995,8 +3012,10 @@ cudaError_t kernel_attributes_once(size_t dynamic_smem) {
     const cudaError_t r = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const cudaError_t steps[] = {
         r,
-        r == cudaSuccess ? opt_in_smem(k_clap<float, 8>, optin) : r,
-        r == cudaSuccess ? opt_in_smem(k_clap<double, 4>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<float, 8, 0>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<double, 4, 0>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<float, 8, 24>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<double, 4, 24>, optin) : r,
         r == cudaSuccess ? opt_in_smem(k_topofit_f32<4>, optin) : r,
         r == cudaSuccess ? opt_in_smem(k_topofit_f32<8>, optin) : r,
         r == cudaSuccess ? opt_in_smem(k_topofit_f32<16>, optin) : r,
