@@ -1260,9 +1260,12 @@ int ps2_random_coherence_histogram(const double* bperp_nm, int64_t n_ifg, double
   CK(cudaMemsetAsync(dh.p, 0, sizeof(int32_t) * PS2_COH_BINS, sc.st));
   double cutoff0, dbin;
   coh_bin_rule(&cutoff0, &dbin);
+  const int n_half = static_cast<int>(std::ceil(8.0 * n_trial_wraps));
+  DevBuf dE;
+  CK(dE.alloc(sizeof(double2) * n_ifg * (2 * n_half + 1)));
   CK(launch_random_hist(dr.as<double>(), n_rand, db.as<double>(), static_cast<int>(n_ifg), dia.as<int64_t>(),
-                        dib.as<int64_t>(), small_baseline ? 1 : 0, static_cast<int>(std::ceil(8.0 * n_trial_wraps)),
-                        cutoff0, dbin, dh.as<int32_t>(), sc.sm, sc.st));
+                        dib.as<int64_t>(), small_baseline ? 1 : 0, n_half, cutoff0, dbin, dE.as<double2>(),
+                        dh.as<int32_t>(), sc.sm, sc.st));
   int32_t h[PS2_COH_BINS];
   CK(cudaMemcpyAsync(h, dh.p, sizeof(h), cudaMemcpyDeviceToHost, sc.st));
   CK(cudaStreamSynchronize(sc.st));

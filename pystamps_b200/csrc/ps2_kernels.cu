@@ -1688,11 +1688,35 @@ cudaError_t launch_snr_weight(const TopoArgs& t, const float* amp, void* w_out, 
 // one warp per random row, lanes over trials for the sweep (each lane sums its
 // trial over the columns in the reference's order), lanes over columns for the
 // refinement with the sums taken in column order by lane 0.
+// The trial phasors e^{-j theta_c m} of every (column, trial), theta_c =
+// (bp_c / range) * pi/4 (topofit_phase_row_coh, native_stage2.rs:1438-1470):
+// the same for every random row, so they are evaluated once, [m][T].
+__global__ void __launch_bounds__(256) k_trial_phasors(const double* __restrict__ bp, int m, int n_half,
+                                                       double2* __restrict__ E) {
+  const int T = 2 * n_half + 1;
+  double mn = INFINITY, mx = -INFINITY;
+  for (int c = 0; c < m; ++c) {
+    mn = fmin(mn, bp[c]);
+    mx = fmax(mx, bp[c]);
+  }
+  double range = mx - mn;
+  if (range == 0.0) range = 1.0;
+  const double qpi = 3.14159265358979323846 / 4.0;
+  const int64_t total = static_cast<int64_t>(m) * T;
+  for (int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int c = static_cast<int>(idx / T), t = static_cast<int>(idx - static_cast<int64_t>(c) * T);
+    double sn, cs;
+    sincos(__dmul_rn(__dmul_rn(bp[c] / range, qpi), static_cast<double>(t - n_half)), &sn, &cs);
+    E[idx] = make_double2(cs, sn);
+  }
+}
+
 __global__ void __launch_bounds__(256) k_random_hist(const double* __restrict__ rnd, int64_t n_rand,
                                                      const double* __restrict__ bp, int m,
                                                      const int64_t* __restrict__ ia, const int64_t* __restrict__ ib,
                                                      int small_baseline, int n_half, double cutoff0, double dbin,
-                                                     int32_t* hist) {
+                                                     const double2* __restrict__ E, int32_t* hist) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   double* ph = reinterpret_cast<double*>(smem_raw) + static_cast<int64_t>(wib) * 3 * m;
@@ -1716,18 +1740,26 @@ __global__ void __launch_bounds__(256) k_random_hist(const double* __restrict__ 
     __syncwarp();
     for (int c = lane; c < m; c += 32)
       ph[c] = small_baseline ? rnd[row + ib[c] * n_rand] - rnd[row + ia[c] * n_rand] : rnd[row + c * n_rand];
+    // e^{j ph_c} once per row; the trial sum of e^{j (ph_c - theta_c m)} is then
+    // e^{j ph_c} e^{-j theta_c m} from the phasor table: 4 FP64 operations per
+    // (trial, column) instead of a sincos (the terms differ from sincos of the
+    // rounded angle in the last bit; the sums keep the column order)
+    for (int c = lane; c < m; c += 32) {
+      double sn, cs;
+      sincos(ph[c], &sn, &cs);
+      t1[c] = cs;
+      t2[c] = sn;
+    }
     __syncwarp();
     double best = -1.0;
     int bt = 0;
     for (int t = lane; t < T; t += 32) {
-      const double trial = static_cast<double>(t - n_half);
       double sre = 0.0, sim = 0.0;
       for (int c = 0; c < m; ++c) {
-        const double p = __dsub_rn(ph[c], __dmul_rn(__dmul_rn(bp[c] / range, qpi), trial));
-        double sn, cs;
-        sincos(p, &sn, &cs);
-        sre = __dadd_rn(sre, cs);
-        sim = __dadd_rn(sim, sn);
+        const double2 e = E[static_cast<int64_t>(c) * T + t];
+        const double cp = t1[c], sp = t2[c];
+        sre = __dadd_rn(sre, __fma_rn(cp, e.x, __dmul_rn(sp, e.y)));
+        sim = __dadd_rn(sim, __fma_rn(sp, e.x, -__dmul_rn(cp, e.y)));
       }
       const double v = hypot(sre, sim) / static_cast<double>(m);
       if (v > best) {
@@ -1799,15 +1831,18 @@ __global__ void __launch_bounds__(256) k_random_hist(const double* __restrict__ 
 
 cudaError_t launch_random_hist(const double* rnd, int64_t n_rand, const double* bp, int m, const int64_t* ia,
                                const int64_t* ib, int small_baseline, int n_half, double cutoff0, double dbin,
-                               int32_t* hist, int sm_count, cudaStream_t st) {
+                               double2* phasors, int32_t* hist, int sm_count, cudaStream_t st) {
   const size_t sm = static_cast<size_t>(8) * 3 * m * sizeof(double);
   cudaError_t e = kernel_attributes_once(sm);
   if (e != cudaSuccess) return e;
+  const int64_t n_ph = static_cast<int64_t>(m) * (2 * n_half + 1);
+  k_trial_phasors<<<static_cast<unsigned>(std::min<int64_t>((n_ph + 255) / 256, static_cast<int64_t>(sm_count) * 8)),
+                    256, 0, st>>>(bp, m, n_half, phasors);
   int64_t blocks = (n_rand + 7) / 8;
   if (blocks > static_cast<int64_t>(sm_count) * 8) blocks = static_cast<int64_t>(sm_count) * 8;
   if (blocks < 1) blocks = 1;
   k_random_hist<<<static_cast<unsigned>(blocks), 256, sm, st>>>(rnd, n_rand, bp, m, ia, ib, small_baseline, n_half,
-                                                                cutoff0, dbin, hist);
+                                                                cutoff0, dbin, phasors, hist);
   return cudaGetLastError();
 }
 

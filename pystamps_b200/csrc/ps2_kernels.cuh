@@ -230,7 +230,7 @@ cudaError_t launch_snr_weight(const TopoArgs& t, const float* amp, void* w_out, 
                               cudaStream_t st);
 cudaError_t launch_random_hist(const double* rnd, int64_t n_rand, const double* bp, int m, const int64_t* ia,
                                const int64_t* ib, int small_baseline, int n_half, double cutoff0, double dbin,
-                               int32_t* hist, int sm_count, cudaStream_t st);
+                               double2* phasors, int32_t* hist, int sm_count, cudaStream_t st);  // phasors: [m * (2*n_half+1)]
 
 // layout helpers
 cudaError_t launch_gather_rows(const void* src, void* dst, const int32_t* perm, int64_t n, int64_t row_bytes,
