@@ -40,10 +40,10 @@ sys.path.insert(0, str(ROOT))
 METRIC = "Stage-2 PS×ifg/s per gamma iter, FP32 vs plain FP64 GPU at max|Δγ|≤1e-4"
 UNIT = "PS*ifg/s"
 FP32_LANES_PER_SM = 128
-# DRAM bytes (read + write) per PS x ifg of one k_topofit_f32 launch, from the ncu
-# capture of the full-scale shape at 250,000 PS x 150 ifg (256x256 grid) in
-# profiles/kernels_full_scale_shape_250k_ps_150_ifg.md (537.4 MB per launch); the
-# reported traffic scales it by N x M.
+# DRAM bytes (read + write) per PS x ifg of one k_topofit_f32 launch, from an ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum) of the full-scale shape
+# with 250,000 PS x 150 ifg (256x256 grid): 537.4 MB per launch; the reported
+# traffic scales it by N x M.
 TOPOFIT_TRAFFIC_BYTES_PER_PS_IFG = 537.4e6 / (250_000 * 150)
 
 
