@@ -151,6 +151,20 @@ int ps2_topofit(const float* cpxphase /* complex64 [n, m] */, const float* bperp
 int ps2_clap_filter_grid(const float* ph_grid /* complex64 [n_i, n_j, m] */, int64_t n_i, int64_t n_j, int64_t m,
                          int64_t clap_window, double alpha, double beta, const double* low_pass, int64_t n_win_ex,
                          float* out /* complex64 [n_i, n_j, m] */);
+/* ---- host-side preparation (prepare_stage2_inputs, native_stage2.rs:447-467,
+ * 563-612) ------------------------------------------------------------------
+ * Threaded host passes (threads 0 = all cores), no device work.
+ * ps2_prepare_phase: ph complex64 [n_ps, n_full] -> ph_nm complex64 [n_ps, m] and
+ *   amp f32 [n_ps, m] over the columns cols[m]: amp = |ph| (hypotf), 1 where it
+ *   is 0; ph_nm = ph / amp (so a zero stays 0).
+ * ps2_prepare_bperp: bperp_mat f64 [n_ps, width] -> f32 [n_ps, m] over cols[m]
+ *   (NULL: all width == m columns); *row_invariant = every row equals the
+ *   first. */
+int ps2_prepare_phase(const float* ph, int64_t n_ps, int64_t n_full, const int64_t* cols, int64_t m, float* ph_nm,
+                      float* amp, int threads);
+int ps2_prepare_bperp(const double* bperp_mat, int64_t n_ps, int64_t width, const int64_t* cols, int64_t m, float* out,
+                      int32_t* row_invariant, int threads);
+
 /* Setup histogram of the coherence of 300,000 (n_rand) random-phase rows, in
  * FP64 on the GPU; the MATLAB v5 uniform generator (seed 2005) runs on the
  * host. ifgday_ix ([n_ifg, 2], 1-based) and n_image are used only when

@@ -23,6 +23,7 @@
 #include <cstring>
 #include <cstdlib>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/ps2cuda.h"
@@ -2159,6 +2160,91 @@ int ps2_shard_finalize(ps2_ctx* c, const double* stats, int64_t n_total, ps2_ite
   fill_stats(c->h_stats, &c->last);
   c->iters_done += 1;
   if (out) *out = c->last;
+  return PS2_OK;
+}
+
+
+// ------------------------------------------------ host-side preparation ------
+// prepare_stage2_inputs (native_stage2.rs:447-467, 563-612) in one threaded pass
+// per array: the same float32 hypotf, zero guard and IEEE divisions as the
+// numpy statement of it, element for element.
+}  // extern "C"
+
+namespace {
+template <typename F>
+void for_rows(int64_t n, int threads, F&& body) {
+  int nt = threads > 0 ? threads : static_cast<int>(std::thread::hardware_concurrency());
+  if (nt < 1) nt = 1;
+  if (static_cast<int64_t>(nt) > n) nt = static_cast<int>(std::max<int64_t>(n, 1));
+  std::vector<std::thread> pool;
+  const int64_t per = (n + nt - 1) / nt;
+  for (int t = 0; t < nt; ++t) {
+    const int64_t a = t * per, b = std::min<int64_t>(n, a + per);
+    if (a >= b) break;
+    pool.emplace_back([&body, a, b] { body(a, b); });
+  }
+  for (auto& th : pool) th.join();
+}
+}  // namespace
+
+extern "C" {
+
+int ps2_prepare_phase(const float* ph, int64_t n_ps, int64_t n_full, const int64_t* cols, int64_t m, float* ph_nm,
+                      float* amp, int threads) {
+  if (!ph || !cols || !ph_nm || !amp || n_ps < 0 || n_full <= 0 || m <= 0 || m > n_full)
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_prepare_phase: invalid arguments");
+  for (int64_t k = 0; k < m; ++k)
+    if (cols[k] < 0 || cols[k] >= n_full)
+      return set_err(PS2_ERR_INVALID_ARG, "ps2_prepare_phase: cols[%lld] = %lld outside 0..%lld", (long long)k,
+                     (long long)cols[k], (long long)n_full - 1);
+  for_rows(n_ps, threads, [&](int64_t a, int64_t b) {
+    for (int64_t r = a; r < b; ++r) {
+      const float* src = ph + 2 * r * n_full;
+      float* dst = ph_nm + 2 * r * m;
+      float* am = amp + r * m;
+      for (int64_t k = 0; k < m; ++k) {
+        const float re = src[2 * cols[k]], im = src[2 * cols[k] + 1];
+        const float mag = std::hypot(re, im);
+        const float safe = mag == 0.0f ? 1.0f : mag;  // a zero magnitude keeps the zero (:452-467)
+        dst[2 * k] = re / safe;
+        dst[2 * k + 1] = im / safe;
+        am[k] = safe;
+      }
+    }
+  });
+  return PS2_OK;
+}
+
+int ps2_prepare_bperp(const double* bmat, int64_t n_ps, int64_t width, const int64_t* cols, int64_t m, float* out,
+                      int32_t* row_invariant, int threads) {
+  if (!bmat || !out || !row_invariant || n_ps <= 0 || width <= 0 || m <= 0 || (!cols && width != m))
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_prepare_bperp: invalid arguments");
+  if (cols)
+    for (int64_t k = 0; k < m; ++k)
+      if (cols[k] < 0 || cols[k] >= width)
+        return set_err(PS2_ERR_INVALID_ARG, "ps2_prepare_bperp: cols[%lld] = %lld outside 0..%lld", (long long)k,
+                       (long long)cols[k], (long long)width - 1);
+  std::vector<double> row0(static_cast<size_t>(m));
+  for (int64_t k = 0; k < m; ++k) row0[k] = bmat[cols ? cols[k] : k];
+  std::mutex mu;
+  bool same = true;
+  for_rows(n_ps, threads, [&](int64_t a, int64_t b) {
+    bool local = true;
+    for (int64_t r = a; r < b; ++r) {
+      const double* src = bmat + r * width;
+      float* dst = out + r * m;
+      for (int64_t k = 0; k < m; ++k) {
+        const double v = src[cols ? cols[k] : k];
+        local = local && (v == row0[k]);  // NaN makes the rows differ, as in numpy
+        dst[k] = static_cast<float>(v);
+      }
+    }
+    if (!local) {
+      std::lock_guard<std::mutex> g(mu);
+      same = false;
+    }
+  });
+  *row_invariant = same ? 1 : 0;
   return PS2_OK;
 }
 

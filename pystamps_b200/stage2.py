@@ -168,16 +168,18 @@ def prepare_patch(patch: dict, *, nr: np.ndarray | None = None, nr_max_nz_ix: fl
     if bperp_full.size != n_full:
         raise Stage2Error(f"ps1.bperp has length {bperp_full.size} but ph1.ph has {n_full} interferograms")
     small = str(_parm(parms, "small_baseline_flag")).strip().lower() == "y"
-    cols = np.arange(n_full) if small else np.array([k for k in range(n_full) if k != master_ix - 1], dtype=np.int64)
+    cols = np.arange(n_full, dtype=np.int64) if small else np.array([k for k in range(n_full) if k != master_ix - 1],
+                                                                     dtype=np.int64)
     m = cols.size
-    sub = ph_full[:, cols]
-    re = np.ascontiguousarray(sub.real, dtype=np.float32)
-    im = np.ascontiguousarray(sub.imag, dtype=np.float32)
-    mag = np.hypot(re, im).astype(np.float32)
-    safe = np.where(mag == 0.0, np.float32(1.0), mag).astype(np.float32)
+    # unit phases and magnitudes (|ph|, 1 where it is 0) in one threaded native
+    # pass: hypotf, the zero guard and the divisions of :452-467
+    ph_full = np.ascontiguousarray(ph_full)
     ph_nm = np.empty((n_ps, m), dtype=np.complex64)
-    ph_nm.real = re / safe
-    ph_nm.imag = im / safe
+    safe = np.empty((n_ps, m), dtype=np.float32)
+    check(lib().ps2_prepare_phase(ctypes.c_void_p(ph_full.ctypes.data), ctypes.c_int64(n_ps), ctypes.c_int64(n_full),
+                                  ctypes.c_void_p(cols.ctypes.data), ctypes.c_int64(m),
+                                  ctypes.c_void_p(ph_nm.ctypes.data), ctypes.c_void_p(safe.ctypes.data),
+                                  ctypes.c_int(0)))
     bperp_nm = bperp_full[cols]
     # bp1.bperp_mat (native_stage2.rs:563-612)
     bmat = patch.get("bperp_mat")
@@ -191,19 +193,25 @@ def prepare_patch(patch: dict, *, nr: np.ndarray | None = None, nr_max_nz_ix: fl
         if bmat.shape[1] == m:
             pass
         elif not small and bmat.shape[1] == n_full:
-            bmat = bmat[:, cols]
+            pass  # the master column is skipped by the native pass below
         else:
             raise Stage2Error(
                 f"bp1.bperp_mat has incompatible shape {bmat.shape[0]}x{bmat.shape[1]} for stage-2 ph shape {n_ps}x{m}")
-    elif small:
-        bmat = np.tile(bperp_nm, (n_ps, 1))
-    if bmat is None or bmat.shape[0] <= 1 or bool(np.all(bmat == bmat[0:1, :])):
+    if bmat is None:  # (small baselines: every row is bperp_nm, row-invariant)
         row_inv = True
-        row_bp = bperp_nm if bmat is None else bmat[0]
-        bperp = np.ascontiguousarray(row_bp.astype(np.float32))
+        bperp = np.ascontiguousarray(bperp_nm.astype(np.float32))
     else:
-        row_inv = False
-        bperp = np.ascontiguousarray(bmat.astype(np.float32))
+        # f32 rows and the row-invariance test (native_stage2.rs:2413-2428) in one pass
+        bmat = np.ascontiguousarray(bmat, dtype=np.float64)
+        sel = cols if bmat.shape[1] != m else None
+        bp32 = np.empty((n_ps, m), dtype=np.float32)
+        inv = ctypes.c_int32(0)
+        check(lib().ps2_prepare_bperp(ctypes.c_void_p(bmat.ctypes.data), ctypes.c_int64(n_ps),
+                                      ctypes.c_int64(bmat.shape[1]),
+                                      ctypes.c_void_p(sel.ctypes.data if sel is not None else 0), ctypes.c_int64(m),
+                                      ctypes.c_void_p(bp32.ctypes.data), ctypes.byref(inv), ctypes.c_int(0)))
+        row_inv = n_ps <= 1 or inv.value == 1
+        bperp = np.ascontiguousarray(bp32[0]) if row_inv else bp32
     d_a = patch.get("D_A")
     if d_a is None or np.asarray(d_a).size != n_ps:
         d_a = np.ones(n_ps)

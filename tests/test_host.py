@@ -7,6 +7,12 @@ import pytest
 from pystamps_b200 import stage2, synth
 
 
+@pytest.fixture(scope="module", autouse=True)
+def _host_library(cuda_lib):
+    """prepare_patch runs its row passes in the library's host code (no device)."""
+    return cuda_lib
+
+
 @pytest.fixture(scope="module")
 def small_patch():
     return synth.make_patch(3000, 10, 31, 21, seed=11, n_rand=2000)
