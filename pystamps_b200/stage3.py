@@ -154,10 +154,13 @@ def max_percent_rand(select_method: str, percent_rand: float, density_rand: floa
 
 # ----------------------------------------------------------- re-estimate ----
 def reestimate(ph_grid, grid_ij, sel, ph_work, bperp_mat, fit_ifg, *, clap_alpha: float, clap_beta: float,
-               low_pass, n_trial_wraps: float, slc_osf: int = 1, clap_win: int = 32, device: int = 0) -> dict:
+               low_pass, n_trial_wraps: float, slc_osf: int = 1, clap_win: int = 32, device: int = 0,
+               ph_cols=None) -> dict:
     """The stage-3 re-estimate (ported.py:4489-4550) of rows `sel` (0-based)
     on the GPU. grid_ij: pm1.grid_ij of all PS (1-based); ph_work: the
-    interferograms without the master column; fit_ifg: 0-based columns."""
+    interferograms without the master column (or, with ph_cols, ph1.ph whole
+    and ph_cols its interferogram columns: only the selected rows are then
+    gathered); fit_ifg: 0-based columns."""
     sel = np.asarray(sel, dtype=np.int64).reshape(-1)
     gij_all = np.asarray(grid_ij).reshape(-1, 2)
     g = np.ascontiguousarray(ph_grid, dtype=np.complex64)
@@ -165,13 +168,15 @@ def reestimate(ph_grid, grid_ij, sel, ph_work, bperp_mat, fit_ifg, *, clap_alpha
         raise Stage3Error(f"ph_grid must be [n_i, n_j, n_ifg], got shape {g.shape}")
     m = g.shape[2]
     ph_w = np.asarray(ph_work)
-    if ph_w.shape[1] != m:
-        raise Stage3Error(f"ph has {ph_w.shape[1]} interferograms but ph_grid has {m}")
+    n_work = ph_w.shape[1] if ph_cols is None else len(ph_cols)
+    if n_work != m:
+        raise Stage3Error(f"ph has {n_work} interferograms but ph_grid has {m}")
     n = sel.size
     lp = np.ascontiguousarray(low_pass, dtype=np.float64)
     if lp.shape != (clap_win, clap_win):
         raise Stage3Error(f"low_pass must be {clap_win}x{clap_win}, got {lp.shape}")
-    ph_s = np.ascontiguousarray(ph_w[sel], dtype=np.complex64)
+    rows = ph_w[sel] if ph_cols is None else ph_w[np.ix_(sel, np.asarray(ph_cols, dtype=np.int64))]
+    ph_s = np.ascontiguousarray(rows, dtype=np.complex64)
     bp_s = np.ascontiguousarray(np.asarray(bperp_mat)[sel], dtype=np.float32)
     gij = np.ascontiguousarray(np.rint(gij_all[sel]), dtype=np.int64)
     fit = np.ascontiguousarray(fit_ifg, dtype=np.int64)
@@ -277,18 +282,22 @@ def select_ps(pm: dict, *, ph, bperp_mat, bperp, D_A, xy, master_ix: int, ifg_in
     if rej > 0 and ix0.size and fit.size:
         ix0 = ix0[bootstrap_coh_std(pm["ph_res"], ix0, fit) < rej]
     ph = np.asarray(ph)
-    ph_work = ph if sb else np.delete(ph, int(master_ix) - 1, axis=1)
+    # the interferograms without the master column, gathered with the selected rows
+    # only (no copy of the whole stack)
+    ph_cols = None if sb else np.delete(np.arange(ph.shape[1]), int(master_ix) - 1)
+    n_work = ph.shape[1] if sb else ph.shape[1] - 1
     bperp = np.asarray(bperp, dtype=np.float64).reshape(-1)
     bperp_work = bperp if sb else np.delete(bperp, int(master_ix) - 1)
-    fit = fit[(fit >= 0) & (fit < ph_work.shape[1])]
+    fit = fit[(fit >= 0) & (fit < n_work)]
     lp = np.asarray(pm["low_pass"], dtype=np.float64)
     clap_win = int(round(float(parms.get("clap_win", 32.0)))) or 32
     if lp.shape != (clap_win, clap_win):
         raise Stage3Error(f"pm1.low_pass is {lp.shape}, not {clap_win}x{clap_win}")
-    r = reestimate(pm["ph_grid"], pm["grid_ij"], ix0, ph_work, bperp_mat, fit,
+    r = reestimate(pm["ph_grid"], pm["grid_ij"], ix0, ph, bperp_mat, fit,
                    clap_alpha=float(parms.get("clap_alpha", 1.0)), clap_beta=float(parms.get("clap_beta", 0.3)),
                    low_pass=lp, n_trial_wraps=float(np.asarray(pm["n_trial_wraps"]).reshape(-1)[0]),
-                   slc_osf=max(1, int(round(float(parms.get("slc_osf", 1.0))))), clap_win=clap_win, device=device)
+                   slc_osf=max(1, int(round(float(parms.get("slc_osf", 1.0))))), clap_win=clap_win, device=device,
+                   ph_cols=ph_cols)
     coh_t = coh_ps.copy()
     coh_t[ix0] = r["coh_ps2"]
     thresh_re, coeffs = coh_threshold_from_dist(coh_t, da, da_max, coh_bins, Nr_dist, low, mpr, method)
