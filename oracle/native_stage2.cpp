@@ -696,7 +696,16 @@ void random_hist(const double* bperp_nm, int64_t m, const double* trials, int64_
 }
 
 // ----------------------------------------------------------- grid index ---
-// stage2_grid_indices, native_stage2.rs:1971-2011
+// Rust's `f32 as i32`: truncation, saturating at the i32 range, NaN -> 0.
+int32_t sat_i32(float v) {
+  if (std::isnan(v)) return 0;
+  if (v >= 2147483647.0f) return INT32_MAX;
+  if (v <= -2147483648.0f) return INT32_MIN;
+  return static_cast<int32_t>(v);
+}
+
+// stage2_grid_indices, native_stage2.rs:1971-2011 (f32::min / f32::max ignore
+// NaN, as std::fmin / std::fmax do)
 void grid_indices(const float* xy, int64_t n, double grid_size, float* gij) {
   float min_x = INFINITY, min_y = INFINITY;
   for (int64_t r = 0; r < n; ++r) {
@@ -708,7 +717,7 @@ void grid_indices(const float* xy, int64_t n, double grid_size, float* gij) {
   for (int64_t r = 0; r < n; ++r) {
     float fi = std::fmax(std::ceil((xy[r * 3 + 2] - min_y + eps) / scale), 1.0f);
     float fj = std::fmax(std::ceil((xy[r * 3 + 1] - min_x + eps) / scale), 1.0f);
-    int32_t i = static_cast<int32_t>(fi), j = static_cast<int32_t>(fj);
+    int32_t i = sat_i32(fi), j = sat_i32(fj);
     gij[r * 2] = static_cast<float>(i);
     gij[r * 2 + 1] = static_cast<float>(j);
     max_i = std::max(max_i, i);
@@ -716,8 +725,8 @@ void grid_indices(const float* xy, int64_t n, double grid_size, float* gij) {
   }
   if (max_i > 1 || max_j > 1)
     for (int64_t r = 0; r < n; ++r) {
-      if (max_i > 1 && static_cast<int32_t>(gij[r * 2]) == max_i) gij[r * 2] = static_cast<float>(max_i - 1);
-      if (max_j > 1 && static_cast<int32_t>(gij[r * 2 + 1]) == max_j) gij[r * 2 + 1] = static_cast<float>(max_j - 1);
+      if (max_i > 1 && sat_i32(gij[r * 2]) == max_i) gij[r * 2] = static_cast<float>(max_i - 1);
+      if (max_j > 1 && sat_i32(gij[r * 2 + 1]) == max_j) gij[r * 2 + 1] = static_cast<float>(max_j - 1);
     }
 }
 

@@ -53,28 +53,38 @@ class Stage2Error(ValueError):
 
 
 # ------------------------------------------------------------ preparation --
+def _saturate_i32(v: np.ndarray) -> np.ndarray:
+    """Rust's float-to-i32 `as` cast: truncation toward zero, saturating at
+    the i32 range (NaN never reaches it here)."""
+    return np.clip(np.trunc(v.astype(np.float64)), -2.0 ** 31, 2.0 ** 31 - 1).astype(np.int64)
+
+
 def grid_indices(xy: np.ndarray, grid_size: float) -> np.ndarray:
-    """stage2_grid_indices (native_stage2.rs:1971-2011), f32 arithmetic."""
+    """stage2_grid_indices (native_stage2.rs:1971-2011), f32 arithmetic.
+
+    The reference's f32 min and max ignore NaN (`f32::min`, `f32::max`): a NaN
+    coordinate takes no part in the minimum and its bin becomes 1
+    (`NaN.ceil().max(1.0)`); a bin beyond the i32 range saturates like `as i32`.
+    """
     xy = np.asarray(xy, dtype=np.float32)
     n = xy.shape[0]
     out = np.zeros((n, 2), dtype=np.float32)
     if n == 0:
         return out
-    x = xy[:, 1]
-    y = xy[:, 2]
     eps = np.float32(1.0e-6)
     scale = np.float32(grid_size)
-    with np.errstate(invalid="ignore"):
-        gi = np.maximum(np.ceil(((y - np.float32(np.min(y))) + eps) / scale), np.float32(1.0)).astype(np.int32)
-        gj = np.maximum(np.ceil(((x - np.float32(np.min(x))) + eps) / scale), np.float32(1.0)).astype(np.int32)
-    mi = max(1, int(gi.max()))
-    mj = max(1, int(gj.max()))
-    if mi > 1:
-        gi[gi == mi] = mi - 1
-    if mj > 1:
-        gj[gj == mj] = mj - 1
-    out[:, 0] = gi.astype(np.float32)
-    out[:, 1] = gj.astype(np.float32)
+    bins = []
+    for col in (2, 1):  # i from y, j from x
+        v = xy[:, col]
+        with np.errstate(invalid="ignore", over="ignore"):
+            lo = np.fmin(np.float32(np.inf), np.fmin.reduce(v))
+            f = np.fmax(np.ceil(((v - lo) + eps) / scale), np.float32(1.0))
+        bins.append(_saturate_i32(f).astype(np.float32))
+    for k, b in enumerate(bins):
+        top = int(max(1, _saturate_i32(b).max()))
+        if top > 1:
+            b[_saturate_i32(b) == top] = np.float32(top - 1)
+        out[:, k] = b
     return out
 
 

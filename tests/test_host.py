@@ -27,6 +27,43 @@ def test_grid_indices_bit_exact_with_oracle(oracle, small_patch):
         np.testing.assert_array_equal(stage2.grid_indices(xy2, g), oracle.grid_indices(xy2, g))
 
 
+def test_grid_indices_nan_and_infinite_coordinates(oracle):
+    """Rust's f32::min/max skip NaN (native_stage2.rs:1973-1989): a NaN
+    coordinate is left out of the minimum and gets bin 1; an infinite one
+    saturates the i32 bin like `as i32`."""
+    rng = np.random.default_rng(5)
+    xy = np.column_stack([np.arange(400), rng.uniform(0, 3000, 400), rng.uniform(0, 2000, 400)]).astype(np.float32)
+    xy[3, 1] = np.nan
+    xy[7, 2] = np.nan
+    xy[9, 1:] = np.nan
+    g = stage2.grid_indices(xy, 50.0)
+    np.testing.assert_array_equal(g, oracle.grid_indices(xy, 50.0))
+    assert g[3, 1] == 1 and g[7, 0] == 1 and g[9, 0] == 1 and g[9, 1] == 1
+    ok = np.isfinite(xy[:, 1]) & np.isfinite(xy[:, 2])
+    np.testing.assert_array_equal(g[ok], stage2.grid_indices(xy[ok], 50.0))
+    # every coordinate NaN: min stays +inf, every bin 1
+    allnan = xy.copy()
+    allnan[:, 1:] = np.nan
+    np.testing.assert_array_equal(stage2.grid_indices(allnan, 50.0), np.ones((400, 2), np.float32))
+    np.testing.assert_array_equal(oracle.grid_indices(allnan, 50.0), np.ones((400, 2), np.float32))
+    inf = xy[:20].copy()
+    inf[4, 2] = np.inf
+    gi = stage2.grid_indices(inf, 50.0)
+    np.testing.assert_array_equal(gi, oracle.grid_indices(inf, 50.0))
+    assert gi[4, 0] == np.float32(2 ** 31 - 2)
+
+
+def test_prepare_patch_with_nan_coordinates_matches_oracle_cells(oracle):
+    patch = synth.make_patch(2000, 8, 24, 21, seed=12, n_rand=1000)
+    xy = np.array(patch["xy"], dtype=np.float32)
+    xy[[5, 50, 500], 1] = np.nan
+    patch = dict(patch, xy=xy)
+    prep = stage2.prepare_patch(patch, nr=np.ones(100), nr_max_nz_ix=100.0)
+    g = oracle.grid_indices(xy, 50.0)
+    assert np.all(prep.grid_ij[[5, 50, 500], 1] == 1)
+    np.testing.assert_array_equal(prep.grid_ij, g)
+
+
 def test_grid_boundary_bin_single_precision():
     xy = np.array([[1.0, -23497.43359375, 0.0], [2.0, -21497.43359375, 0.0], [3.0, -20497.43359375, 0.0]],
                   dtype=np.float32)
