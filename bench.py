@@ -16,8 +16,10 @@ value  : device-resident inputs, K iterations timed with CUDA events on the
 e2e    : one public-API stage-2 run per step from pinned host buffers (upload,
          layout, iterate to convergence, download of K/C/coh/N_opt), metric =
          N_ps * N_ifg * iterations / t.
---impl reference : the CPU restatement of the reference's native stage 2 on all
-         host cores, a bounded sample per step (see cpu_baseline.sample).
+--impl reference : the oracle (C++ restatement of the reference's native
+         stage 2) on all host cores: each step one whole gamma iteration on the
+         PS of the patch's 96 x 96-cell corner (see cpu_baseline.sample); the
+         product library is not loaded on this path.
 """
 from __future__ import annotations
 
@@ -136,38 +138,70 @@ def load_peaks() -> dict:
 
 
 # ------------------------------------------------------------ CPU leg -------
-def cpu_sample(w, patch, prep, rows: int = 20_000, ifgs_clap: int = 4, threads: int = 0) -> dict:
-    """Per-iteration time of the oracle (CPU restatement of the reference's
-    native stage 2) on the full workload, from a bounded sample: the row-wise
-    steps (fill, bin, extract, topofit) on `rows` PS x all ifgs, scaled by
-    N_ps / rows, plus CLAP on the full grid for `ifgs_clap` ifgs, scaled by
-    N_ifg / ifgs_clap."""
+# The CPU figures time the oracle (the C++ restatement of the reference's
+# native stage 2, crates/pystamps-core/src/native_stage2.rs) doing WHOLE gamma
+# iterations (fill + bin, CLAP of every interferogram, extract, topofit,
+# weighting update, convergence test: the loop body :261-406) on a spatial
+# sample of the workload: the PS of the workload's corner of
+# SAMPLE_CELLS x SAMPLE_CELLS grid cells (every interferogram, the same trial
+# count and PS density). Work per PS x ifg is then that of the whole patch
+# (CLAP cost follows the cell count, topofit the PS count); nothing is scaled.
+SAMPLE_CELLS = 96
+
+
+def workload_config(w, n_ps: int, n_ifg: int, n_i: int, n_j: int, trials: int) -> dict:
+    """The config dict both arms print (identical by construction)."""
+    return {"workload": w.name, "n_ps": int(n_ps), "n_ifg": int(n_ifg), "grid": [int(n_i), int(n_j)],
+            "trials": int(trials),
+            "l2": (f"inputs larger than L2 (ph_nm {n_ps * n_ifg * 8 / 1e9:.2f} GB per step)"
+                   if n_ps * n_ifg * 8 > 126e6 else "inputs smaller than L2 (no flush; small config)")}
+
+
+def corner_subpatch(patch: dict, cells: int) -> dict:
+    """The PS of the patch's first `cells` x `cells` grid cells (the
+    reference's grid rule, via the oracle) as a patch of their own, rows in
+    their original order."""
     from oracle import oracle as O
 
-    n, m = prep.n_ps, prep.n_ifg
-    rows = min(rows, n)
-    sub = slice(0, rows)
-    ph_nm = np.ascontiguousarray(prep.ph_nm[sub])
-    bp = prep.bperp.astype(np.float64) if prep.row_invariant else np.ascontiguousarray(prep.bperp[sub], dtype=np.float64)
-    k = np.zeros(rows)
-    wv = np.ascontiguousarray(prep.weight0[sub])
-    gl = prep.grid_lin[sub]
-    t0 = time.perf_counter()
-    pw = O.fill_phase_weight(ph_nm, bp, k, wv, threads=threads)
-    grid = O.accumulate_grid(pw, gl, prep.n_i, prep.n_j)
-    patch_ph = O.extract_patch_phase(grid, gl, threads=threads)  # stands in for the filtered grid (same access)
-    O.fit_rows(patch_ph, ph_nm, bp, prep.n_trial_wraps, threads=threads)
-    t_rows = time.perf_counter() - t0
-    rng = np.random.default_rng(0)
-    g = (rng.standard_normal((prep.n_i, prep.n_j, ifgs_clap)) +
-         1j * rng.standard_normal((prep.n_i, prep.n_j, ifgs_clap))).astype(np.complex64)
-    t0 = time.perf_counter()
-    O.clap_filter_grid_stack(g, prep.clap_alpha, prep.clap_beta, prep.low_pass, n_win=prep.clap_window,
-                             threads=threads)
-    t_clap = time.perf_counter() - t0
-    t_iter = t_rows * (n / rows) + t_clap * (m / ifgs_clap)
-    return {"t_iter_s": t_iter, "t_rows_s": t_rows, "t_clap_s": t_clap, "rows": rows, "ifgs_clap": ifgs_clap,
-            "value": n * m / t_iter}
+    gij = O.grid_indices(patch["xy"], float(patch["parms"].get("filter_grid_size", 50.0)))
+    keep = np.where((gij[:, 0] <= cells) & (gij[:, 1] <= cells))[0]
+    sub = dict(patch)
+    for k in ("ph", "bperp_mat", "D_A", "xy"):
+        sub[k] = np.ascontiguousarray(np.asarray(patch[k])[keep])
+    sub.pop("truth", None)
+    return sub
+
+
+def oracle_iterations(patch: dict, n_iter: int, threads: int, n_rand: int = 20_000) -> dict:
+    """n_iter whole iterations of the oracle's stage-2 loop on `patch` (the
+    stop rule disabled so exactly n_iter run), with the random-phase
+    histogram from n_rand rows (setup, outside the timed loop). Returns the
+    wall time of each iteration."""
+    from oracle import oracle as O
+
+    p = dict(patch, parms=dict(patch["parms"], gamma_change_convergence=0.0, gamma_max_iterations=int(n_iter)))
+    bp = np.asarray(patch["bperp"], dtype=np.float64).reshape(-1)
+    bp_nm = np.delete(bp, int(patch.get("master_ix", 1)) - 1)
+    lam = float(p["parms"].get("lambda", 0.0555))
+    max_k = float(p["parms"].get("max_topo_err", 15.0)) / (lam * 830_000.0 * math.sin(float(p["mean_incidence"])) /
+                                                          (4.0 * math.pi))
+    ntw = float((bp_nm.max() - bp_nm.min()) * max_k / (2.0 * math.pi))
+    nr, mx = O.random_hist(bp_nm, ntw, n_rand=n_rand, threads=threads)
+    p["nr_override"] = np.concatenate([nr, [mx]])
+    res = O.stage2_run(p, threads=threads)
+    return {"iter_seconds": [float(t) for t in res["iter_seconds"]], "n_ps": int(np.asarray(p["ph"]).shape[0]),
+            "n_ifg": int(res["n_ifg"]), "grid": [int(res["n_i"]), int(res["n_j"])], "trials": int(res["n_trials"])}
+
+
+def cpu_baseline_sample(sub: dict, n_iter: int, threads: int) -> dict:
+    """Whole oracle iterations on a corner sub-patch (corner_subpatch)."""
+    r = oracle_iterations(sub, n_iter, threads)
+    t = statistics.median(r["iter_seconds"])
+    return {"value": r["n_ps"] * r["n_ifg"] / t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"whole oracle gamma iterations (median of {n_iter}, {t:.2f} s each) on the PS of the "
+                       f"{SAMPLE_CELLS}x{SAMPLE_CELLS}-cell corner of the patch: {r['n_ps']} PS x {r['n_ifg']} ifg, "
+                       f"{r['grid'][0]}x{r['grid'][1]} grid, {r['trials']} trials, all {threads} host threads"),
+            "what": "C++ restatement of crates/pystamps-core/src/native_stage2.rs (Rust toolchain absent)"}
 
 
 def ncores() -> int:
@@ -178,31 +212,43 @@ def ncores() -> int:
 
 
 def run_reference(args, rank: int, world: int):
+    """The reference arm: the oracle (CPU restatement of the reference's
+    native stage 2) on all host threads, rank 0 only. Each step is one whole
+    oracle gamma iteration on the PS of the workload's corner of
+    SAMPLE_CELLS x SAMPLE_CELLS cells; the metric is PS x ifg of the sample
+    per second of iteration. No product library is loaded on this path."""
     if rank != 0:
         return
-    from pystamps_b200 import stage2 as S
+    from oracle import oracle as O
+    from pystamps_b200 import synth
 
-    w, patch = make_workload(args.workload, 0, args.n_ps)
-    prep = S.prepare_patch(patch, nr=np.ones(100), nr_max_nz_ix=100.0)
-    vals = []
-    for i in range(args.warmup + args.steps):
-        r = cpu_sample(w, patch, prep)
-        if i >= args.warmup:
-            vals.append(r)
-    v = statistics.median([r["value"] for r in vals])
-    t_iter = statistics.median([r["t_iter_s"] for r in vals])
-    sample = (f"per step: oracle fill+bin+extract+topofit on {vals[0]['rows']} of {prep.n_ps} PS x {prep.n_ifg} ifg "
-              f"(scaled x{prep.n_ps / vals[0]['rows']:.0f}) + CLAP on the full {prep.n_i}x{prep.n_j} grid for "
-              f"{vals[0]['ifgs_clap']} of {prep.n_ifg} ifg (scaled x{prep.n_ifg / vals[0]['ifgs_clap']:.1f})")
+    w = synth.ALIASES.get(args.workload) or synth.WORKLOADS[args.workload]
+    if args.n_ps:
+        import dataclasses
+
+        w = dataclasses.replace(w, name=f"{w.name}-at-{args.n_ps}-ps", n_ps=args.n_ps)
+    patch = synth.make_workload(w, patch_id=0)
+    gij = O.grid_indices(patch["xy"], 50.0)
+    n_i, n_j = int(gij[:, 0].max()), int(gij[:, 1].max())
+    config = workload_config(w, patch["ph"].shape[0], patch["ph"].shape[1] - 1, n_i, n_j, w.n_trials)
+    sub = corner_subpatch(patch, SAMPLE_CELLS)
+    del patch
+    threads = ncores()
+    r = oracle_iterations(sub, args.warmup + args.steps, threads)
+    ts = r["iter_seconds"][args.warmup:]
+    t_total = float(sum(ts))
+    v = r["n_ps"] * r["n_ifg"] * len(ts) / t_total
+    sample = (f"per step: one whole oracle gamma iteration on the PS of the {SAMPLE_CELLS}x{SAMPLE_CELLS}-cell "
+              f"corner of the patch ({r['n_ps']} PS x {r['n_ifg']} ifg, {r['grid'][0]}x{r['grid'][1]} grid, "
+              f"{r['trials']} trials), all {threads} host threads; {args.warmup} warm-up iterations untimed")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": t_iter * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, pystamps_b200.synth)",
-        "config": {"workload": w.name, "n_ps": prep.n_ps, "n_ifg": prep.n_ifg, "grid": [prep.n_i, prep.n_j],
-                   "trials": 2 * math.ceil(8 * prep.n_trial_wraps) + 1},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": ncores(), "kind": "port", "sample": sample,
+        "warmup": args.warmup, "ms_per_step": t_total / len(ts) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, pystamps_b200.synth)", "config": config,
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
                          "what": "C++ restatement of crates/pystamps-core/src/native_stage2.rs (Rust toolchain absent)"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "iter_seconds": ts,
     }
     print(json.dumps(line), flush=True)
 
@@ -313,6 +359,7 @@ def run_ours(args, rank: int, world: int, dist):
     t_prep = time.perf_counter() - t0
     inc = float(patch["mean_incidence"])
     lam = float(patch["parms"].get("lambda", 0.0555))
+    cpu_patch = corner_subpatch(patch, SAMPLE_CELLS) if rank == 0 and not args.no_cpu else None
     del patch
     n, m = prep.n_ps, prep.n_ifg
     T = 2 * math.ceil(8 * prep.n_trial_wraps) + 1
@@ -442,9 +489,18 @@ def run_ours(args, rank: int, world: int, dist):
             c32.iterate(1)
             c64.iterate(1)
             a1 = c32.download(["coh_ps", "K_ps"])
-            b1 = c64.download(["coh_ps", "K_ps"])
+            b1 = c64.download(["coh_ps", "K_ps", "ph_patch"])
         d1 = np.abs(a1["coh_ps"] - b1["coh_ps"])
         dk1 = np.abs(a1["K_ps"] - b1["K_ps"]) * kconv
+        # PS beyond the bounds, classified by the FP64 trial search of their rows
+        from pystamps_b200.precision import classify_ties
+
+        out_rows = np.flatnonzero((d1 > 1e-4) | (dk1 > 1e-3))
+        bp_rows = prep.bperp if prep.row_invariant else prep.bperp[out_rows]
+        cls = classify_ties(prep.ph_nm[out_rows], b1["ph_patch"][out_rows], bp_rows, prep.n_trial_wraps)
+        del b1
+        nontie = ~cls["tie"]
+        tie_rows = out_rows[cls["tie"]]
         # to convergence, each path on its own trajectory
         a = S.run_stage2(prep, precision="fp32", keys=["coh_ps", "K_ps"])
         b = S.run_stage2(prep, precision="fp64", keys=["coh_ps", "K_ps"])
@@ -454,31 +510,34 @@ def run_ours(args, rank: int, world: int, dist):
                     "dgamma_max": float(d1.max()), "dgamma_p9999": float(np.quantile(d1, 0.9999)),
                     "n_dgamma_above_1e-4": int((d1 > 1e-4).sum()), "dK_m_p9999": float(np.nanquantile(dk1, 0.9999)),
                     "n_dK_above_1e-3_m": int((dk1 > 1e-3).sum()),
-                    "note": "PS above the bounds are argmax / refinement-wrap ties (classified in "
-                            "tests/test_gpu_precision.py on the 250k-PS shape)"},
+                    "n_argmax_ties": int(cls["argmax_tie"].sum()), "n_wrap_ties": int(cls["wrap_tie"].sum()),
+                    "n_nontie_above_1e-4": int((d1[out_rows] > 1e-4)[nontie].sum()),
+                    "n_nontie_above_1e-3_m": int((dk1[out_rows] > 1e-3)[nontie].sum()),
+                    "nontie_dgamma_max": float(np.delete(d1, tie_rows).max()),
+                    "nontie_dK_m_max": float(np.nanmax(np.delete(dk1, tie_rows))),
+                    "note": "PS above the bounds classified by an FP64 trial search of their rows "
+                            "(pystamps_b200.precision.classify_ties): argmax ties (best and runner-up trial "
+                            "within 1e-6 relative) and refinement wrap ties (a residual angle within 1e-4 rad "
+                            "of +-pi)"},
                 "converged": {"iterations_fp32": a["i_loop"], "iterations_fp64": b["i_loop"],
                               "dgamma_median": float(np.median(d)), "dgamma_p99": float(np.quantile(d, 0.99)),
                               "dgamma_max": float(d.max()), "dK_m_median": float(np.nanmedian(dk)),
                               "dK_m_p99": float(np.nanquantile(dk, 0.99))}}
 
     cpu = None
-    if rank == 0 and not args.no_cpu:
-        r = cpu_sample(w, None, prep)
-        cpu = {"value": r["value"], "unit": UNIT, "cores": ncores(), "kind": "port",
-               "sample": f"oracle row steps on {r['rows']} PS x {m} ifg scaled x{n / r['rows']:.0f} + CLAP on the "
-                         f"full grid for {r['ifgs_clap']} ifg scaled x{m / r['ifgs_clap']:.1f}; "
-                         f"t_iter={r['t_iter_s']:.2f} s"}
+    if rank == 0 and not args.no_cpu and cpu_patch is not None:
+        cpu = cpu_baseline_sample(cpu_patch, 3, ncores())
+    del cpu_patch
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator pystamps_b200.synth)",
-            "config": {"workload": w.name, "n_ps": n, "n_ifg": m, "grid": [prep.n_i, prep.n_j], "trials": T,
-                       "l2": f"inputs larger than L2 (ph_nm {prep.ph_nm.nbytes / 1e9:.2f} GB per step)",
-                       "per_kernel_ms": {"bin": bin_ms, "clap": clap_ms, "topofit": topo_ms,
-                                         "finalize": per[3] / args.steps},
-                       "prepare_s": t_prep, "parallelism": f"replicas x{world}"},
+            "config": workload_config(w, n, m, prep.n_i, prep.n_j, T),
+            "parallelism": f"replicas x{world}",
+            "per_kernel_ms": {"bin": bin_ms, "clap": clap_ms, "topofit": topo_ms, "finalize": per[3] / args.steps},
+            "prepare_s": t_prep,
             "roofline": roofline, "roofline_bin": bin_roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clocks, "fp64_gpu": fp64,
             "fp32_over_fp64": (value / fp64["value"]) if fp64 else None, "precision_vs_fp64": prec,

@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -971,6 +972,7 @@ struct orc_stage2_out {
   double* gamma_change_hist;  // [gamma_max_iterations] gamma_change_rms per iteration
   double* coh_hist;           // NULL or [gamma_max_iterations, n] coh per iteration
   double* K_hist;             // NULL or [gamma_max_iterations, n] K per iteration
+  double* iter_seconds;       // NULL or [gamma_max_iterations] wall time of each loop iteration
   // scalars
   double Nr_max_nz_ix, gamma_change_save, n_trial_wraps;
   int64_t i_loop, n_i, n_j, n_ifg, n_trials;
@@ -1088,6 +1090,13 @@ static int run_stage2(const orc_stage2_in* in, orc_stage2_out* out, int threads)
   double gamma_change_save = 0.0;
   int64_t i_loop = 1;
   const int64_t max_iter = std::max<int64_t>(in->gamma_max_iterations, 1);
+  auto t_iter = std::chrono::steady_clock::now();
+  auto record_time = [&]() {
+    const auto t_now = std::chrono::steady_clock::now();
+    if (out->iter_seconds && i_loop <= in->gamma_max_iterations)
+      out->iter_seconds[i_loop - 1] = std::chrono::duration<double>(t_now - t_iter).count();
+    t_iter = t_now;
+  };
   for (;;) {
     // fill_phase_weight
     parallel_for(n, threads, [&](int64_t b, int64_t e) {
@@ -1143,7 +1152,10 @@ static int run_stage2(const orc_stage2_in* in, orc_stage2_out* out, int threads)
     coh_save = coh;
     if (out->gamma_change_hist && i_loop <= in->gamma_max_iterations) out->gamma_change_hist[i_loop - 1] = gamma_change_rms;
     bool stop = std::fabs(gamma_change_change) < in->gamma_change_convergence || i_loop >= max_iter;
-    if (stop) break;
+    if (stop) {
+      record_time();
+      break;
+    }
     if (in->psquare) {
       std::vector<double> na(kCohBins);
       hist_with_centers(coh.data(), n, coh_bins.data(), kCohBins, na.data());
@@ -1172,6 +1184,7 @@ static int run_stage2(const orc_stage2_in* in, orc_stage2_out* out, int threads)
         weighting[r] = sig != 0.0 ? gg / sig : 0.0;
       }
     }
+    record_time();
     ++i_loop;
   }
   // outputs

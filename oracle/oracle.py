@@ -240,7 +240,7 @@ class _Out(ctypes.Structure):
         ("ph_grid", ctypes.c_void_p), ("ph_weight", ctypes.c_void_p), ("grid_ij", ctypes.c_void_p),
         ("low_pass", ctypes.c_void_p), ("Nr", ctypes.c_void_p), ("coh_ps_save", ctypes.c_void_p),
         ("gamma_change_hist", ctypes.c_void_p), ("coh_hist", ctypes.c_void_p), ("K_hist", ctypes.c_void_p),
-        ("Nr_max_nz_ix", ctypes.c_double), ("gamma_change_save", ctypes.c_double),
+        ("iter_seconds", ctypes.c_void_p), ("Nr_max_nz_ix", ctypes.c_double), ("gamma_change_save", ctypes.c_double),
         ("n_trial_wraps", ctypes.c_double),
         ("i_loop", _c_i64), ("n_i", _c_i64), ("n_j", _c_i64), ("n_ifg", _c_i64), ("n_trials", _c_i64),
     ]
@@ -252,7 +252,8 @@ def stage2_run(patch, *, threads=None, fp64: bool = False, keep_history: bool = 
     ``patch`` is a mapping with the keys produced by
     ``pystamps_b200.synth.make_patch`` (ph, bperp, master_ix, bperp_mat, D_A, xy,
     mean_incidence, parms...). Returns the pm1.mat variables of
-    native_stage2.rs:1899-1965 plus per-iteration histories.
+    native_stage2.rs:1899-1965 plus per-iteration histories (gamma_change_hist,
+    iter_seconds: wall time of each loop iteration, native_stage2.rs:261-406).
     """
     ph = np.ascontiguousarray(patch["ph"], dtype=np.complex64)
     n, mf = ph.shape
@@ -304,6 +305,7 @@ def stage2_run(patch, *, threads=None, fp64: bool = False, keep_history: bool = 
         ph_res=np.empty((n, m), rdt), ph_patch=np.empty((n, m), cdt), ph_weight=np.empty((n, m), cdt),
         grid_ij=np.empty((n, 2), np.float32), low_pass=np.empty((int(round(inp.clap_win)),) * 2),
         Nr=np.empty(100), coh_ps_save=np.empty(n), gamma_change_hist=np.full(max_it, np.nan),
+        iter_seconds=np.full(max_it, np.nan),
     )
     if keep_history:
         bufs["coh_hist"] = np.full((max_it, n), np.nan)
@@ -330,6 +332,7 @@ def stage2_run(patch, *, threads=None, fp64: bool = False, keep_history: bool = 
         grid_size=inp.grid_size, coh_bins=COH_BINS.copy(), step_number=1.0,
     )
     res["gamma_change_hist"] = res["gamma_change_hist"][:it]
+    res["iter_seconds"] = res["iter_seconds"][:it]
     if keep_history:
         res["coh_hist"] = res["coh_hist"][:it]
         res["K_hist"] = res["K_hist"][:it]

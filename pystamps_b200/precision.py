@@ -20,6 +20,74 @@ import numpy as np
 from . import stage2 as S
 from . import synth
 
+ARGMAX_TIE_REL = 1e-6  # best and runner-up trial coherence this close (relative): an argmax tie
+WRAP_TIE_RAD = 1e-4    # a refinement residual angle this close to +-pi: a wrap tie
+
+
+def trial_values(n_trial_wraps: float) -> np.ndarray:
+    """The trial multipliers -ceil(8 n)..ceil(8 n) (native_stage2.rs:1305-1308)."""
+    n = math.ceil(8.0 * n_trial_wraps)
+    return np.arange(-n, n + 1, dtype=np.float64)
+
+
+def trial_coherences(ph_nm, ph_patch, bperp, n_trial_wraps: float) -> np.ndarray:
+    """FP64 statement of topofit's trial search (native_stage2.rs:1207-1257)
+    for a few rows: coherence of every trial, [rows, trials]. psdph =
+    conj(ph_patch) * ph_nm; a zero element takes no part (the reference's
+    valid columns)."""
+    z = np.conj(np.asarray(ph_patch, np.complex128)) * np.asarray(ph_nm, np.complex128)
+    bp = np.broadcast_to(np.asarray(bperp, np.float64), z.shape)
+    valid = z != 0
+    big = np.where(valid, bp, -np.inf).max(axis=1)
+    small = np.where(valid, bp, np.inf).min(axis=1)
+    rng = big - small
+    rng[~np.isfinite(rng) | (rng == 0)] = 1.0
+    trials = trial_values(n_trial_wraps)
+    denom = np.abs(z).sum(axis=1)
+    denom[denom == 0] = 1.0
+    theta = (bp / rng[:, None]) * (math.pi / 4)
+    s = np.einsum("rc,rct->rt", z, np.exp(-1j * theta[:, :, None] * trials[None, None, :]))
+    return np.abs(s) / denom[:, None]
+
+
+def wrap_distance(ph_nm, ph_patch, bperp, n_trial_wraps: float, best_ix=None) -> np.ndarray:
+    """Per row, min over interferograms of pi - |arg(res * conj(offset))| at
+    the winning trial (refine_candidate, native_stage2.rs:1259-1303), FP64.
+    best_ix: winning trial index per row (default: argmax of
+    trial_coherences)."""
+    z = np.asarray(ph_nm, np.complex128) * np.conj(np.asarray(ph_patch, np.complex128))
+    bp = np.broadcast_to(np.asarray(bperp, np.float64), z.shape)
+    rng = bp.max(axis=1) - bp.min(axis=1)
+    rng[rng == 0] = 1.0
+    if best_ix is None:
+        best_ix = np.argmax(trial_coherences(ph_nm, ph_patch, bperp, n_trial_wraps), axis=1)
+    k0 = (math.pi / 4) / rng * trial_values(n_trial_wraps)[best_ix]
+    res = z * np.exp(-1j * k0[:, None] * bp)
+    off = res.sum(axis=1)
+    ang = np.angle(res * np.conj(off)[:, None])
+    return (math.pi - np.abs(ang)).min(axis=1)
+
+
+def classify_ties(ph_nm, ph_patch, bperp, n_trial_wraps: float) -> dict:
+    """Tie classes of the given rows (few rows: every trial in FP64):
+    argmax ties (best and runner-up trial within ARGMAX_TIE_REL relative) and
+    wrap ties (a refinement residual angle within WRAP_TIE_RAD of +-pi). Rows
+    that are neither are genuine FP32/FP64 differences."""
+    ph_nm = np.atleast_2d(ph_nm)
+    ph_patch = np.atleast_2d(ph_patch)
+    bp = np.asarray(bperp, np.float64)
+    bp = bp[None, :] if bp.ndim == 1 else np.atleast_2d(bp)
+    if ph_nm.shape[0] == 0:
+        e = np.zeros(0, bool)
+        return {"argmax_tie": e, "wrap_tie": e, "tie": e}
+    coh = trial_coherences(ph_nm, ph_patch, bp, n_trial_wraps)
+    srt = np.sort(coh, axis=1)
+    best = srt[:, -1]
+    second = srt[:, -2] if coh.shape[1] > 1 else np.zeros(coh.shape[0])
+    argmax_tie = (best - second) <= ARGMAX_TIE_REL * np.maximum(best, 1e-30)
+    wrap_tie = wrap_distance(ph_nm, ph_patch, bp, n_trial_wraps, np.argmax(coh, axis=1)) < WRAP_TIE_RAD
+    return {"argmax_tie": argmax_tie, "wrap_tie": wrap_tie, "tie": argmax_tie | wrap_tie}
+
 
 def study(prep: S.PreparedPatch, k_to_m: float, iterations: int = 8, device: int = 0) -> list[dict]:
     out = []
