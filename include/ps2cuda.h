@@ -17,9 +17,17 @@
  *  - ps2_grid_accumulate replaces accumulate_weighted_grid (src/lib.rs:1013-1087)
  *    behind the Python registry kernel "stage2_grid_accumulate"
  *    (pystamps/kernels/accelerated.py:410, 429-443).
- *  - ps2_topofit replaces ps_topofit_batch_generic_f32 / _generic
- *    (src/lib.rs:1159-1247) behind "stage2_topofit" (accelerated.py:411, 446-460)
- *    with the native driver's first-argmax peak rule (native_stage2.rs:1207-1257).
+ *  - ps2_topofit is the native driver's topofit over rows (fit_stage2_rows /
+ *    topofit_row / refine_candidate, native_stage2.rs:659-720, 1207-1303):
+ *    first-argmax peak rule, the rule of the gamma loop itself.
+ *  - ps2_topofit_near_max replaces the registry kernels "stage2_topofit",
+ *    "stage2_topofit_row_invariant" and "stage2_topofit_coh_row_invariant"
+ *    (pystamps/kernels/accelerated.py:316-380, 411-427, 446-493), i.e.
+ *    ported._ps_topofit_single (pystamps/pipeline/ported.py:2355-2431, near-max
+ *    tolerance 2e-4) and the PyO3 ps_topofit_batch_* (src/lib.rs:525-586,
+ *    1159-1379, tolerance 5e-3): the tolerance is an argument.
+ *  - ps2_histogram_with_centers replaces histogram_with_centers
+ *    (src/lib.rs:2443-2455) behind "stage2_histogram" (accelerated.py:235-265, 496-509).
  *  - ps2_clap_filter_grid replaces clap_filter_grid_stack
  *    (native_stage2.rs:742-922) / ported._clap_filt_grid_stack_prepared
  *    (pystamps/pipeline/ported.py:1208-1298).
@@ -151,6 +159,23 @@ int ps2_topofit(const float* cpxphase /* complex64 [n, m] */, const float* bperp
 int ps2_clap_filter_grid(const float* ph_grid /* complex64 [n_i, n_j, m] */, int64_t n_i, int64_t n_j, int64_t m,
                          int64_t clap_window, double alpha, double beta, const double* low_pass, int64_t n_win_ex,
                          float* out /* complex64 [n_i, n_j, m] */);
+/* The registry's topofit rule over rows: per row only the non-zero columns
+ * take part (an all-zero row gives NaN K, C, coh and a zero residual); trial
+ * coherences; every local maximum within near_max_tol of the largest is
+ * refined and the reference's choice among them is kept
+ * (_ps_topofit_near_max_trial_indices / _select_candidate / _refine_candidate,
+ * pystamps/pipeline/ported.py:2433-2513). precision PS2_PRECISION_FP32: cpxphase
+ * complex64 and bperp f32 (the reference's single-precision path, taken when
+ * either input is single precision); PS2_PRECISION_FP64: complex128 and f64.
+ * residual: NULL or complex64 [n, m]. Synchronous; host pointers. */
+int ps2_topofit_near_max(const void* cpxphase, const void* bperp, int32_t bperp_row_invariant, int32_t precision,
+                         double n_trial_wraps, int64_t n, int64_t m, double near_max_tol, double* K, double* C,
+                         double* coh, float* residual);
+/* Counts of the finite values per centre (f64 [n_centers]): equally spaced
+ * centres use the ceil rule, others the nearest-midpoint rule
+ * (pystamps/kernels/accelerated.py:235-265). Host pointers. */
+int ps2_histogram_with_centers(const double* values, int64_t n, const double* centers, int64_t n_centers,
+                               double* out);
 /* ---- host-side preparation (prepare_stage2_inputs, native_stage2.rs:447-467,
  * 563-612) ------------------------------------------------------------------
  * Threaded host passes (threads 0 = all cores), no device work.

@@ -1150,6 +1150,108 @@ int ps2_topofit(const float* cpxphase, const float* bperp, int32_t row_inv, doub
   return PS2_OK;
 }
 
+int ps2_topofit_near_max(const void* cpxphase, const void* bperp, int32_t row_inv, int32_t precision,
+                         double n_trial_wraps, int64_t n, int64_t m, double near_max_tol, double* K, double* C,
+                         double* coh, float* residual) {
+  if (!cpxphase || !bperp || !K || !C || !coh || n < 0 || m <= 0 || !(near_max_tol >= 0.0))
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_topofit_near_max: invalid arguments");
+  if (precision != PS2_PRECISION_FP32 && precision != PS2_PRECISION_FP64)
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_topofit_near_max: precision %d", precision);
+  if (m > 4096) return set_err(PS2_ERR_UNSUPPORTED, "m %lld > 4096 is not supported", (long long)m);
+  if (!(n_trial_wraps >= 0.0) || n_trial_wraps > 512.0)
+    return set_err(PS2_ERR_INVALID_ARG, "n_trial_wraps %g out of range [0, 512]", n_trial_wraps);
+  if (n == 0) return PS2_OK;
+  const bool fp64 = precision == PS2_PRECISION_FP64;
+  const int n_half = static_cast<int>(std::ceil(8.0 * n_trial_wraps));
+  const size_t smem = topofit_near_max_smem(fp64, static_cast<int>(m), n_half);
+  int dev = 0, smem_max = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (smem > static_cast<size_t>(smem_max))
+    return set_err(PS2_ERR_UNSUPPORTED, "ps2_topofit_near_max: %lld columns x %d trials need %zu bytes of shared "
+                   "memory per row (device limit %d)", (long long)m, 2 * n_half + 1, smem, smem_max);
+  Scoped sc;
+  int rc = scoped_init(sc);
+  if (rc) return rc;
+  const size_t rs = fp64 ? sizeof(double) : sizeof(float);
+  DevBuf dc, db, dk, dcc, dh, dr;
+  CK(dc.alloc(2 * rs * n * m));
+  CK(cudaMemcpyAsync(dc.p, cpxphase, 2 * rs * n * m, cudaMemcpyHostToDevice, sc.st));
+  const int64_t nb = row_inv ? m : n * m;
+  CK(db.alloc(rs * nb));
+  CK(cudaMemcpyAsync(db.p, bperp, rs * nb, cudaMemcpyHostToDevice, sc.st));
+  CK(dk.alloc(sizeof(double) * n));
+  CK(dcc.alloc(sizeof(double) * n));
+  CK(dh.alloc(sizeof(double) * n));
+  if (residual) CK(dr.alloc(sizeof(float) * 2 * n * m));
+  NearMaxArgs a{};
+  a.cpx = dc.p;
+  a.bp = db.p;
+  a.bp_row_inv = row_inv ? 1 : 0;
+  a.n = n;
+  a.M = static_cast<int>(m);
+  a.n_half = n_half;
+  a.tol = near_max_tol;
+  a.K = dk.as<double>();
+  a.C = dcc.as<double>();
+  a.coh = dh.as<double>();
+  a.residual = residual ? dr.as<float2>() : nullptr;
+  CK(launch_topofit_near_max(a, fp64, sc.sm, sc.st));
+  CK(cudaMemcpyAsync(K, dk.p, sizeof(double) * n, cudaMemcpyDeviceToHost, sc.st));
+  CK(cudaMemcpyAsync(C, dcc.p, sizeof(double) * n, cudaMemcpyDeviceToHost, sc.st));
+  CK(cudaMemcpyAsync(coh, dh.p, sizeof(double) * n, cudaMemcpyDeviceToHost, sc.st));
+  if (residual) CK(cudaMemcpyAsync(residual, dr.p, sizeof(float) * 2 * n * m, cudaMemcpyDeviceToHost, sc.st));
+  CK(cudaStreamSynchronize(sc.st));
+  return PS2_OK;
+}
+
+int ps2_histogram_with_centers(const double* values, int64_t n, const double* centers, int64_t n_centers,
+                               double* out) {
+  if ((!values && n > 0) || n < 0 || n_centers < 0 || (!centers && n_centers > 0) || (!out && n_centers > 0))
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_histogram_with_centers: invalid arguments");
+  if (n_centers == 0) return PS2_OK;
+  if (n_centers > (1 << 24)) return set_err(PS2_ERR_UNSUPPORTED, "ps2_histogram_with_centers: too many centres");
+  const int nc = static_cast<int>(n_centers);
+  if (nc == 1) {  // every finite value in the one bin
+    int64_t k = 0;
+    for (int64_t i = 0; i < n; ++i) k += std::isfinite(values[i]) ? 1 : 0;
+    out[0] = static_cast<double>(k);
+    return PS2_OK;
+  }
+  // equal spacing test and the ceil rule's constants, as the reference computes them
+  double amax = 0.0;
+  for (int i = 0; i < nc; ++i) amax = std::max(amax, std::fabs(centers[i]));
+  const double d0 = centers[1] - centers[0];
+  bool equal = true;  // all |diff - diff[0]| <= eps * max(1, max |centre|)
+  for (int i = 0; i + 1 < nc; ++i)
+    if (!(std::fabs((centers[i + 1] - centers[i]) - d0) <= 2.220446049250313e-16 * std::max(1.0, amax))) equal = false;
+  const double d = nc < 3 ? 1.0 : (centers[nc - 1] - centers[0]) / static_cast<double>(nc - 1);
+  const double cutoff0 = (centers[0] + centers[1]) / 2.0;
+  std::vector<double> mids(nc - 1);
+  for (int i = 0; i + 1 < nc; ++i) mids[i] = (centers[i] + centers[i + 1]) / 2.0;
+  if (n == 0) {
+    for (int i = 0; i < nc; ++i) out[i] = 0.0;
+    return PS2_OK;
+  }
+  Scoped sc;
+  int rc = scoped_init(sc);
+  if (rc) return rc;
+  DevBuf dv, dm, dcnt;
+  CK(dv.alloc(sizeof(double) * n));
+  CK(cudaMemcpyAsync(dv.p, values, sizeof(double) * n, cudaMemcpyHostToDevice, sc.st));
+  CK(dm.alloc(sizeof(double) * (nc - 1)));
+  CK(cudaMemcpyAsync(dm.p, mids.data(), sizeof(double) * (nc - 1), cudaMemcpyHostToDevice, sc.st));
+  CK(dcnt.alloc(sizeof(unsigned long long) * nc));
+  CK(cudaMemsetAsync(dcnt.p, 0, sizeof(unsigned long long) * nc, sc.st));
+  CK(launch_hist_centers(dv.as<double>(), n, dm.as<double>(), nc, equal ? 1 : 0, d, cutoff0,
+                         dcnt.as<unsigned long long>(), sc.sm, sc.st));
+  std::vector<unsigned long long> cnt(nc);
+  CK(cudaMemcpyAsync(cnt.data(), dcnt.p, sizeof(unsigned long long) * nc, cudaMemcpyDeviceToHost, sc.st));
+  CK(cudaStreamSynchronize(sc.st));
+  for (int i = 0; i < nc; ++i) out[i] = static_cast<double>(cnt[i]);
+  return PS2_OK;
+}
+
 int ps2_clap_filter_grid(const float* ph_grid, int64_t n_i, int64_t n_j, int64_t m, int64_t clap_window, double alpha,
                          double beta, const double* low_pass, int64_t n_win_ex, float* out) {
   if (!ph_grid || !out || !low_pass || n_i <= 0 || n_j <= 0 || m <= 0)

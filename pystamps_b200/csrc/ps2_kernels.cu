@@ -2178,6 +2178,266 @@ cudaError_t launch_s3_fit(const S3FitArgs& a, int sm_count, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// ================================================= registry topofit =======
+// The registry's topofit (pystamps/kernels/accelerated.py:316-380 ->
+// ported._ps_topofit_single, pystamps/pipeline/ported.py:2355-2431; the PyO3
+// twin src/lib.rs:525-586 uses the same rule with tolerance 5e-3): per row,
+// the non-zero columns only (zero columns take no part; an all-zero row gives
+// NaN), trial coherences with columns summed in order, the near-max candidate
+// set (local maxima within `tol` of the maximum), every candidate refined
+// (_ps_topofit_refine_candidate, :2480-2513) and the reference's choice among
+// them (_ps_topofit_select_candidate, :2451-2477). R is the row's real type:
+// float for complex64 rows (the reference's single-precision path), double for
+// complex128 rows. One warp per row.
+template <typename R>
+struct NearFit {
+  R K, C, coh;
+};
+
+template <typename R>
+__device__ __forceinline__ typename CT<R>::C cis_neg_r(R x) {
+  R s, c;
+  sincos_r(x, &s, &c);
+  return mk(c, -s);
+}
+
+template <typename R>
+__device__ NearFit<R> near_refine(const typename CT<R>::C* cv, const R* bv, int nf, R den_lin, double coarse_k0,
+                                  int lane) {
+  using C = typename CT<R>::C;
+  R K0 = static_cast<R>(coarse_k0);
+  R ox = 0, oy = 0;
+  for (int k = lane; k < nf; k += 32) {
+    const C r = cmul_rn(cv[k], cis_neg_r<R>(mul_rn(K0, bv[k])));
+    ox = add_rn(ox, r.x);
+    oy = add_rn(oy, r.y);
+  }
+  ox = warp_sum(ox);
+  oy = warp_sum(oy);
+  R mo = 0;
+  for (int k = lane; k < nf; k += 32) {
+    const C r = cmul_rn(cv[k], cis_neg_r<R>(mul_rn(K0, bv[k])));
+    const C q = cmul_rn(r, mk(ox, -oy));
+    const R wgt = hypot_r(cv[k].x, cv[k].y);
+    mo = add_rn(mo, mul_rn(mul_rn(wgt, bv[k]), mul_rn(wgt, atan2_r(q.y, q.x))));
+  }
+  mo = warp_sum(mo);
+  K0 = add_rn(K0, mo / den_lin);
+  R mx = 0, my = 0, den = 0;
+  for (int k = lane; k < nf; k += 32) {
+    const C r = cmul_rn(cv[k], cis_neg_r<R>(mul_rn(K0, bv[k])));
+    mx = add_rn(mx, r.x);
+    my = add_rn(my, r.y);
+    den = add_rn(den, hypot_r(r.x, r.y));
+  }
+  mx = warp_sum(mx);
+  my = warp_sum(my);
+  den = warp_sum(den);
+  if (den == R(0)) den = R(1);
+  return {K0, atan2_r(my, mx), hypot_r(mx, my) / den};
+}
+
+template <typename R>
+__global__ void __launch_bounds__(32) k_topofit_near_max(NearMaxArgs a) {
+  using C = typename CT<R>::C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x;
+  const int M = a.M, T = 2 * a.n_half + 1;
+  C* cv = reinterpret_cast<C*>(smem_raw);  // valid columns, compacted in column order
+  R* bv = reinterpret_cast<R*>(cv + M);
+  R* tp = bv + M;
+  R* ct = tp + M;
+  int* col = reinterpret_cast<int*>(ct + T);
+  const C* cpx = static_cast<const C*>(a.cpx);
+  const R* bp = static_cast<const R*>(a.bp);
+  const double nanv = __longlong_as_double(0x7ff8000000000000LL);
+  for (int64_t r = blockIdx.x; r < a.n; r += gridDim.x) {
+    int nf = 0;
+    for (int c0 = 0; c0 < M; c0 += 32) {
+      const int c = c0 + lane;
+      C v = mk(R(0), R(0));
+      R b = 0;
+      bool valid = false;
+      if (c < M) {
+        v = cpx[r * M + c];
+        b = a.bp_row_inv ? bp[c] : bp[r * M + c];
+        valid = !(v.x == R(0) && v.y == R(0));  // complex != 0 (NaN parts count as non-zero)
+        if (a.residual) a.residual[r * M + c] = make_float2(0.f, 0.f);
+      }
+      const unsigned bal = __ballot_sync(kFull, valid);
+      if (valid) {
+        const int k = nf + __popc(bal & ((1u << lane) - 1u));
+        cv[k] = v;
+        bv[k] = b;
+        col[k] = c;
+      }
+      nf += __popc(bal);
+    }
+    __syncwarp();
+    if (nf == 0) {
+      if (lane == 0) a.K[r] = a.C[r] = a.coh[r] = nanv;
+      continue;
+    }
+    R mn = bv[0], mx = bv[0];
+    for (int k = lane; k < nf; k += 32) {
+      mn = mn < bv[k] ? mn : bv[k];
+      mx = mx > bv[k] ? mx : bv[k];
+    }
+    mn = warp_min(mn);
+    mx = warp_max(mx);
+    double range = static_cast<double>(add_rn(mx, -mn));
+    if (range == 0.0) range = 1.0;
+    const R range_r = static_cast<R>(range), qp = static_cast<R>(3.14159265358979323846 / 4.0);
+    R den = 0, dl = 0;
+    for (int k = lane; k < nf; k += 32) {
+      tp[k] = mul_rn(bv[k] / range_r, qp);
+      const R ab = hypot_r(cv[k].x, cv[k].y);
+      const R wb = mul_rn(ab, bv[k]);
+      den = add_rn(den, ab);
+      dl = add_rn(dl, mul_rn(wb, wb));
+    }
+    R denom = warp_sum(den), den_lin = warp_sum(dl);
+    if (denom == R(0)) denom = R(1);
+    if (den_lin == R(0)) den_lin = R(1);
+    __syncwarp();
+    // coherence of every trial, columns summed in order
+    R cmax = -1;
+    for (int t = lane; t < T; t += 32) {
+      const R tm = static_cast<R>(t - a.n_half);
+      R sx = 0, sy = 0;
+      for (int k = 0; k < nf; ++k) {
+        const C p = cmul_rn(cis_neg_r<R>(mul_rn(tp[k], tm)), cv[k]);
+        sx = add_rn(sx, p.x);
+        sy = add_rn(sy, p.y);
+      }
+      ct[t] = hypot_r(sx, sy) / denom;
+      cmax = cmax > ct[t] ? cmax : ct[t];
+    }
+    cmax = warp_max(cmax);
+    __syncwarp();
+    int n_cand = 0, first = -1, last = -1, coarse_best = -1, refined_best = -1;
+    NearFit<R> best_fit{0, 0, -1};
+    R coarse_best_v = -1;
+    for (int t0 = 0; t0 < T; t0 += 32) {
+      const int t = t0 + lane;
+      bool cand = false;
+      if (t < T) {
+        const R v = ct[t];
+        bool lm;
+        if (T == 1) lm = true;
+        else if (t == 0) lm = v >= ct[1];
+        else if (t == T - 1) lm = v >= ct[T - 2];
+        else lm = v >= ct[t - 1] && v >= ct[t + 1];
+        cand = lm && static_cast<double>(v) >= static_cast<double>(cmax) - a.tol;
+      }
+      unsigned bal = __ballot_sync(kFull, cand);
+      while (bal) {
+        const int tt = t0 + __ffs(bal) - 1;
+        bal &= bal - 1;
+        if (first < 0) first = tt;
+        last = tt;
+        ++n_cand;
+        if (ct[tt] > coarse_best_v) {
+          coarse_best_v = ct[tt];
+          coarse_best = tt;
+        }
+        const NearFit<R> f =
+            near_refine<R>(cv, bv, nf, den_lin, (3.14159265358979323846 / 4.0) / range * (tt - a.n_half), lane);
+        if (static_cast<double>(f.coh) > static_cast<double>(best_fit.coh)) {
+          best_fit = f;
+          refined_best = tt;
+        }
+      }
+    }
+    if (n_cand == 0) {  // no local maximum within tol (NaN coherences): np.argmax (a NaN wins)
+      for (int t = 0; t < T; ++t) {
+        if (isnan(ct[t])) {
+          coarse_best = t;
+          break;
+        }
+        if (ct[t] > coarse_best_v) {
+          coarse_best_v = ct[t];
+          coarse_best = t;
+        }
+      }
+      if (coarse_best < 0) coarse_best = 0;
+    }
+    int pick = refined_best;
+    if (n_cand <= 1 || (n_cand == 2 && first == 0 && last == T - 1)) pick = coarse_best;
+    if (pick < 0) pick = coarse_best >= 0 ? coarse_best : 0;
+    NearFit<R> f = best_fit;
+    if (pick != refined_best)
+      f = near_refine<R>(cv, bv, nf, den_lin, (3.14159265358979323846 / 4.0) / range * (pick - a.n_half), lane);
+    if (a.residual)
+      for (int k = lane; k < nf; k += 32) {
+        const C res = cmul_rn(cv[k], cis_neg_r<R>(mul_rn(f.K, bv[k])));
+        a.residual[r * M + col[k]] = make_float2(static_cast<float>(res.x), static_cast<float>(res.y));
+      }
+    if (lane == 0) {
+      a.K[r] = static_cast<double>(f.K);
+      a.C[r] = static_cast<double>(f.C);
+      a.coh[r] = static_cast<double>(f.coh);
+    }
+    __syncwarp();
+  }
+}
+
+size_t topofit_near_max_smem(bool fp64, int M, int n_half) {
+  const size_t rs = fp64 ? sizeof(double) : sizeof(float);
+  return static_cast<size_t>(M) * (2 * rs + rs + rs + sizeof(int)) + static_cast<size_t>(2 * n_half + 1) * rs + 16;
+}
+
+cudaError_t launch_topofit_near_max(const NearMaxArgs& a, bool fp64, int sm_count, cudaStream_t st) {
+  if (a.n <= 0) return cudaSuccess;
+  const size_t sm = topofit_near_max_smem(fp64, a.M, a.n_half);
+  cudaError_t e = kernel_attributes_once(sm);
+  if (e != cudaSuccess) return e;
+  const int64_t blocks = std::min<int64_t>(a.n, static_cast<int64_t>(sm_count) * 32);
+  if (fp64)
+    k_topofit_near_max<double><<<static_cast<unsigned>(blocks), 32, sm, st>>>(a);
+  else
+    k_topofit_near_max<float><<<static_cast<unsigned>(blocks), 32, sm, st>>>(a);
+  return cudaGetLastError();
+}
+
+// ================================================ histogram with centers ==
+// The registry's stage2_histogram (pystamps/kernels/accelerated.py:235-265):
+// equally spaced centres use the ceil rule 1 + max(0, min(nc-1,
+// ceil((v - cutoff0) / d))); otherwise the bin is searchsorted(mids, v,
+// 'left') clipped to [0, nc-1]. Non-finite values are skipped. Integer
+// atomics: the counts do not depend on the order.
+__global__ void __launch_bounds__(256) k_hist_centers(const double* __restrict__ v, int64_t n,
+                                                      const double* __restrict__ mids, int nc, int equal, double d,
+                                                      double cutoff0, unsigned long long* __restrict__ counts) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double s = v[i];
+    if (!isfinite(s)) continue;
+    int b;
+    if (equal) {
+      const double q = ceil((s - cutoff0) / d);
+      b = static_cast<int>(fmax(0.0, fmin(static_cast<double>(nc - 1), q)));
+    } else {
+      int lo = 0, hi = nc - 1;  // first of the nc-1 mids that is >= s
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (mids[mid] < s) lo = mid + 1;
+        else hi = mid;
+      }
+      b = lo;
+    }
+    atomicAdd(&counts[b], 1ull);
+  }
+}
+
+cudaError_t launch_hist_centers(const double* v, int64_t n, const double* mids, int nc, int equal, double d,
+                                double cutoff0, unsigned long long* counts, int sm_count, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int64_t blocks = std::min<int64_t>((n + 255) / 256, static_cast<int64_t>(sm_count) * 8);
+  k_hist_centers<<<static_cast<unsigned>(blocks), 256, 0, st>>>(v, n, mids, nc, equal, d, cutoff0, counts);
+  return cudaGetLastError();
+}
+
 // ============================================================== batches ===
 // Many patches, each iteration one launch per step over every active patch.
 // Work units are numbered patch after patch (prefix tables); a unit finds its
@@ -3059,6 +3319,8 @@ cudaError_t kernel_attributes_once(size_t dynamic_smem) {
         r == cudaSuccess ? opt_in_smem(k_random_hist, optin) : r,
         r == cudaSuccess ? opt_in_smem(k_s3_clap, optin) : r,
         r == cudaSuccess ? opt_in_smem(k_s3_fit, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_topofit_near_max<float>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_topofit_near_max<double>, optin) : r,
         r == cudaSuccess ? opt_in_smem(k_batch_clap, optin) : r,
         r == cudaSuccess ? opt_in_smem(k_batch_topofit<4>, optin) : r,
         r == cudaSuccess ? opt_in_smem(k_batch_topofit<8>, optin) : r,

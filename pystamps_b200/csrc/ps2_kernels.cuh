@@ -218,6 +218,27 @@ cudaError_t topofit_geometry(const TopoArgs& a, int grid_cap, int* L_out, int* m
 cudaError_t launch_batch_reset(const BatchArgs& b, cudaStream_t st);
 cudaError_t launch_s3_clap(const S3ClapArgs& a, const Twiddles32f& tf, int sm_count, cudaStream_t st);
 cudaError_t launch_s3_fit(const S3FitArgs& a, int sm_count, cudaStream_t st);
+
+// ----------------------------------------------------- registry topofit --
+// _ps_topofit_single over rows (pystamps/pipeline/ported.py:2355-2431):
+// near-max candidates within tol, each refined, the reference's choice.
+struct NearMaxArgs {
+  const void* cpx;   // complex [n, M] (complex64 or complex128)
+  const void* bp;    // real [n, M], or [M] when bp_row_inv
+  int bp_row_inv;
+  int64_t n;
+  int M, n_half;
+  double tol;
+  double* K;
+  double* C;
+  double* coh;
+  float2* residual;  // complex64 [n, M] or NULL
+};
+size_t topofit_near_max_smem(bool fp64, int M, int n_half);
+cudaError_t launch_topofit_near_max(const NearMaxArgs& a, bool fp64, int sm_count, cudaStream_t st);
+// histogram_with_centers (pystamps/kernels/accelerated.py:235-265)
+cudaError_t launch_hist_centers(const double* v, int64_t n, const double* mids, int nc, int equal, double d,
+                                double cutoff0, unsigned long long* counts, int sm_count, cudaStream_t st);
 cudaError_t launch_batch_bin(const BatchArgs& b, int64_t total, int sm_count, cudaStream_t st);
 cudaError_t launch_batch_clap(const BatchArgs& b, int64_t total, const Twiddles32f& tf, int sm_count,
                               cudaStream_t st);

@@ -20,7 +20,9 @@ Fixtures (all seeded):
 * stage2_iter1.npz    -- ported.stage2_estimate_gamma(kernel_backend="python")
                          on a 3,000 PS x 10 ifg synthetic patch, one iteration
                          (gamma_max_iterations=1, so the random-phase histogram
-                         does not enter), written as pm1.mat and re-read.
+                         does not enter), written as pm1.mat and re-read: the
+                         19 pm1 variables as stored (shapes, dtypes) and the
+                         parms the patch was written with.
 * stage2_3ps.npz      -- the same entry point on the reference's 3-PS fixture
                          (native_stage2.rs:2698-2769: empty CLAP, all rows
                          invalid).
@@ -30,6 +32,13 @@ Fixtures (all seeded):
                          (complex64 unit phasors, f32 bperp) on 128 rows, and
                          ported._coh_threshold_from_dist for both selection
                          methods.
+* registry_kernels.npz -- the registry kernels stage2_topofit,
+                         stage2_topofit_row_invariant,
+                         stage2_topofit_coh_row_invariant and stage2_histogram
+                         (pystamps/kernels/accelerated.py:410-509) with the
+                         python provider, on the reference's own random case and
+                         on seeded 400 x 40 rows with zero columns, in complex64
+                         and complex128.
 * stage3_select.npz   -- ported.stage3_select_ps after the Python stage 2 on a
                          10,000 PS x 8 ifg patch over a 40 x 40 grid: the
                          select1.mat variables (ix, keep_ix, ph_patch2,
@@ -150,7 +159,8 @@ def _run_python_stage2(ported, p: dict) -> dict:
         ported.stage2_estimate_gamma(patch, kernel_backend="python")
         pm = loadmat(patch / "pm1.mat")
     keys = ["K_ps", "C_ps", "coh_ps", "N_opt", "ph_res", "ph_patch", "ph_grid", "ph_weight", "grid_ij",
-            "n_trial_wraps", "i_loop", "coh_ps_save", "gamma_change_save", "low_pass", "grid_size"]
+            "n_trial_wraps", "i_loop", "coh_ps_save", "gamma_change_save", "low_pass", "grid_size", "Nr",
+            "Nr_max_nz_ix", "coh_bins", "step_number"]
     return {k: np.asarray(pm[k]) for k in keys if k in pm}
 
 
@@ -165,6 +175,8 @@ def make_stage2_iter1(ported) -> None:
         HERE / "stage2_iter1.npz",
         ph=p["ph"], bperp=p["bperp"], bperp_mat=p["bperp_mat"], D_A=p["D_A"], xy=p["xy"],
         mean_incidence=p["mean_incidence"], max_topo_err=20.0,
+        parms_keys=np.asarray(list(p["parms"].keys())),
+        parms_values=np.asarray([str(v) for v in p["parms"].values()]),
         **{"pm_" + k: v for k, v in pm.items()},
     )
 
@@ -275,6 +287,60 @@ def make_stage3_select(ported) -> None:
     )
 
 
+def make_registry(ported) -> None:
+    """The reference's stage-2 registry kernels with the python provider
+    (pystamps/kernels/accelerated.py:410-509): topofit (generic and
+    row-invariant, complex64 and complex128 inputs, rows with zero columns and
+    an all-zero row), the row-invariant coherence and the histogram."""
+    from pystamps.kernels import accelerated as accel
+
+    out = {}
+    # the random case of the reference's native-vs-python test (tests/test_kernels_accelerated.py:666-713)
+    rng = np.random.default_rng(11)
+    out["t0_cpx"] = np.exp(1j * rng.normal(size=(6, 5))).astype(np.complex128)
+    out["t0_bp"] = rng.normal(size=(6, 5)).astype(np.float64)
+    out["t0_bprow"] = np.tile(np.asarray([-120.0, -40.0, 0.0, 55.0, 90.0]), (6, 1))
+    out["t0_ntw"] = np.float64(1.5)
+    # larger seeded rows: 400 x 40, row-variant bperp, trial count 81
+    rng = np.random.default_rng(77)
+    n, m = 400, 40
+    bp_ifg = rng.uniform(-300, 300, m)
+    bp = (1.0 + 0.02 * rng.uniform(-0.5, 0.5, n))[:, None] * bp_ifg[None, :]
+    k = rng.uniform(-0.04, 0.04, n)
+    cpx = np.exp(1j * (k[:, None] * bp + rng.normal(0.0, rng.uniform(0.1, 1.5, n)[:, None], (n, m))))
+    cpx *= rng.uniform(0.5, 1.5, (n, m))
+    cpx[rng.random((n, m)) < 0.03] = 0
+    cpx[5] = 0
+    out["t1_cpx"] = cpx.astype(np.complex128)
+    out["t1_bp"] = bp.astype(np.float64)
+    out["t1_ntw"] = np.float64(4.94)
+    for name in ("t0", "t1"):
+        c128, b64, ntw = out[name + "_cpx"], out[name + "_bp"], float(out[name + "_ntw"])
+        brow = out.get(name + "_bprow", np.tile(b64[0], (b64.shape[0], 1)))
+        for prec, c, b, br in (("d", c128, b64, brow), ("s", c128.astype(np.complex64), b64.astype(np.float32),
+                                                        brow.astype(np.float32))):
+            K, C, coh, res = accel.run_stage2_topofit_kernel(c, b, ntw, backend="python")
+            out.update({f"{name}{prec}_gen_K": K, f"{name}{prec}_gen_C": C, f"{name}{prec}_gen_coh": coh,
+                        f"{name}{prec}_gen_res": res})
+            K, C, coh, res = accel.run_stage2_topofit_row_invariant_kernel(c, br, ntw, backend="python")
+            out.update({f"{name}{prec}_row_K": K, f"{name}{prec}_row_C": C, f"{name}{prec}_row_coh": coh,
+                        f"{name}{prec}_row_res": res})
+        out[name + "_cohrow"] = accel.run_stage2_topofit_coh_row_invariant_kernel(c128, brow, ntw, backend="python")
+    # histogram: the reference's case, the 100 coherence centres, unequal centres, one centre
+    rng = np.random.default_rng(5)
+    cases = {
+        "h0": (np.asarray([0.1, 0.49, 0.7, 0.9, np.nan]), np.asarray([0.0, 0.5, 1.0])),
+        "h1": (np.concatenate([rng.random(10_000), [np.nan, np.inf, -0.3, 1.7, 0.005, 0.995]]),
+               0.005 + 0.01 * np.arange(100)),
+        "h2": (rng.normal(0.0, 2.0, 5_000), np.asarray([-3.0, -1.0, -0.5, 0.0, 0.25, 2.0, 5.0])),
+        "h3": (rng.random(100), np.asarray([0.5])),
+    }
+    for name, (v, c) in cases.items():
+        out[name + "_v"], out[name + "_c"] = v, c
+        out[name + "_out"] = accel.run_stage2_histogram_kernel(v, c, backend="python")
+    np.savez_compressed(HERE / "registry_kernels.npz", **out)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, type=Path)
@@ -282,7 +348,7 @@ def main() -> None:
     a = ap.parse_args()
     ported = _import_reference(a.reference)
     todo = {"clap": make_clap, "topofit": make_topofit, "iter1": make_stage2_iter1, "3ps": make_stage2_3ps,
-            "stage3_units": make_stage3_units, "stage3_select": make_stage3_select}
+            "stage3_units": make_stage3_units, "stage3_select": make_stage3_select, "registry": make_registry}
     for name, fn in todo.items():
         if a.only and name not in a.only.split(","):
             continue

@@ -106,7 +106,7 @@ def test_topofit_against_oracle(K, oracle, golden):
     cpx = d["cpx"].astype(np.complex64)
     bp = d["bperp"]
     ntw = float(d["n_trial_wraps"])
-    Kg, Cg, hg, rg = K.run_stage2_topofit_kernel(cpx, bp, ntw)
+    Kg, Cg, hg, rg = K.run_native_topofit_rows(cpx, bp, ntw)
     Ko, Co, ho, ro, _ = oracle.topofit(cpx, bp, ntw)
     np.testing.assert_allclose(Kg, Ko, rtol=K_REL_TOL, atol=1e-7)
     np.testing.assert_allclose(hg, ho, rtol=0, atol=1e-5)
@@ -121,7 +121,7 @@ def test_topofit_zero_columns_and_empty_rows(K, oracle):
     cpx[rng.random((n, m)) < 0.1] = 0
     cpx[7] = 0  # all-zero row -> NaN
     bp = rng.uniform(-300, 300, (n, m))
-    Kg, Cg, hg, rg = K.run_stage2_topofit_kernel(cpx, bp, 3.3)
+    Kg, Cg, hg, rg = K.run_native_topofit_rows(cpx, bp, 3.3)
     Ko, Co, ho, ro, _ = oracle.topofit(cpx, bp.astype(np.float32).astype(np.float64), 3.3)
     assert np.isnan(Kg[7]) and np.isnan(hg[7]) and np.isnan(Cg[7])
     ok = ~np.isnan(Ko)
@@ -139,7 +139,7 @@ def test_topofit_random_rows_argmax_and_ties(K, oracle, m, ntw):
     k = rng.uniform(-0.04, 0.04, n)
     cpx = (np.exp(1j * (k[:, None] * bp + rng.normal(0, 0.8, (n, m))))).astype(np.complex64)
     bp32 = bp.astype(np.float32).astype(np.float64)
-    Kg, Cg, hg, _ = K.run_stage2_topofit_kernel(cpx, bp32, ntw)
+    Kg, Cg, hg, _ = K.run_native_topofit_rows(cpx, bp32, ntw)
     fr = oracle.fit_rows(np.ones((n, m), np.complex64), cpx, bp32, ntw)
     tie = _tie_mask(fr.best_coh, fr.second_coh)
     good = ~tie
