@@ -1,0 +1,149 @@
+"""CUDA path against the oracle on the benchmark shapes themselves.
+
+Config A (20,000 PS x 20 ifg, 64x64 grid, 81 trials) at full size: three
+teacher-forced iterations (each GPU iteration against the oracle's iteration
+applied to the GPU's previous state) and the loop run freely to convergence.
+
+Configs B (250,000 x 60, 128x128, 161 trials), D (100,000 x 40, 96x96, 121
+trials) and E (2,000,000 x 150, 256x256, 161 trials), first iteration:
+  * the binned grid bit-exact against the oracle's fill_phase_weight +
+    accumulate_grid on the whole grid;
+  * CLAP on the whole grid for a seeded subset of interferograms, through the
+    loop's resampled unit phase (ph_patch) and through the standalone CLAP
+    entry on the same grid slices;
+  * topofit against the oracle's fit_rows on a seeded sample of rows using
+    the GPU's own ph_patch; argmax ties (best and runner-up trial within 1e-6
+    relative) are counted and left out of the K tolerance.
+
+Config B, converged: the FP32 path's drift from the plain FP64 GPU path is
+compared with the oracle's own FP32-vs-FP64 drift on the same patch, so the
+free-running difference is shown to be the algorithm's sensitivity.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TIE_REL = 1e-6
+K_REL_TOL = 1e-4
+COH_TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def S(cuda_lib):
+    from pystamps_b200 import stage2
+
+    return stage2
+
+
+def _fit_check(fr, g_K, g_coh, g_nopt, where: str):
+    """Topofit of sampled rows against the oracle: returns the tie count and the largest differences."""
+    tie = (fr.best_coh - fr.second_coh) <= TIE_REL * np.maximum(fr.best_coh, 1e-30)
+    np.testing.assert_array_equal(np.isnan(g_K), np.isnan(fr.K), err_msg=where)
+    np.testing.assert_array_equal(g_nopt, fr.N_opt, err_msg=where)
+    good = ~tie & ~np.isnan(fr.K)
+    dcoh = np.abs(g_coh - fr.coh)[good]
+    dK = (np.abs(g_K - fr.K) / np.maximum(np.abs(fr.K), 1e-3))[good]
+    assert dcoh.max() <= COH_TOL, (where, dcoh.max())
+    assert dK.max() <= K_REL_TOL, (where, dK.max())
+    return int(tie.sum()), float(dcoh.max()), float(dK.max())
+
+
+def test_config_A_teacher_forced_full_size(S, oracle):
+    from pystamps_b200 import synth
+
+    from test_gpu_parity import _teacher_forced
+
+    patch = synth.make_workload("A")
+    n_ties = _teacher_forced(S, oracle, patch, iterations=3)
+    print(f"config A, 3 teacher-forced iterations: {n_ties} argmax ties")
+
+
+def test_config_A_free_running_to_convergence(S, oracle):
+    """Whole loop at config A, GPU and oracle each on their own state: same
+    iteration count, cells and invalid rows; the drift is bounded like the
+    smaller free-running tests and reported beside the oracle's own FP32 vs
+    FP64 drift."""
+    from pystamps_b200 import synth
+
+    from test_gpu_parity import _loop_compare, _sensitivity
+
+    patch = synth.make_workload("A")
+    g, o = _loop_compare(S, oracle, patch)
+    np.testing.assert_array_equal(g["grid_ij"], o["grid_ij"])
+    assert g["i_loop"] == o["i_loop"]
+    np.testing.assert_array_equal(np.isnan(g["K_ps"]), np.isnan(o["K_ps"]))
+    d = np.abs(g["coh_ps"] - o["coh_ps"])
+    d_gpu, d_ref = _sensitivity(oracle, patch, g, o)
+    print(f"config A converged ({g['i_loop']} iterations): median |dgamma| {d_gpu:.2e} "
+          f"(oracle FP32 vs FP64 {d_ref:.2e}), p90 {np.quantile(d, 0.9):.2e}, max {d.max():.2e}")
+    assert d_gpu <= 5e-4
+    assert np.quantile(d, 0.9) <= 1e-3
+
+
+def _first_iteration(S, oracle, name: str, n_clap_ifg: int, n_rows: int):
+    from pystamps_b200 import kernels, synth
+
+    patch = synth.make_workload(name)
+    prep = S.prepare_patch(patch)
+    del patch
+    with S.Stage2Context() as ctx:
+        ctx.load(prep)
+        ctx.iterate(1)
+        g = ctx.download(["ph_grid", "ph_patch", "K_ps", "coh_ps", "N_opt"])
+    bp = prep.bperp
+    # binning, whole grid, bit-exact (iteration 1: K = 0, w = 1/D_A)
+    pw = oracle.fill_phase_weight(prep.ph_nm, bp.astype(np.float64), np.zeros(prep.n_ps), prep.weight0)
+    grid_o = oracle.accumulate_grid(pw, prep.grid_lin, prep.n_i, prep.n_j)
+    del pw
+    np.testing.assert_array_equal(g["ph_grid"], grid_o)
+    # CLAP on the whole grid for a seeded subset of interferograms
+    rng = np.random.default_rng(2005 + prep.n_ifg)
+    sel = np.sort(rng.choice(prep.n_ifg, size=min(n_clap_ifg, prep.n_ifg), replace=False))
+    sub = np.ascontiguousarray(g["ph_grid"][:, :, sel])
+    filt_o = oracle.clap_filter_grid_stack(sub, prep.clap_alpha, prep.clap_beta, prep.low_pass)
+    filt_g = kernels.run_stage2_clap_filter_kernel(sub, prep.clap_alpha, prep.clap_beta, prep.low_pass)
+    rel = np.abs(filt_g - filt_o) / np.abs(filt_o).max()
+    assert rel.max() <= 2e-6, rel.max()
+    patch_o = oracle.extract_patch_phase(filt_o, prep.grid_lin)
+    dp = np.abs(g["ph_patch"][:, sel] - patch_o)
+    assert dp.max() <= 2e-4 and np.quantile(dp, 0.999) <= 1e-5, (dp.max(), np.quantile(dp, 0.999))
+    # topofit of a seeded row sample with the GPU's own resampled phase
+    rows = np.sort(rng.choice(prep.n_ps, size=min(n_rows, prep.n_ps), replace=False))
+    bpr = bp.astype(np.float64) if prep.row_invariant else np.ascontiguousarray(bp[rows], dtype=np.float64)
+    fr = oracle.fit_rows(g["ph_patch"][rows], prep.ph_nm[rows], bpr, prep.n_trial_wraps)
+    ties, dcoh, dK = _fit_check(fr, g["K_ps"][rows], g["coh_ps"][rows], g["N_opt"][rows], name)
+    print(f"config {name} first iteration: grid bit-exact ({prep.n_i}x{prep.n_j}x{prep.n_ifg}); CLAP on "
+          f"{sel.size} ifg max rel {rel.max():.2e}, ph_patch max {dp.max():.2e}; topofit on {rows.size} rows: "
+          f"{ties} argmax ties, non-tie max |dcoh| {dcoh:.2e}, max rel |dK| {dK:.2e}")
+
+
+@pytest.mark.parametrize("name,n_clap_ifg,n_rows", [("B", 12, 50_000), ("D", 12, 50_000), ("E", 8, 50_000)])
+def test_first_iteration_teacher_forced_benchmark_configs(S, oracle, name, n_clap_ifg, n_rows):
+    _first_iteration(S, oracle, name, n_clap_ifg, n_rows)
+
+
+def test_config_B_converged_drift_is_the_algorithms(S, oracle):
+    """FP32 vs FP64 after convergence at config B: the GPU pair (FP32 path vs
+    plain FP64 path) against the oracle pair (the restatement in FP32 vs its
+    FP64 instantiation). Both trajectories separate through the P-square
+    table's round(1000 coh) steps and argmax near-ties; the GPU's drift must
+    be of the same size as the reference algorithm's own."""
+    from pystamps_b200 import synth
+
+    patch = synth.make_workload("B")
+    prep = S.prepare_patch(patch)
+    a = S.run_stage2(prep, precision="fp32", keys=["coh_ps", "K_ps"])
+    b = S.run_stage2(prep, precision="fp64", keys=["coh_ps", "K_ps"])
+    nr = np.concatenate([prep.nr, [prep.nr_max_nz_ix]])
+    o32 = oracle.stage2_run(dict(patch, nr_override=nr))
+    o64 = oracle.stage2_run(dict(patch, nr_override=nr), fp64=True)
+    dg = np.abs(a["coh_ps"] - b["coh_ps"])
+    do = np.abs(o32["coh_ps"] - o64["coh_ps"])
+    q = lambda d, p: float(np.quantile(d, p))  # noqa: E731
+    print(f"config B converged: GPU FP32 vs FP64 ({a['i_loop']}/{b['i_loop']} it) median {np.median(dg):.2e} "
+          f"p99 {q(dg, 0.99):.2e} max {dg.max():.2e}; oracle FP32 vs FP64 ({o32['i_loop']}/{o64['i_loop']} it) "
+          f"median {np.median(do):.2e} p99 {q(do, 0.99):.2e} max {do.max():.2e}")
+    assert abs(a["i_loop"] - o32["i_loop"]) <= 1
+    assert q(dg, 0.5) <= 3 * q(do, 0.5) + 1e-6
+    assert q(dg, 0.99) <= 3 * q(do, 0.99) + 1e-5
