@@ -132,6 +132,12 @@ int ps2_iterate(ps2_ctx* ctx, int64_t n_iter, ps2_iter_stats* stats);
  * first call after ps2_load_patch. PS2_NO_GRAPH=1 in the environment selects
  * individual launches throughout. */
 int ps2_run_to_convergence(ps2_ctx* ctx, ps2_iter_stats* last);
+/* Runs ONE gamma iteration under the reference's stop rule: when the rule
+ * holds the P-square update is skipped, as the loop does before it ends
+ * (native_stage2.rs:307-314); *stats (may be NULL) receives its statistics.
+ * For callers that act between iterations (per-iteration pm1 dumps,
+ * checkpoints); ps2_run_to_convergence is the fast path. */
+int ps2_step(ps2_ctx* ctx, ps2_iter_stats* stats);
 /* Resets the loop state of the loaded patch to iteration 1 (K=0, w=weight0). */
 int ps2_reset(ps2_ctx* ctx);
 int ps2_download(ps2_ctx* ctx, ps2_outputs* out);
@@ -141,6 +147,20 @@ int ps2_download(ps2_ctx* ctx, ps2_outputs* out);
  * each kernel family in it: [0] binning, [1] CLAP windows + overlap-add,
  * [2] topofit, [3] convergence / weighting update. */
 int ps2_last_timing(const ps2_ctx* ctx, double* total_ms, double* per_kernel_ms /*[4] or NULL*/);
+/* Checkpoint / resume of the gamma loop (the reference has none; its
+ * PYSTAMPS_STAGE2_NATIVE_DEBUG_PM dumps, native_stage2.rs:259, 337-356,
+ * 385-404, write pm1_iter_NN.mat but cannot restart from them).
+ * ps2_export_state copies the loop state after the last iteration (K, weights,
+ * coherence, C, N_opt, the P-square table, scaled Nr, the convergence state and
+ * iteration count; ph_res with SNR weighting) into a host buffer: call it with
+ * buf NULL to get the size in *bytes, then with a buffer of that size. The
+ * blob is opaque (the context's cell-sorted row order) and valid for the same
+ * patch loaded the same way, in the same precision: ps2_import_state into a
+ * context holding that patch restores the state, and ps2_run_to_convergence /
+ * ps2_step / ps2_iterate then continue from the next iteration with the same
+ * results as an uninterrupted run. Mismatched or truncated states are rejected. */
+int ps2_export_state(ps2_ctx* ctx, void* buf, int64_t* bytes);
+int ps2_import_state(ps2_ctx* ctx, const void* buf, int64_t bytes);
 /* Times the FP32 topofit of the loaded patch with 4, 8, 16 and 32 lanes per PS
  * and keeps the fastest for this context and for later loads with the same
  * n_ifg and power-of-two PS bucket (process-wide table). ms_per_candidate:
@@ -214,7 +234,10 @@ int ps2_random_coherence_histogram(const double* bperp_nm, int64_t n_ifg, double
  * serialised by the caller. The first call on a device resolves the array's
  * device address (cudaGetSymbolAddress) with that device current; make that
  * first call before any stream capture. low_pass is a host pointer
- * [32*32]. This entry point has no counterpart in the reference. */
+ * [32*32]; its values (and the window weights) travel to the GPU inside the
+ * arguments of a kernel the call queues, so the caller may reuse or free it as
+ * soon as the call returns. This entry point has no counterpart in the
+ * reference. */
 int ps2_clap_filter_grid_noalloc(const float* d_ph_grid, int64_t n_i, int64_t n_j, int64_t m, int64_t clap_window,
                                  double alpha, double beta, const double* low_pass, int64_t n_win_ex, float* d_out,
                                  void* stream);

@@ -14,6 +14,7 @@
 // Real/complex are f32/complex64 for PS2_PRECISION_FP32 and f64/complex128
 // for PS2_PRECISION_FP64.
 #include <cuda_runtime.h>
+#include <sched.h>
 
 #include <algorithm>
 #include <cmath>
@@ -23,6 +24,7 @@
 #include <cstring>
 #include <cstdlib>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -512,6 +514,38 @@ int reset_state(ps2_ctx* c) {
   return PS2_OK;
 }
 
+// Checkpoint blob of the gamma loop (ps2_export_state / ps2_import_state).
+struct StateHeader {
+  char magic[8];  // "PS2LOOP\0"
+  int32_t version, fp64, psquare, reserved;
+  int64_t N, M, G, iters_done;
+  ps2_iter_stats last;
+};
+constexpr int32_t kStateVersion = 1;
+
+// The loop state after an iteration, in the blob's order: K (current), K
+// binned with, w, coh, C (real [N] each), N_opt (u8 [N]), the P-square table
+// (f64 [1001]), scaled Nr (f64 [100]), the convergence state (f64 [4]) and the
+// last statistics record (f64 [8]); with SNR weighting also ph_res (real [N, M]).
+struct StatePart {
+  DevBuf* buf;
+  size_t bytes;
+};
+std::vector<StatePart> state_parts(ps2_ctx* c) {
+  const size_t R = rsz(c), N = static_cast<size_t>(c->N);
+  std::vector<StatePart> v = {{&c->K[0], R * N}, {&c->K[1], R * N}, {&c->w, R * N},
+                              {&c->coh, R * N},  {&c->C, R * N},    {&c->nopt, N},
+                              {&c->lut, sizeof(double) * 1001},   {&c->nr_scaled, sizeof(double) * PS2_COH_BINS},
+                              {&c->state, sizeof(double) * 4},    {&c->stats, sizeof(double) * 8}};
+  if (!c->psquare) v.push_back({&c->ph_res, R * N * static_cast<size_t>(c->M)});
+  return v;
+}
+size_t state_bytes(ps2_ctx* c) {
+  size_t b = sizeof(StateHeader);
+  for (const auto& p : state_parts(c)) b += p.bytes;
+  return b;
+}
+
 }  // namespace
 
 // ====================================================================== ABI
@@ -747,6 +781,28 @@ int ps2_load_patch(ps2_ctx* c, const ps2_patch_desc* d) {
   return PS2_OK;
 }
 
+int ps2_step(ps2_ctx* c, ps2_iter_stats* stats) {
+  if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "no patch loaded");
+  CK(cudaSetDevice(c->device));
+  int rc = ensure_events(c, 5);
+  if (rc) return rc;
+  c->launches = 0;
+  rc = run_one_iteration(c, false, c->evpool.data());
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(c->h_stats, c->stats.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  float ms;
+  c->last_ms = 0.0;
+  for (int i = 0; i < 4; ++i) {
+    CK(cudaEventElapsedTime(&ms, c->evpool[i], c->evpool[i + 1]));
+    c->kernel_ms[i] = ms;
+    c->last_ms += ms;
+  }
+  fill_stats(c->h_stats, &c->last);
+  if (stats) *stats = c->last;
+  return PS2_OK;
+}
+
 int ps2_reset(ps2_ctx* c) {
   if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "no patch loaded");
   CK(cudaSetDevice(c->device));
@@ -845,6 +901,70 @@ int ps2_run_to_convergence(ps2_ctx* c, ps2_iter_stats* last) {
     if (c->last.stop) break;
   }
   if (last) *last = c->last;
+  return PS2_OK;
+}
+
+int ps2_export_state(ps2_ctx* c, void* buf, int64_t* bytes) {
+  if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "no patch loaded");
+  if (!bytes) return set_err(PS2_ERR_INVALID_ARG, "ps2_export_state: bytes is NULL");
+  const size_t need = state_bytes(c);
+  if (!buf) {
+    *bytes = static_cast<int64_t>(need);
+    return PS2_OK;
+  }
+  if (*bytes < static_cast<int64_t>(need))
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_export_state: buffer of %lld bytes, %zu needed", (long long)*bytes, need);
+  CK(cudaSetDevice(c->device));
+  StateHeader h{};
+  std::memcpy(h.magic, "PS2LOOP", 8);
+  h.version = kStateVersion;
+  h.fp64 = c->fp64 ? 1 : 0;
+  h.psquare = c->psquare;
+  h.N = c->N;
+  h.M = c->M;
+  h.G = c->G;
+  h.iters_done = c->iters_done;
+  h.last = c->last;
+  unsigned char* out = static_cast<unsigned char*>(buf);
+  std::memcpy(out, &h, sizeof(h));
+  size_t off = sizeof(h);
+  for (const auto& p : state_parts(c)) {
+    CK(cudaMemcpyAsync(out + off, p.buf->p, p.bytes, cudaMemcpyDeviceToHost, c->st));
+    off += p.bytes;
+  }
+  CK(cudaStreamSynchronize(c->st));
+  *bytes = static_cast<int64_t>(need);
+  return PS2_OK;
+}
+
+int ps2_import_state(ps2_ctx* c, const void* buf, int64_t bytes) {
+  if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "no patch loaded");
+  if (!buf || bytes < static_cast<int64_t>(sizeof(StateHeader)))
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_import_state: no state");
+  StateHeader h;
+  std::memcpy(&h, buf, sizeof(h));
+  if (std::memcmp(h.magic, "PS2LOOP", 8) != 0 || h.version != kStateVersion)
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_import_state: not a loop state of this library version");
+  if (h.fp64 != (c->fp64 ? 1 : 0) || h.psquare != c->psquare || h.N != c->N || h.M != c->M || h.G != c->G)
+    return set_err(PS2_ERR_INVALID_ARG,
+                   "ps2_import_state: the state is of a %lld x %lld patch (%lld cells, %s, %s weighting); the "
+                   "loaded patch is %lld x %lld (%lld cells, %s, %s weighting)",
+                   (long long)h.N, (long long)h.M, (long long)h.G, h.fp64 ? "FP64" : "FP32",
+                   h.psquare ? "P-square" : "SNR", (long long)c->N, (long long)c->M, (long long)c->G,
+                   c->fp64 ? "FP64" : "FP32", c->psquare ? "P-square" : "SNR");
+  if (bytes < static_cast<int64_t>(state_bytes(c)))
+    return set_err(PS2_ERR_INVALID_ARG, "ps2_import_state: state truncated (%lld of %zu bytes)", (long long)bytes,
+                   state_bytes(c));
+  CK(cudaSetDevice(c->device));
+  const unsigned char* in = static_cast<const unsigned char*>(buf);
+  size_t off = sizeof(h);
+  for (const auto& p : state_parts(c)) {
+    CK(cudaMemcpyAsync(p.buf->p, in + off, p.bytes, cudaMemcpyHostToDevice, c->st));
+    off += p.bytes;
+  }
+  CK(cudaStreamSynchronize(c->st));
+  c->iters_done = h.iters_done;
+  c->last = h.last;
   return PS2_OK;
 }
 
@@ -1396,6 +1516,20 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 std::mutex g_noalloc_mu;
 void* g_noalloc_ptr[128] = {nullptr};
 
+// The low-pass filter and the scaled pyramid weights reach the scratch array
+// as a kernel argument (copied when the launch is queued), so the call queues
+// no copy from host memory whose lifetime ends with the call.
+struct NoAllocTables {
+  double low_pass[1024];
+  double ws[1024];
+  int n_ws;
+};
+
+__global__ void k_noalloc_tables(const NoAllocTables t, double* __restrict__ lp, double* __restrict__ ws) {
+  for (int i = threadIdx.x; i < 1024; i += blockDim.x) lp[i] = t.low_pass[i];
+  for (int i = threadIdx.x; i < t.n_ws; i += blockDim.x) ws[i] = t.ws[i];
+}
+
 int noalloc_scratch(void** out) {
   int dev = 0;
   CK(cudaGetDevice(&dev));
@@ -1447,8 +1581,13 @@ int ps2_clap_filter_grid_noalloc(const float* d_ph_grid, int64_t n_i, int64_t n_
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   std::vector<double> ws = window_weight_scaled(static_cast<int>(clap_window), 32);
-  CK(cudaMemcpyAsync(lp, low_pass, sizeof(double) * 1024, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(wsd, ws.data(), sizeof(double) * ws.size(), cudaMemcpyHostToDevice, st));
+  if (ws.size() > 1024) return set_err(PS2_ERR_UNSUPPORTED, "ps2_clap_filter_grid_noalloc: window too large");
+  NoAllocTables tables;
+  std::memcpy(tables.low_pass, low_pass, sizeof(double) * 1024);
+  std::memcpy(tables.ws, ws.data(), sizeof(double) * ws.size());
+  tables.n_ws = static_cast<int>(ws.size());
+  k_noalloc_tables<<<1, 256, 0, st>>>(tables, lp, wsd);
+  CK(cudaGetLastError());
   // the padded copy rewrites every element, so nothing stale survives from an earlier call
   CK(launch_pad_grid(d_ph_grid, grid, G, static_cast<int>(m), Mp, 8, st));
   if (W > 0) {
@@ -2273,18 +2412,45 @@ int ps2_shard_finalize(ps2_ctx* c, const double* stats, int64_t n_total, ps2_ite
 }  // extern "C"
 
 namespace {
+// Host threads this process may run on: its CPU affinity set (a job on a
+// shared host is usually pinned to fewer cores than the machine has).
+int usable_cores() {
+  cpu_set_t set;
+  CPU_ZERO(&set);
+  if (sched_getaffinity(0, sizeof(set), &set) == 0) {
+    const int n = CPU_COUNT(&set);
+    if (n > 0) return n;
+  }
+  const int hc = static_cast<int>(std::thread::hardware_concurrency());
+  return hc > 0 ? hc : 1;
+}
+
+// Splits rows [0, n) into contiguous ranges, one per thread (threads <= 0:
+// the usable cores), capped at the row count. The last range runs on the
+// calling thread, and so does any range whose thread cannot be started, so no
+// exception crosses the C ABI.
 template <typename F>
 void for_rows(int64_t n, int threads, F&& body) {
-  int nt = threads > 0 ? threads : static_cast<int>(std::thread::hardware_concurrency());
+  int nt = threads > 0 ? threads : usable_cores();
   if (nt < 1) nt = 1;
   if (static_cast<int64_t>(nt) > n) nt = static_cast<int>(std::max<int64_t>(n, 1));
   std::vector<std::thread> pool;
+  std::vector<std::pair<int64_t, int64_t>> left;
   const int64_t per = (n + nt - 1) / nt;
   for (int t = 0; t < nt; ++t) {
     const int64_t a = t * per, b = std::min<int64_t>(n, a + per);
     if (a >= b) break;
-    pool.emplace_back([&body, a, b] { body(a, b); });
+    if (t + 1 == nt) {
+      left.emplace_back(a, b);
+      continue;
+    }
+    try {
+      pool.emplace_back([&body, a, b] { body(a, b); });
+    } catch (const std::system_error&) {
+      left.emplace_back(a, b);
+    }
   }
+  for (const auto& r : left) body(r.first, r.second);
   for (auto& th : pool) th.join();
 }
 }  // namespace

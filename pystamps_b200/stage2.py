@@ -21,6 +21,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import os
 from dataclasses import dataclass, field
 from pathlib import Path
 
@@ -354,6 +355,26 @@ class Stage2Context:
     def reset(self) -> None:
         check(self._lib.ps2_reset(self._ctx))
 
+    def step(self) -> dict:
+        """One iteration under the stop rule (ps2_step)."""
+        st = _lib.IterStats()
+        check(self._lib.ps2_step(self._ctx, ctypes.byref(st)))
+        return st.as_dict()
+
+    def export_state(self) -> bytes:
+        """The loop state after the last iteration (ps2_export_state): an opaque
+        checkpoint for this patch, loaded the same way, in this precision."""
+        n = ctypes.c_int64(0)
+        check(self._lib.ps2_export_state(self._ctx, None, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        check(self._lib.ps2_export_state(self._ctx, buf, ctypes.byref(n)))
+        return buf.raw[:n.value]
+
+    def import_state(self, state: bytes) -> None:
+        """Resume from a checkpoint of export_state (ps2_import_state): the next
+        step/iterate/run continues with the iteration after the checkpoint."""
+        check(self._lib.ps2_import_state(self._ctx, ctypes.c_char_p(state), ctypes.c_int64(len(state))))
+
     def run(self) -> dict:
         st = _lib.IterStats()
         check(self._lib.ps2_run_to_convergence(self._ctx, ctypes.byref(st)))
@@ -557,6 +578,19 @@ def stage2_estimate_gamma(patch_dir, backend: str = "auto", kernel_backend: str 
         raise ValueError(f"Unsupported stage-2 kernel backend '{kernel_backend}' for this package. Use: cuda")
     patch_dir = Path(patch_dir)
     patch = load_patch_dir(patch_dir)
-    res = run_stage2(patch, precision=precision, device=device)
+    if os.environ.get("PYSTAMPS_STAGE2_NATIVE_DEBUG_PM") is None:
+        res = run_stage2(patch, precision=precision, device=device)
+    else:
+        # the reference's per-iteration dumps (native_stage2.rs:259, 337-356,
+        # 385-404): pm1_iter_NN.mat after every iteration
+        p = prepare_patch(patch)
+        with Stage2Context(device) as ctx:
+            ctx.load(p, precision)
+            while True:
+                st = ctx.step()
+                res = ctx.download()
+                write_pm1(patch_dir / f"pm1_iter_{res['i_loop']:02d}.mat", res)
+                if st["stop"]:
+                    break
     write_pm1(patch_dir / "pm1.mat", res)
     return f"Stage 2 computed coherence for {res['K_ps'].size} candidates in {res['i_loop']} iterations using the cuda backend"
