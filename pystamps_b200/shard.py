@@ -8,7 +8,9 @@ relative order, so each cell's rows are binned in the reference's order. One
 gamma iteration is
 
     ps2_shard_bin      the rank's rows into its copy of the grid
-    sum over ranks     cells are disjoint, so the sum is the patch grid exactly
+    halo exchange      each rank receives, from the ranks owning them, the
+                       cells its CLAP windows read (cells are disjoint, so a
+                       copy is the patch grid exactly)
     ps2_shard_filter   CLAP of the windows that meet the rank's rows of cells,
                        overlap-add of its own cells
     ps2_shard_fit      topofit of the rank's rows -> histogram, sum of squared
@@ -21,8 +23,8 @@ Per-PS results are those of one context over the whole patch; the convergence
 RMS adds rank totals and can differ from it in the last bits.
 
 run_sharded(prep, group) runs one rank under torch.distributed (NCCL for CUDA
-tensors; the exchanges are one all-reduce of the grid and one of 102 doubles per
-iteration). run_sharded_local(prep, n) runs n ranks as n contexts of one
+tensors; per iteration a halo exchange of the grid cells each rank's CLAP
+reads, point to point, and one all-reduce of 102 doubles). run_sharded_local(prep, n) runs n ranks as n contexts of one
 process, the sums taken in rank order, the same arithmetic without a process
 group.
 """
@@ -78,6 +80,30 @@ def shard_patch(p: PreparedPatch, lo: int, hi: int) -> tuple[PreparedPatch, np.n
         grid_ij=np.ascontiguousarray(p.grid_ij[rows]), grid_lin=np.ascontiguousarray(gl[rows]),
         weight0=np.ascontiguousarray(p.weight0[rows]))
     return sub, rows
+
+
+def needed_cells(lo: int, hi: int, n_i: int, n_j: int, n_win: int) -> tuple[int, int]:
+    """Cells [c0, c1) whose binned values the CLAP of a rank owning cells
+    [lo, hi) reads: every window that meets the rank's rows of cells spans
+    n_win rows, so the rows from n_win - 1 above its first row to n_win - 1
+    below its last (clipped to the grid) cover them all."""
+    a, b = lo // n_j, (hi - 1) // n_j
+    r0, r1 = max(0, a - n_win + 1), min(n_i - 1, b + n_win - 1)
+    return r0 * n_j, (r1 + 1) * n_j
+
+
+def halo_plan(ranges: Sequence[tuple[int, int]], n_i: int, n_j: int, n_win: int) -> list[tuple[int, int, int, int]]:
+    """(src, dst, c0, c1) for every ordered pair of ranks: the cells of src's
+    range that dst reads. Cells are disjoint between ranks, so dst's grid
+    after receiving these slices holds the patch grid on every cell it reads."""
+    need = [needed_cells(lo, hi, n_i, n_j, n_win) for lo, hi in ranges]
+    plan = []
+    for q, (lo, hi) in enumerate(ranges):
+        for r, (n0, n1) in enumerate(need):
+            c0, c1 = max(lo, n0), min(hi, n1)
+            if q != r and c0 < c1:
+                plan.append((q, r, c0, c1))
+    return plan
 
 
 class ShardRank:
@@ -137,9 +163,9 @@ def iterate_shards(ranks: Sequence, sum_grids: Callable, sum_stats: Callable, n_
     the bound of ps2_run_to_convergence."""
     last = None
     for _ in range(max(int(max_iterations), 1) + 1):
-        grid = sum_grids([r.bin() for r in ranks])
-        for r in ranks:
-            r.filter(grid)
+        grids = sum_grids([r.bin() for r in ranks])
+        for r, g in zip(ranks, grids):
+            r.filter(g)
         stats = sum_stats([r.fit() for r in ranks])
         its = [r.finalize(stats, n_total) for r in ranks]
         last = its[0]
@@ -151,20 +177,28 @@ def iterate_shards(ranks: Sequence, sum_grids: Callable, sum_stats: Callable, n_
 
 
 def run_sharded_local(p: PreparedPatch, n_shards: int, *, device: int = 0, precision: str = "fp32",
-                      keys=("K_ps", "C_ps", "coh_ps", "N_opt")) -> dict:
+                      keys=("K_ps", "C_ps", "coh_ps", "N_opt"), exchange: str = "halo") -> dict:
     """All shards of a patch as contexts of this process on one GPU (ranks
-    emulated, sums in rank order on the device). Returns the per-PS keys in
-    the whole patch's row order, ph_grid if asked, and the last statistics."""
+    emulated: the halo slices copied between the ranks' grids, or the grids
+    summed in rank order). Returns the per-PS keys in the whole patch's row
+    order, ph_grid if asked, and the last statistics."""
     import torch
 
-    ranks = [ShardRank(p, lo, hi, device=device, precision=precision)
-             for lo, hi in split_cells(p.grid_lin, p.n_i * p.n_j, n_shards)]
+    ranges = split_cells(p.grid_lin, p.n_i * p.n_j, n_shards)
+    ranks = [ShardRank(p, lo, hi, device=device, precision=precision) for lo, hi in ranges]
+    plan = halo_plan(ranges, p.n_i, p.n_j, p.clap_window)
     try:
         def sum_grids(gs):
+            if exchange == "halo":
+                w = gs[0].numel() // (p.n_i * p.n_j)
+                views = [g.view(-1, w) for g in gs]
+                for q, r, c0, c1 in plan:
+                    views[r][c0:c1].copy_(views[q][c0:c1])
+                return gs
             acc = torch.zeros_like(gs[0])
             for g in gs:
                 acc += g
-            return acc
+            return [acc] * len(gs)
 
         def sum_stats(ss):
             acc = np.zeros(SHARD_STATS)
@@ -180,17 +214,28 @@ def run_sharded_local(p: PreparedPatch, n_shards: int, *, device: int = 0, preci
 
 
 def run_sharded(p: PreparedPatch, *, group=None, device: int | None = None, precision: str = "fp32",
-                keys=("K_ps", "C_ps", "coh_ps", "N_opt"), rank_factory: Callable | None = None) -> dict:
+                keys=("K_ps", "C_ps", "coh_ps", "N_opt"), rank_factory: Callable | None = None,
+                exchange: str = "halo") -> dict:
     """This process's shard of a patch under torch.distributed (one rank per
     GPU; every rank passes the whole PreparedPatch and takes shard `rank` of
     `world`). Returns this rank's rows ("rows": their indices in the patch),
     its per-PS keys and the last statistics (the same on every rank).
+    exchange "halo": each rank sends the other ranks only the cells of its
+    range their CLAP windows read (halo_plan; point-to-point, at the
+    full-scale shape about 23 of 256 cell rows per neighbour instead of the
+    whole 78.6 MB grid); "allreduce": the grid summed over all ranks.
     rank_factory(p, lo, hi) replaces the GPU shard (host tests of the loop)."""
     import torch
     import torch.distributed as dist
 
     rank, world = dist.get_rank(group), dist.get_world_size(group)
-    lo, hi = split_cells(p.grid_lin, p.n_i * p.n_j, world)[rank]
+    ranges = split_cells(p.grid_lin, p.n_i * p.n_j, world)
+    lo, hi = ranges[rank]
+    plan = halo_plan(ranges, p.n_i, p.n_j, p.clap_window)
+
+    def peer(r):
+        return r if group is None else dist.get_global_rank(group, r)
+
     if rank_factory is None:
         dev = torch.cuda.current_device() if device is None else int(device)
         r = ShardRank(p, lo, hi, device=dev, precision=precision)
@@ -198,14 +243,29 @@ def run_sharded(p: PreparedPatch, *, group=None, device: int | None = None, prec
         r = rank_factory(p, lo, hi)
     try:
         def sum_grids(gs):
-            dist.all_reduce(gs[0], op=dist.ReduceOp.SUM, group=group)
-            return gs[0]
+            if exchange != "halo":
+                dist.all_reduce(gs[0], op=dist.ReduceOp.SUM, group=group)
+                return gs
+            g = gs[0].view(-1, gs[0].numel() // (p.n_i * p.n_j))
+            ops = []
+            for q, dst, c0, c1 in plan:
+                if q == rank:
+                    ops.append(dist.P2POp(dist.isend, g[c0:c1], peer(dst), group))
+                elif dst == rank:
+                    ops.append(dist.P2POp(dist.irecv, g[c0:c1], peer(q), group))
+            if ops:
+                for req in dist.batch_isend_irecv(ops):
+                    req.wait()
+            return gs
 
         def sum_stats(ss):
             t = torch.from_numpy(np.ascontiguousarray(ss[0], dtype=np.float64)).to(r.grid.device)
             dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
             return t.cpu().numpy()
 
+        # every rank joins one collective first (the communicator then exists
+        # before the first point-to-point batch)
+        dist.barrier(group=group)
         last = iterate_shards([r], sum_grids, sum_stats, p.n_ps, p.gamma_max_iterations)
         out = r.download(keys)
         out["rows"] = r.rows

@@ -77,6 +77,9 @@ def test_shard_patch_keeps_rows_in_order(row_invariant):
     np.testing.assert_array_equal(np.sort(np.concatenate(seen)), np.arange(p.n_ps))
 
 
+EXCHANGE = "halo"
+
+
 class HostShard:
     """Stand-in for ShardRank on CPU: the grid holds, per cell, the sum of its
     rows' weight0 plus the iteration; statistics are the rows' counts per
@@ -104,7 +107,10 @@ class HostShard:
         whole = np.zeros(self.p.n_i * self.p.n_j)
         np.add.at(whole, self.p.grid_lin, self.p.weight0)
         whole += self.it
-        self.grids_ok.append(bool(np.allclose(grid.numpy(), whole, rtol=0, atol=1e-12)))
+        c0, c1 = shard.needed_cells(self.lo, self.hi, self.p.n_i, self.p.n_j, self.p.clap_window)
+        if EXCHANGE == "allreduce":
+            c0, c1 = 0, whole.size
+        self.grids_ok.append(bool(np.allclose(grid.numpy()[c0:c1], whole[c0:c1], rtol=0, atol=1e-12)))
 
     def fit(self):
         st = np.zeros(shard.SHARD_STATS)
@@ -132,40 +138,77 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _rank_main(rank, world, port, q):
+def _rank_main(rank, world, port, q, exchange="halo", n_i=12):
     import torch.distributed as dist
 
+    global EXCHANGE
+    EXCHANGE = exchange
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        p = _fake_prepared(seed=3)
-        out = shard.run_sharded(p, rank_factory=lambda pp, lo, hi: HostShard(pp, lo, hi))
+        p = _fake_prepared(seed=3, n_i=n_i)
+        out = shard.run_sharded(p, rank_factory=lambda pp, lo, hi: HostShard(pp, lo, hi), exchange=exchange)
         q.put((rank, out["rows"].tolist(), out["K_ps"].tolist(), out["grids_ok"], out["stats"]))
     finally:
         dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_exchange_grid_and_statistics():
+@pytest.mark.parametrize("exchange,world,n_i", [("halo", 2, 12), ("allreduce", 2, 12), ("halo", 3, 80)])
+def test_gloo_ranks_exchange_grid_and_statistics(exchange, world, n_i):
+    """Two or three gloo ranks: every rank receives the patch grid on every
+    cell its CLAP reads (the halo) or the whole summed grid, and all stop on
+    the summed statistics. With 80 rows of cells and a 32-cell window the
+    halo of a middle rank reaches both neighbours."""
     import multiprocessing as mp
 
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, q, exchange, n_i)) for r in range(world)]
     for pr in procs:
         pr.start()
-    got = sorted([q.get(timeout=300) for _ in range(2)])
+    got = sorted([q.get(timeout=300) for _ in range(world)])
     for pr in procs:
         pr.join(timeout=120)
         assert pr.exitcode == 0
-    p = _fake_prepared(seed=3)
+    p = _fake_prepared(seed=3, n_i=n_i)
     rows = np.concatenate([np.array(g[1]) for g in got])
     np.testing.assert_array_equal(np.sort(rows), np.arange(p.n_ps))
     for _, r, k, ok, _st in got:
         np.testing.assert_array_equal(np.array(k), p.weight0[np.array(r)] * 2.0)
         assert ok and all(ok)  # every rank received the whole grid every iteration
     # the stop rule came from the summed statistics: sum(rows)/(it+1)/n < 0.3 first at it = 3
-    assert got[0][4] == got[1][4]
+    assert all(g[4] == got[0][4] for g in got)
     assert got[0][4]["i_loop"] == 4 and got[0][4]["stop"] == 1
     assert len(got[0][3]) == 4
+
+
+def test_halo_plan_covers_every_window():
+    """Each rank's needed rows contain every CLAP window that meets its rows
+    (windows at stride n_win/4 with the reference's shifted edge windows,
+    native_stage2.rs:957-995), and the plan delivers exactly the needed cells
+    owned by other ranks."""
+    n_i, n_j, nw = 70, 9, 24
+    rng = np.random.default_rng(1)
+    gl = rng.integers(0, n_i * n_j, 5000)
+    ranges = shard.split_cells(gl, n_i * n_j, 5)
+    inc = nw // 4
+    wins = []
+    for ix in range((n_i + inc - 1) // inc - 3):
+        i1 = ix * inc
+        wins.append(min(i1, n_i - nw))
+    plan = shard.halo_plan(ranges, n_i, n_j, nw)
+    for r, (lo, hi) in enumerate(ranges):
+        c0, c1 = shard.needed_cells(lo, hi, n_i, n_j, nw)
+        a, b = lo // n_j, (hi - 1) // n_j
+        for i1 in wins:
+            if i1 <= b and i1 + nw - 1 >= a:  # the window meets the rank's rows
+                assert c0 <= i1 * n_j and (i1 + nw) * n_j <= c1
+        got = np.zeros(n_i * n_j, bool)
+        got[lo:hi] = True
+        for q, dst, s0, s1 in plan:
+            if dst == r:
+                assert not got[s0:s1].any()
+                got[s0:s1] = True
+        assert got[c0:c1].all()
