@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-stage3", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="one patch split over the ranks by cell ranges (strong scaling) instead of replicas")
     return ap.parse_args()
 
 
@@ -546,6 +548,78 @@ def run_ours(args, rank: int, world: int, dist):
         print(json.dumps(line), flush=True)
 
 
+def run_shard(args, rank: int, world: int, dist):
+    """One patch over all ranks (pystamps_b200.shard): rank r owns the PS of a
+    contiguous cell range; per iteration bin -> halo exchange of the cells each
+    rank's CLAP reads -> CLAP/overlap of its cells -> topofit of its rows ->
+    all-reduce of 102 statistics -> finalize. value = N*M*K / t, t the K timed
+    iterations (barriers and a device synchronise around them, host clock, max
+    over ranks): strong scaling, the total work fixed."""
+    import torch
+
+    from pystamps_b200 import shard
+    from pystamps_b200 import stage2 as S
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    w, patch = make_workload(args.workload, 0, args.n_ps)  # the same patch on every rank
+    prep = S.prepare_patch(patch)
+    del patch
+    n, m = prep.n_ps, prep.n_ifg
+    T = 2 * math.ceil(8 * prep.n_trial_wraps) + 1
+    ranges = shard.split_cells(prep.grid_lin, prep.n_i * prep.n_j, world)
+    lo, hi = ranges[rank]
+    plan = shard.halo_plan(ranges, prep.n_i, prep.n_j, prep.clap_window)
+    r = shard.ShardRank(prep, lo, hi, device=dev)
+    halo_bytes = sum((c1 - c0) for q, dst, c0, c1 in plan if q == rank) * (r.grid.numel() // (prep.n_i * prep.n_j)) \
+        * r.grid.element_size()
+
+    def one_iteration():
+        g = r.bin()
+        if dist is not None:
+            shard.halo_exchange(g, plan, rank, prep.n_i * prep.n_j)
+        r.filter(g)
+        st = r.fit()
+        if dist is not None:
+            t = torch.from_numpy(st).to(g.device)
+            dist.all_reduce(t, op=dist.ReduceOp.SUM)
+            st = t.cpu().numpy()
+        return r.finalize(st, n)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    barrier()
+    for _ in range(max(args.warmup, 1)):
+        one_iteration()
+    barrier()
+    clk = ClockSampler(dev)
+    clk.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        one_iteration()
+    barrier()
+    t = time.perf_counter() - t0
+    clocks = clk.stop()
+    if dist is not None:
+        tt = torch.tensor([t], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    r.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": n * m * args.steps / t, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded generator pystamps_b200.synth)",
+                "config": workload_config(w, n, m, prep.n_i, prep.n_j, T),
+                "parallelism": f"shard x{world} (cell ranges, halo exchange)", "clocks": clocks,
+                "halo_bytes_rank0_per_iteration": int(halo_bytes), "cells_rank0": [lo, hi],
+                "timing": "host clock around K synchronous shard iterations, barriers on both sides"}
+        print(json.dumps(line), flush=True)
+
+
 def run_batched(args, rank: int, world: int, dist):
     """The uneven multi-patch workload: 64 patches, PS log-uniform in 5k-400k,
     30-120 interferograms, LPT-assigned to ranks. Every patch of the rank is
@@ -671,6 +745,8 @@ def main():
             run_reference(args, rank, world)
         elif args.workload == "C":
             run_batched(args, rank, world, dist)
+        elif args.shard:
+            run_shard(args, rank, world, dist)
         else:
             run_ours(args, rank, world, dist)
     finally:

@@ -106,6 +106,25 @@ def halo_plan(ranges: Sequence[tuple[int, int]], n_i: int, n_j: int, n_win: int)
     return plan
 
 
+def halo_exchange(grid, plan, rank: int, n_cells: int, group=None) -> None:
+    """This rank's part of one halo exchange under torch.distributed: send
+    the planned slices of its own cells, receive the slices it reads, in place
+    in the flat grid buffer (n_cells rows of equal width)."""
+    import torch.distributed as dist
+
+    g = grid.view(-1, grid.numel() // n_cells)
+    peer = (lambda r: r) if group is None else (lambda r: dist.get_global_rank(group, r))
+    ops = []
+    for q, dst, c0, c1 in plan:
+        if q == rank:
+            ops.append(dist.P2POp(dist.isend, g[c0:c1], peer(dst), group))
+        elif dst == rank:
+            ops.append(dist.P2POp(dist.irecv, g[c0:c1], peer(q), group))
+    if ops:
+        for req in dist.batch_isend_irecv(ops):
+            req.wait()
+
+
 class ShardRank:
     """One rank's rows of a patch on one GPU, with the four shard calls."""
 
@@ -233,9 +252,6 @@ def run_sharded(p: PreparedPatch, *, group=None, device: int | None = None, prec
     lo, hi = ranges[rank]
     plan = halo_plan(ranges, p.n_i, p.n_j, p.clap_window)
 
-    def peer(r):
-        return r if group is None else dist.get_global_rank(group, r)
-
     if rank_factory is None:
         dev = torch.cuda.current_device() if device is None else int(device)
         r = ShardRank(p, lo, hi, device=dev, precision=precision)
@@ -246,16 +262,7 @@ def run_sharded(p: PreparedPatch, *, group=None, device: int | None = None, prec
             if exchange != "halo":
                 dist.all_reduce(gs[0], op=dist.ReduceOp.SUM, group=group)
                 return gs
-            g = gs[0].view(-1, gs[0].numel() // (p.n_i * p.n_j))
-            ops = []
-            for q, dst, c0, c1 in plan:
-                if q == rank:
-                    ops.append(dist.P2POp(dist.isend, g[c0:c1], peer(dst), group))
-                elif dst == rank:
-                    ops.append(dist.P2POp(dist.irecv, g[c0:c1], peer(q), group))
-            if ops:
-                for req in dist.batch_isend_irecv(ops):
-                    req.wait()
+            halo_exchange(gs[0], plan, rank, p.n_i * p.n_j, group)
             return gs
 
         def sum_stats(ss):
