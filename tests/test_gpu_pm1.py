@@ -13,7 +13,9 @@ the same patch:
   shapes and dtypes exactly;
 * values within the per-key tolerances of artifact_tolerances.json:45-72
   (f64: atol 1e-6, rtol 1e-8; complex64 / f32: atol 1e-4, rtol 1e-5; grid_ij,
-  grid_size, i_loop, step_number exact), except:
+  grid_size, i_loop, step_number exact; C_ps, the angle of a sum of unit
+  phasors that both implementations form in f32 in different orders, within
+  1e-6 + 4 * 2^-24 / coh_ps), except:
   - D1 (peak rule): the Python driver keeps every local maximum within 2e-4
     of the best trial and refines each (ported.py:2433-2478), the native driver
     the first argmax (native_stage2.rs:1253), which this library follows. Rows
@@ -110,18 +112,31 @@ def test_pm1_round_trip_matches_reference_pm1(cuda_lib, golden, oracle, tmp_path
     print(f"pm1 round trip: {int(multi.sum())} of {multi.size} rows have several near-max candidates (D1)")
     assert multi.mean() < 0.05
     tol = {True: (1e-6, 1e-8), False: (1e-4, 1e-5)}
+    bad = []
     for k in REQUIRED:
         if k in ("Nr", "Nr_max_nz_ix"):  # D4, checked below
             continue
         a, b = np.asarray(pm[k]), np.asarray(d["pm_" + k])
         if k in EXACT:
-            np.testing.assert_array_equal(a, b, err_msg=k)
+            if not np.array_equal(a, b):
+                bad.append((k, "not equal"))
             continue
         atol, rtol = tol[k in F64]
         if k in PEAK_RULE_KEYS:
             a, b = a[~multi], b[~multi]
-        ok = np.isclose(a, b, atol=atol, rtol=rtol, equal_nan=True)
-        assert ok.all(), (k, int((~ok).sum()), float(np.nanmax(np.abs(a - b))))
+        if k == "C_ps":
+            # C = arg of the sum of the M residual phasors, computed in f32 by
+            # both implementations in different summation orders: its error
+            # is ~ M eps / |sum| = eps / coh, so the bound grows where the
+            # coherence is low (4 M 2^-24 / (M coh) on top of the 1e-6)
+            coh = np.asarray(d["pm_coh_ps"])[~multi]
+            dc = np.abs(np.angle(np.exp(1j * (a - b))))
+            ok = (dc <= atol + 4 * 2.0 ** -24 / np.maximum(coh, 1e-3)) | (np.isnan(a) & np.isnan(b))
+        else:
+            ok = np.isclose(a, b, atol=atol, rtol=rtol, equal_nan=True)
+        if not ok.all():
+            bad.append((k, int((~ok).sum()), float(np.nanmax(np.abs(a - b)))))
+    assert not bad, bad
     # D4: Nr is the native driver's histogram (the oracle's restatement, exact)
     prep = S.prepare_patch(S.load_patch_dir(patch), nr=np.ones(100), nr_max_nz_ix=1.0)
     nr, mx = oracle.random_hist(prep.bperp_nm, prep.n_trial_wraps)
