@@ -14,8 +14,8 @@ the same patch:
 * values within the per-key tolerances of artifact_tolerances.json:45-72
   (f64: atol 1e-6, rtol 1e-8; complex64 / f32: atol 1e-4, rtol 1e-5; grid_ij,
   grid_size, i_loop, step_number exact; C_ps, the angle of a sum of unit
-  phasors that both implementations form in f32 in different orders, within
-  1e-6 + 4 * 2^-24 / coh_ps), except:
+  phasors whose inputs differ by ~1e-6 between the implementations, within
+  1e-6 + 2e-6 / coh_ps), except:
   - D1 (peak rule): the Python driver keeps every local maximum within 2e-4
     of the best trial and refines each (ported.py:2433-2478), the native driver
     the first argmax (native_stage2.rs:1253), which this library follows. Rows
@@ -125,13 +125,14 @@ def test_pm1_round_trip_matches_reference_pm1(cuda_lib, golden, oracle, tmp_path
         if k in PEAK_RULE_KEYS:
             a, b = a[~multi], b[~multi]
         if k == "C_ps":
-            # C = arg of the sum of the M residual phasors, computed in f32 by
-            # both implementations in different summation orders: its error
-            # is ~ M eps / |sum| = eps / coh, so the bound grows where the
-            # coherence is low (4 M 2^-24 / (M coh) on top of the 1e-6)
+            # C = arg of the sum of the M residual phasors. Their inputs differ
+            # by ~1e-6 between the implementations (this library's FP32 CLAP,
+            # the reference's f64 one cast to complex64; f32 sums in different
+            # orders), and an angle error is that over |sum| / M = coh, so the
+            # bound grows where the coherence is low: 1e-6 + 2e-6 / coh
             coh = np.asarray(d["pm_coh_ps"])[~multi]
             dc = np.abs(np.angle(np.exp(1j * (a - b))))
-            ok = (dc <= atol + 4 * 2.0 ** -24 / np.maximum(coh, 1e-3)) | (np.isnan(a) & np.isnan(b))
+            ok = (dc <= atol + 2e-6 / np.maximum(coh, 1e-3)) | (np.isnan(a) & np.isnan(b))
         else:
             ok = np.isclose(a, b, atol=atol, rtol=rtol, equal_nan=True)
         if not ok.all():
