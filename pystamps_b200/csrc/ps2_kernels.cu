@@ -146,25 +146,195 @@ __device__ __forceinline__ void bin_task(const BinArgs& a, const int64_t task, c
     a.bp_row_inv ? bin_task_t<R, 0, true>(a, task, lane) : bin_task_t<R, 0, false>(a, task, lane);
 }
 
+// The single-patch binning kernel: the same warp tasks and the same
+// sequential row sums as bin_task_t, with each warp's rows staged through
+// shared memory by asynchronous copies (cp.async). A warp walks its tasks'
+// rows in chunks of kBinRows and keeps kBinStages - 1 chunks in flight while it
+// sums the current one, so the phase and bperp rows stream without holding
+// them in registers. Every lane copies and reads only its own interferogram
+// column; the per-row scalars (K, w or coh) are copied by the first lanes and
+// read by all after a warp barrier.
+constexpr int kBinRows = 8;
+constexpr int kBinStages = 3;
+constexpr int kBinWarps = 4;
+
 template <typename R>
-__global__ void __launch_bounds__(256) k_bin(BinArgs a) {
-  const int lane = threadIdx.x & 31;
-  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+struct BinStage {
+  float2 ph[kBinRows][32];
+  float bp[kBinRows][32];
+  R k[kBinRows];
+  R w[kBinRows];  // mode 0: weights; mode 1: previous coherence
+};
+
+__device__ __forceinline__ void cp_async_4(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(smem))),
+               "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_8(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(smem))),
+               "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N));
+}
+template <typename R>
+__device__ __forceinline__ void cp_async_r(R* smem, const R* gmem) {
+  if constexpr (sizeof(R) == 8)
+    cp_async_8(smem, gmem);
+  else
+    cp_async_4(smem, gmem);
+}
+
+// psquare_weighting lookup (native_stage2.rs:1674-1682) of one coherence
+template <typename R>
+__device__ __forceinline__ R psquare_weight(const BinArgs& a, const R cohv) {
+  const double v = __dmul_rn(static_cast<double>(cohv), 1000.0);
+  double r = v >= 0.0 ? floor(__dadd_rn(v, 0.5)) : ceil(__dsub_rn(v, 0.5));
+  r = fmin(fmax(r, 0.0), static_cast<double>(a.lut_len - 1));
+  const int ix = isnan(r) ? 0 : static_cast<int>(r);
+  const double t = 1.0 - a.lut[ix];
+  return static_cast<R>(t * t);
+}
+
+// A position in a warp's sequence of row chunks: task, first row, rows.
+struct BinPos {
+  int64_t task;
+  int r0, nr, s1;
+};
+
+template <typename R, int MODE, bool ROWINV>
+__device__ __forceinline__ void bin_issue(const BinArgs& a, const BinPos& q, BinStage<R>& st, const int lane,
+                                          const int64_t ntask) {
+  if (q.task < ntask) {
+    const int chunk = static_cast<int>(q.task % a.nchunk);
+    const int c = chunk * 32 + lane;
+    const int64_t M = a.M;
+    const float2* ph = static_cast<const float2*>(a.ph_nm);
+    if (c < a.M) {
+      for (int i = 0; i < q.nr; ++i) {
+        const int64_t s = q.r0 + i;
+        cp_async_8(&st.ph[i][lane], ph + s * M + c);
+        if (MODE != 3 && !ROWINV) cp_async_4(&st.bp[i][lane], a.bp + s * M + c);
+      }
+    }
+    if (MODE != 3 && lane < q.nr) {
+      cp_async_r(&st.k[lane], static_cast<const R*>(a.K) + q.r0 + lane);
+      cp_async_r(&st.w[lane], static_cast<const R*>(MODE == 1 ? a.coh : a.w) + q.r0 + lane);
+    }
+  }
+  cp_async_commit();
+}
+
+template <typename R>
+__device__ __forceinline__ BinPos bin_first(const BinArgs& a, const int64_t task, const int64_t ntask) {
+  BinPos q{task, 0, 0, 0};
+  if (task < ntask) {
+    const int64_t cell = task / a.nchunk;
+    q.r0 = a.cell_start[cell];
+    q.s1 = a.cell_start[cell + 1];
+    q.nr = q.s1 - q.r0 < kBinRows ? q.s1 - q.r0 : kBinRows;
+  }
+  return q;
+}
+
+template <typename R>
+__device__ __forceinline__ BinPos bin_next(const BinArgs& a, const BinPos& q, const int64_t step, const int64_t ntask) {
+  if (q.r0 + q.nr < q.s1) {
+    BinPos n = q;
+    n.r0 = q.r0 + q.nr;
+    n.nr = n.s1 - n.r0 < kBinRows ? n.s1 - n.r0 : kBinRows;
+    return n;
+  }
+  return bin_first<R>(a, q.task + step, ntask);
+}
+
+template <typename R, int MODE, bool ROWINV>
+__device__ __forceinline__ void bin_warp_async(const BinArgs& a, BinStage<R>* stages, const int64_t first_task,
+                                               const int64_t step, const int lane) {
+  using C = typename CT<R>::C;
   const int64_t ntask = a.G * a.nchunk;
-  for (int64_t task = gw; task < ntask; task += nw) bin_task<R>(a, task, lane);
+  R* __restrict__ W = static_cast<R*>(a.w);
+  C* __restrict__ grid = static_cast<C*>(a.grid);
+  BinPos issue_pos = bin_first<R>(a, first_task, ntask);
+  BinPos cur = issue_pos;
+#pragma unroll
+  for (int p = 0; p < kBinStages - 1; ++p) {
+    bin_issue<R, MODE, ROWINV>(a, issue_pos, stages[p], lane, ntask);
+    if (issue_pos.task < ntask) issue_pos = bin_next<R>(a, issue_pos, step, ntask);
+  }
+  R ax = R(0), ay = R(0);
+  for (int64_t e = 0; cur.task < ntask; ++e) {
+    bin_issue<R, MODE, ROWINV>(a, issue_pos, stages[(e + kBinStages - 1) % kBinStages], lane, ntask);
+    if (issue_pos.task < ntask) issue_pos = bin_next<R>(a, issue_pos, step, ntask);
+    cp_async_wait<kBinStages - 1>();
+    __syncwarp();
+    const BinStage<R>& st = stages[e % kBinStages];
+    const int chunk = static_cast<int>(cur.task % a.nchunk);
+    const int c = chunk * 32 + lane;
+    const bool active = c < a.M;
+    const bool write_w = MODE == 1 && chunk == 0 && lane == 0;
+    for (int i = 0; i < cur.nr; ++i) {
+      const R wv = MODE == 3 ? R(1) : (MODE == 1 ? psquare_weight<R>(a, st.w[i]) : st.w[i]);
+      if (write_w) W[cur.r0 + i] = wv;
+      if (!active) continue;
+      const float2 v = st.ph[i][lane];
+      if (MODE == 3) {
+        ax = add_rn(ax, static_cast<R>(v.x));
+        ay = add_rn(ay, static_cast<R>(v.y));
+      } else {
+        const R bv = ROWINV ? static_cast<R>(a.bp[c]) : static_cast<R>(st.bp[i][lane]);
+        const R phs = -(bv * st.k[i]);
+        R sn, cs;
+        sincos_r(phs, &sn, &cs);
+        const C r = cmul_rn(mk(static_cast<R>(v.x), static_cast<R>(v.y)), mk(cs, sn));
+        ax = add_rn(ax, mul_rn(r.x, wv));
+        ay = add_rn(ay, mul_rn(r.y, wv));
+      }
+    }
+    __syncwarp();
+    if (cur.r0 + cur.nr >= cur.s1) {  // the task's last chunk: its cell column is complete
+      const int64_t cell = cur.task / a.nchunk;
+      if (c < a.Mp) grid[cell * a.Mp + c] = active ? mk(ax, ay) : mk(R(0), R(0));
+      ax = R(0);
+      ay = R(0);
+    }
+    cur = bin_next<R>(a, cur, step, ntask);
+  }
+  cp_async_wait<0>();
+}
+
+template <typename R>
+__global__ void __launch_bounds__(32 * kBinWarps) k_bin(BinArgs a) {
+  __shared__ BinStage<R> stages[kBinWarps][kBinStages];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t gw = static_cast<int64_t>(blockIdx.x) * kBinWarps + wib;
+  const int64_t nw = static_cast<int64_t>(gridDim.x) * kBinWarps;
+  BinStage<R>* st = stages[wib];
+  if (a.mode == 3)
+    bin_warp_async<R, 3, false>(a, st, gw, nw, lane);
+  else if (a.mode == 1)
+    a.bp_row_inv ? bin_warp_async<R, 1, true>(a, st, gw, nw, lane) : bin_warp_async<R, 1, false>(a, st, gw, nw, lane);
+  else
+    a.bp_row_inv ? bin_warp_async<R, 0, true>(a, st, gw, nw, lane) : bin_warp_async<R, 0, false>(a, st, gw, nw, lane);
 }
 
 cudaError_t launch_bin(const BinArgs& a, bool fp64, int sm_count, cudaStream_t st) {
   const int64_t warps = a.G * a.nchunk;
-  int64_t blocks = (warps + 7) / 8;
-  const int64_t cap = static_cast<int64_t>(sm_count) * 16;
+  int64_t blocks = (warps + kBinWarps - 1) / kBinWarps;
+  int per_sm = 0;
+  cudaError_t e = fp64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bin<double>, 32 * kBinWarps, 0)
+                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bin<float>, 32 * kBinWarps, 0);
+  if (e != cudaSuccess) return e;
+  if (a.blocks_per_sm > 0 && a.blocks_per_sm < per_sm) per_sm = a.blocks_per_sm;
+  const int64_t cap = static_cast<int64_t>(sm_count) * (per_sm > 0 ? per_sm : 1);
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
   if (fp64)
-    k_bin<double><<<static_cast<unsigned>(blocks), 256, 0, st>>>(a);
+    k_bin<double><<<static_cast<unsigned>(blocks), 32 * kBinWarps, 0, st>>>(a);
   else
-    k_bin<float><<<static_cast<unsigned>(blocks), 256, 0, st>>>(a);
+    k_bin<float><<<static_cast<unsigned>(blocks), 32 * kBinWarps, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -747,6 +917,7 @@ static cudaError_t launch_clap_nwin(const ClapArgs& a, const typename CT<R>::Tw&
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clap<R, NW, NWIN>, 32 * NW, sm);
   if (e != cudaSuccess) return e;
+  if (a.blocks_per_sm > 0 && a.blocks_per_sm < per_sm) per_sm = a.blocks_per_sm;
   const int64_t blocks = std::min<int64_t>(ntask, static_cast<int64_t>(sm_count) * (per_sm > 0 ? per_sm : 1));
   k_clap<R, NW, NWIN><<<static_cast<unsigned>(blocks), 32 * NW, sm, st>>>(a, tw);
   return cudaGetLastError();
@@ -758,11 +929,13 @@ static cudaError_t launch_clap_nw(const ClapArgs& a, const typename CT<R>::Tw& t
   return a.n_win == 24 ? launch_clap_nwin<R, NW, 24>(a, tw, sm_count, st) : launch_clap_nwin<R, NW, 0>(a, tw, sm_count, st);
 }
 
-// FP32: 8 warps per block (16 resident warps per SM, shared memory bound);
-// FP64: 4 (its tiles are twice the size)
+// FP32: 8 warps per block by default (16 resident warps per SM, shared memory
+// bound), 4 when the launch shape asks for it; FP64: 4 (its tiles are twice the
+// size). Every window's arithmetic is the same whatever the shape.
 cudaError_t launch_clap(const ClapArgs& a, bool fp64, const Twiddles32f& tf, const Twiddles32d& td, int sm_count,
                         cudaStream_t st) {
-  return fp64 ? launch_clap_nw<double, 4>(a, td, sm_count, st) : launch_clap_nw<float, 8>(a, tf, sm_count, st);
+  if (fp64) return launch_clap_nw<double, 4>(a, td, sm_count, st);
+  return a.nw_block == 4 ? launch_clap_nw<float, 4>(a, tf, sm_count, st) : launch_clap_nw<float, 8>(a, tf, sm_count, st);
 }
 
 // Overlap-add as a gather: cell (i, j) sums the windows that cover it, in the
@@ -836,9 +1009,10 @@ cudaError_t launch_overlap(const OverlapArgs& a, bool fp64, cudaStream_t st) {
 // Column data (psdph z_c, theta_c = bp_c/range*pi/4, e^{-j theta_c}, bp_c)
 // live in shared memory. The trial sweep evaluates
 //   S_m = sum_c z_c e^{-j theta_c m}
-// for 32 consecutive m at a time: the phasor u = z e^{-j theta m} advances by
-// one complex multiply per trial and is re-anchored with a directly computed
-// e^{-j theta m} every 16 trials; the group then reduces its 32 partial sums
+// for the trial pairs +-m, 16 magnitudes |m| at a time (sweep_trial_pairs): the
+// phasor e^{-j theta m} is anchored exactly at the first magnitude of the block
+// and advanced by a complex recurrence, two trials per packed FP32x2 value, so
+// it is re-anchored every 16 steps; the group then reduces its 32 partial sums
 // with a transposing butterfly, each lane ending with 32/L of the trials.
 
 constexpr float kQuarterPiF = 3.14159265358979323846f / 4.0f;  // Rust std::f32::consts::PI / 4.0
@@ -923,7 +1097,8 @@ struct ColumnSmem {
 };
 
 // Trials +m and -m from one rotation chain, two columns per packed FP32x2
-// instruction. For a column z = (x, y) and w = e^{-j m theta}:
+// instruction (the form of the last, odd magnitude of a sweep; the blocks of
+// 2-16 magnitudes pack two trials instead, sweep_trial_pairs). For a column z = (x, y) and w = e^{-j m theta}:
 //   z w       = (x w.x - y w.y, x w.y + y w.x)               trial +m
 //   z conj(w) = (x w.x + y w.y, y w.x - x w.y) = z e^{+j m theta}   trial -m
 // so the four sums  sum x w.x, sum x w.y, sum y w.y, sum y w.x  give both
@@ -1024,6 +1199,98 @@ __device__ __forceinline__ void sweep_pairs(const ColumnSmem& cs, const float qr
   }
 }
 
+// One block of W trial magnitudes |m| = m0 .. m0+W-1 (W even, m0 >= 1) with
+// two TRIALS per packed FP32x2 value: slot i of each accumulator holds
+// (|m| = m0+2i, m0+2i+1), so W trial pairs cost 2W accumulator registers and
+// one exact anchor per column covers all W magnitudes. Per column:
+// w(m0) = e^{-j m0 theta} exactly, w(m0+1) = w(m0) e^{-j theta}, then both
+// halves advance by e^{-2j theta} (one packed complex multiply per two
+// magnitudes). The four sums P = sum x w.x, Q = sum x w.y, R = sum y w.x,
+// U = sum y w.y give S(+m) = (P - U, Q + R) and S(-m) = (P + U, R - Q) for both
+// trials of a slot. Each lane sums its columns in column order; the group
+// joins its lanes with the transposing reduction.
+template <int W, int L>
+__device__ __forceinline__ void sweep_trial_pairs(const ColumnSmem& cs, const float qr, const int ncl, const int gl,
+                                                  const int m0, const int n_half, float& best_sq, int& best_t) {
+  constexpr int H = W / 2;
+  float2 P[H], Q[H], R[H], U[H];
+#pragma unroll
+  for (int i = 0; i < H; ++i) {
+    P[i] = make_float2(0.f, 0.f);
+    Q[i] = make_float2(0.f, 0.f);
+    R[i] = make_float2(0.f, 0.f);
+    U[i] = make_float2(0.f, 0.f);
+  }
+#pragma unroll 2
+  for (int k = 0; k < ncl; ++k) {
+    const int c = gl + L * k;
+    const float x = cs.zx[c], y = cs.zy[c], rx = cs.rx[c], ry = cs.ry[c];
+    const float2 a0 = cis_neg_anchor(cs.bp[c] * qr * static_cast<float>(m0));
+    const float a1x = fmaf(a0.x, rx, -a0.y * ry), a1y = fmaf(a0.x, ry, a0.y * rx);
+    const float r2x = fmaf(rx, rx, -ry * ry), r2y = 2.f * rx * ry;
+    float2 Wx = make_float2(a0.x, a1x), Wy = make_float2(a0.y, a1y);
+    const float2 X = make_float2(x, x), Y = make_float2(y, y);
+    const float2 Rx = make_float2(r2x, r2x), Ry = make_float2(r2y, r2y), NRy = make_float2(-r2y, -r2y);
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+      P[i] = __ffma2_rn(X, Wx, P[i]);
+      Q[i] = __ffma2_rn(X, Wy, Q[i]);
+      R[i] = __ffma2_rn(Y, Wx, R[i]);
+      U[i] = __ffma2_rn(Y, Wy, U[i]);
+      if (i + 1 < H) {
+        const float2 t = __fmul2_rn(Wy, NRy);
+        const float2 u = __fmul2_rn(Wy, Rx);
+        const float2 wx = Wx;
+        Wx = __ffma2_rn(wx, Rx, t);
+        Wy = __ffma2_rn(wx, Ry, u);
+      }
+    }
+  }
+  // slots 0..W-1: trials +m0..+m0+W-1; W..2W-1: trials -m0..-(m0+W-1)
+  float2 S[2 * W];
+#pragma unroll
+  for (int i = 0; i < H; ++i) {
+    S[2 * i] = make_float2(P[i].x - U[i].x, Q[i].x + R[i].x);
+    S[2 * i + 1] = make_float2(P[i].y - U[i].y, Q[i].y + R[i].y);
+    S[W + 2 * i] = make_float2(P[i].x + U[i].x, R[i].x - Q[i].x);
+    S[W + 2 * i + 1] = make_float2(P[i].y + U[i].y, R[i].y - Q[i].y);
+  }
+  int base;
+  const int cnt = group_transpose_reduce<2 * W, L>(S, gl, base);
+#pragma unroll
+  for (int j = 0; j < (2 * W / L > 1 ? 2 * W / L : 1); ++j) {
+    if (j < cnt) {
+      const int idx = base + j;
+      const int t = idx < W ? n_half + m0 + idx : n_half - (m0 + idx - W);
+      const float sq = S[j].x * S[j].x + S[j].y * S[j].y;
+      if (sq > best_sq || (sq == best_sq && t < best_t)) {
+        best_sq = sq;
+        best_t = t;
+      }
+    }
+  }
+}
+
+// L2 prefetch of the rows a warp reads on its next pass (the PS group s0n ..
+// s0n+G-1): the phase rows and, unless bperp is row invariant, the bperp rows,
+// one 128-byte line per lane per instruction, all inside the arrays.
+template <int G, bool ROWINV>
+__device__ __forceinline__ void prefetch_rows(const void* ph, const float* bp, const int64_t s0n, const int64_t N,
+                                              const int64_t M, const int lane) {
+  if (s0n >= N) return;
+  const int64_t s1 = s0n + G < N ? s0n + G : N;
+  const char* p0 = static_cast<const char*>(ph) + s0n * M * 8;
+  const int64_t nb = (s1 - s0n) * M * 8;
+  for (int64_t o = static_cast<int64_t>(lane) * 128; o < nb; o += 32 * 128)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p0 + o));
+  if (!ROWINV) {
+    const char* b0 = reinterpret_cast<const char*>(bp + s0n * M);
+    const int64_t nbb = (s1 - s0n) * M * 4;
+    for (int64_t o = static_cast<int64_t>(lane) * 128; o < nbb; o += 32 * 128)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(b0 + o));
+  }
+}
+
 // The work of block `vb` of a launch of `nvb` blocks over one patch: PS
 // groups s0 = (vb * 4 + warp) * G + k * nvb * 4 * G. The batched kernel runs
 // the same virtual blocks, so a patch's per-block rms partials, and with them
@@ -1060,6 +1327,8 @@ __device__ __forceinline__ void topofit_vblock_t(const TopoArgs& a, const int mp
     const int64_t s = s0 + g;
     const bool active = s < a.N;
     const int64_t cell = (active && LOOP) ? a.cell_of[s] : 0;
+    prefetch_rows<G, ROWINV>(LOOP ? static_cast<const void*>(ph_nm) : static_cast<const void*>(cpx), a.bp, s0 + step,
+                             a.N, M, lane);
     bool zero = false, nonzero = false;
     float mn = __int_as_float(0x7f800000), mx = -mn;
     // four columns per round with their global loads issued first
@@ -1143,13 +1412,18 @@ __device__ __forceinline__ void topofit_vblock_t(const TopoArgs& a, const int mp
     best_sq = s0x * s0x + s0y * s0y;
     int best_t = a.n_half;
     int m0 = 1;
-    for (; a.n_half - m0 + 1 >= 8; m0 += 8) sweep_pairs<8, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
+    for (; a.n_half - m0 + 1 >= 16; m0 += 16)
+      sweep_trial_pairs<16, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
+    if (a.n_half - m0 + 1 >= 8) {
+      sweep_trial_pairs<8, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
+      m0 += 8;
+    }
     if (a.n_half - m0 + 1 >= 4) {
-      sweep_pairs<4, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
+      sweep_trial_pairs<4, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
       m0 += 4;
     }
     if (a.n_half - m0 + 1 >= 2) {
-      sweep_pairs<2, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
+      sweep_trial_pairs<2, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
       m0 += 2;
     }
     if (a.n_half - m0 + 1 >= 1) sweep_pairs<1, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
@@ -3310,6 +3584,8 @@ cudaError_t kernel_attributes_once(size_t dynamic_smem) {
         r == cudaSuccess ? opt_in_smem(k_clap<float, 8, 0>, optin) : r,
         r == cudaSuccess ? opt_in_smem(k_clap<double, 4, 0>, optin) : r,
         r == cudaSuccess ? opt_in_smem(k_clap<float, 8, 24>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<float, 4, 0>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<float, 4, 24>, optin) : r,
         r == cudaSuccess ? opt_in_smem(k_clap<double, 4, 24>, optin) : r,
         r == cudaSuccess ? opt_in_smem(k_topofit_f32<4>, optin) : r,
         r == cudaSuccess ? opt_in_smem(k_topofit_f32<8>, optin) : r,
