@@ -38,7 +38,7 @@ EXPORTED = (
     "ps2_coherence_forward", "ps2_coherence_backward", "ps2_batch_run", "ps3_reestimate",
     "ps2_stage3_reestimate", "ps2_shard_bin", "ps2_shard_filter", "ps2_shard_fit", "ps2_shard_finalize",
     "ps2_prepare_phase", "ps2_prepare_bperp", "ps2_topofit_near_max", "ps2_histogram_with_centers",
-    "ps2_export_state", "ps2_import_state", "ps2_step",
+    "ps2_export_state", "ps2_import_state", "ps2_step", "ps2_launch_shapes",
 )
 
 

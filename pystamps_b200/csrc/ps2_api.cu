@@ -189,28 +189,37 @@ std::vector<double> window_weight_scaled(int n_win, int n_ex) {
   return out;
 }
 
-// Autotuned lanes per PS for the FP32 topofit, keyed by (n_ifg, log2 n_ps).
+// Launch shapes chosen by ps2_autotune, kept process-wide per (interferogram
+// bucket, PS bucket, precision): the FP32 topofit's lanes per PS, CLAP's warps
+// per block and resident blocks per SM, binning's resident blocks per SM
+// (0 everywhere: the built-in rules).
+struct TuneShape {
+  int lanes = 0, clap_nw = 0, clap_bps = 0, bin_bps = 0;
+};
 std::mutex g_tune_mu;
-std::vector<std::pair<int64_t, int>> g_tune_cache;
-int64_t tune_key(int64_t M, int64_t N) {
+std::vector<std::pair<int64_t, TuneShape>> g_tune_cache;
+int64_t tune_key(int64_t M, int64_t N, bool fp64) {
   int64_t lb = 0;
   while ((int64_t(1) << lb) < N) ++lb;
-  return M * 64 + lb;
+  return (((M + 7) / 8) * 64 + lb) * 2 + (fp64 ? 1 : 0);
 }
-int tune_lookup(int64_t key) {
-  std::lock_guard<std::mutex> g(g_tune_mu);
-  for (auto& kv : g_tune_cache)
-    if (kv.first == key) return kv.second;
-  return 0;
-}
-void tune_store(int64_t key, int lanes) {
+bool tune_lookup(int64_t key, TuneShape* out) {
   std::lock_guard<std::mutex> g(g_tune_mu);
   for (auto& kv : g_tune_cache)
     if (kv.first == key) {
-      kv.second = lanes;
+      *out = kv.second;
+      return true;
+    }
+  return false;
+}
+void tune_store(int64_t key, const TuneShape& v) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  for (auto& kv : g_tune_cache)
+    if (kv.first == key) {
+      kv.second = v;
       return;
     }
-  g_tune_cache.emplace_back(key, lanes);
+  g_tune_cache.emplace_back(key, v);
 }
 
 }  // namespace
@@ -255,6 +264,7 @@ struct ps2_ctx {
   bool last_run_graph = false;
   int64_t graph_body_launches = 0;
   int topo_lanes = 0;  // 0: rule from n_ifg; else chosen by ps2_autotune
+  int clap_nw = 0, clap_bps = 0, bin_bps = 0;  // launch shapes (0: built-in rules)
   int topo_blocks = 0;
   int64_t iters_done = 0;  // since load/reset
   double* h_stats = nullptr;  // pinned [8]
@@ -295,6 +305,7 @@ BinArgs bin_args(ps2_ctx* c, int mode, const void* K) {
   a.lut_len = 1001;
   a.mode = mode;
   a.grid = c->grid.p;
+  a.blocks_per_sm = c->bin_bps;
   return a;
 }
 
@@ -315,6 +326,8 @@ ClapArgs clap_args(ps2_ctx* c, const void* grid, void* win) {
   a.wscaled = c->wscaled.as<double>();
   for (int i = 0; i < 7; ++i) a.g7[i] = c->g7[i];
   a.win_out = win;
+  a.nw_block = c->clap_nw;
+  a.blocks_per_sm = c->clap_bps;
   return a;
 }
 
@@ -772,7 +785,14 @@ int ps2_load_patch(ps2_ctx* c, const ps2_patch_desc* d) {
   CK(c->hist.alloc(sizeof(int32_t) * PS2_COH_BINS));
   CK(c->n_invalid.alloc(sizeof(int32_t)));
   c->topo_blocks = topofit_grid_blocks(c->sm_count, c->fp64);
-  c->topo_lanes = tune_lookup(tune_key(c->M, c->N));
+  {
+    TuneShape ts;
+    if (!tune_lookup(tune_key(c->M, c->N, c->fp64), &ts)) ts = TuneShape{};
+    c->topo_lanes = ts.lanes;
+    c->clap_nw = ts.clap_nw;
+    c->clap_bps = ts.clap_bps;
+    c->bin_bps = ts.bin_bps;
+  }
   CK(cudaMemsetAsync(c->filt.p, 0, Cz * G * c->Mp, c->st));
   CK(c->rms_partial.alloc(sizeof(double) * c->topo_blocks));
   rc = reset_state(c);
@@ -971,41 +991,114 @@ int ps2_import_state(ps2_ctx* c, const void* buf, int64_t bytes) {
 int ps2_autotune(ps2_ctx* c, int32_t* chosen_lanes, double* ms_per_candidate) {
   if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "no patch loaded");
   CK(cudaSetDevice(c->device));
-  const int cands[4] = {4, 8, 16, 32};
-  if (c->fp64) {
-    if (chosen_lanes) *chosen_lanes = 0;
-    return PS2_OK;  // the plain FP64 kernel has a single shape
-  }
   int rc = ensure_events(c, 2);
   if (rc) return rc;
-  DevBuf kk, cc, hh;
-  CK(kk.alloc(rsz(c) * c->N));
-  CK(cc.alloc(rsz(c) * c->N));
-  CK(hh.alloc(rsz(c) * c->N));
-  int best = 0;
-  double best_ms = 1e300;
-  for (int i = 0; i < 4; ++i) {
-    TopoArgs t = topo_args(c, kk.p, cc.p, hh.p);
-    t.nopt = nullptr;
-    t.accumulate_stats = 0;
-    t.lanes = cands[i];
-    CK(launch_topofit(t, false, c->topo_blocks, c->st));  // warm-up
+  auto timed = [&](auto&& launch, double* ms_out) -> int {
+    CK(launch());  // warm-up
     CK(cudaEventRecord(c->evpool[0], c->st));
-    CK(launch_topofit(t, false, c->topo_blocks, c->st));
+    CK(launch());
     CK(cudaEventRecord(c->evpool[1], c->st));
     CK(cudaStreamSynchronize(c->st));
     float ms;
     CK(cudaEventElapsedTime(&ms, c->evpool[0], c->evpool[1]));
-    if (ms_per_candidate) ms_per_candidate[i] = ms;
-    if (ms < best_ms) {
-      best_ms = ms;
-      best = cands[i];
+    *ms_out = ms;
+    return PS2_OK;
+  };
+  TuneShape best;
+  // topofit lanes per PS (FP32; the plain FP64 kernel has a single shape),
+  // on scratch outputs so the loop state is untouched
+  if (!c->fp64) {
+    const int cands[4] = {4, 8, 16, 32};
+    DevBuf kk, cc, hh;
+    CK(kk.alloc(rsz(c) * c->N));
+    CK(cc.alloc(rsz(c) * c->N));
+    CK(hh.alloc(rsz(c) * c->N));
+    double best_ms = 1e300;
+    for (int i = 0; i < 4; ++i) {
+      TopoArgs t = topo_args(c, kk.p, cc.p, hh.p);
+      t.nopt = nullptr;
+      t.accumulate_stats = 0;
+      t.lanes = cands[i];
+      double ms = 0;
+      rc = timed([&] { return launch_topofit(t, false, c->topo_blocks, c->st); }, &ms);
+      if (rc) return rc;
+      if (ms_per_candidate) ms_per_candidate[i] = ms;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best.lanes = cands[i];
+      }
+    }
+  } else if (chosen_lanes) {
+    *chosen_lanes = 0;
+  }
+  // CLAP warps per block and resident blocks per SM, into the window scratch
+  // (the loop recomputes it every iteration)
+  {
+    const int nws[2] = {8, 4}, bpss[2] = {0, 1};
+    double best_ms = 1e300;
+    for (int a = 0; a < (c->fp64 ? 1 : 2); ++a)
+      for (int b = 0; b < 2; ++b) {
+        ClapArgs ca = clap_args(c, c->grid.p, c->win.p);
+        ca.nw_block = c->fp64 ? 0 : nws[a];
+        ca.blocks_per_sm = bpss[b];
+        double ms = 0;
+        rc = timed([&] { return launch_clap(ca, c->fp64, c->twf, c->twd, c->sm_count, c->st); }, &ms);
+        if (rc) return rc;
+        if (ms < best_ms) {
+          best_ms = ms;
+          best.clap_nw = ca.nw_block;
+          best.clap_bps = bpss[b];
+        }
+      }
+  }
+  // binning resident blocks per SM, mode 0 into a scratch grid
+  {
+    DevBuf g2;
+    CK(g2.alloc(csz(c) * c->G * c->Mp));
+    const int bpss[3] = {0, 4, 2};
+    double best_ms = 1e300;
+    for (int b = 0; b < 3; ++b) {
+      BinArgs ba = bin_args(c, 0, c->K[0].p);
+      ba.grid = g2.p;
+      ba.blocks_per_sm = bpss[b];
+      double ms = 0;
+      rc = timed([&] { return launch_bin(ba, c->fp64, c->sm_count, c->st); }, &ms);
+      if (rc) return rc;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best.bin_bps = bpss[b];
+      }
     }
   }
-  c->topo_lanes = best;
-  drop_loop_graph(c);  // the captured loop holds the previous shape
-  tune_store(tune_key(c->M, c->N), best);
-  if (chosen_lanes) *chosen_lanes = best;
+  c->topo_lanes = best.lanes;
+  c->clap_nw = best.clap_nw;
+  c->clap_bps = best.clap_bps;
+  c->bin_bps = best.bin_bps;
+  drop_loop_graph(c);  // the captured loop holds the previous shapes
+  tune_store(tune_key(c->M, c->N, c->fp64), best);
+  if (chosen_lanes && !c->fp64) *chosen_lanes = best.lanes;
+  return PS2_OK;
+}
+
+int ps2_launch_shapes(ps2_ctx* c, int32_t* get, const int32_t* set) {
+  if (!c || !c->loaded) return set_err(PS2_ERR_NOT_LOADED, "no patch loaded");
+  if (get) {
+    get[0] = c->topo_lanes;
+    get[1] = c->clap_nw;
+    get[2] = c->clap_bps;
+    get[3] = c->bin_bps;
+  }
+  if (set) {
+    if (!(set[0] == 0 || set[0] == 4 || set[0] == 8 || set[0] == 16 || set[0] == 32) ||
+        !(set[1] == 0 || set[1] == 4 || set[1] == 8) || set[2] < 0 || set[3] < 0)
+      return set_err(PS2_ERR_INVALID_ARG, "ps2_launch_shapes: lanes 0/4/8/16/32, CLAP warps 0/4/8, blocks per SM >= 0");
+    if (c->fp64 && set[1] == 8) return set_err(PS2_ERR_UNSUPPORTED, "ps2_launch_shapes: FP64 CLAP runs 4 warps");
+    c->topo_lanes = set[0];
+    c->clap_nw = set[1];
+    c->clap_bps = set[2];
+    c->bin_bps = set[3];
+    drop_loop_graph(c);
+  }
   return PS2_OK;
 }
 

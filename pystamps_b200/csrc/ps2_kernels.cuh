@@ -32,6 +32,7 @@ struct BinArgs {
   int lut_len;
   int mode;              // 0: w given; 1: w = (1 - lut[round(1000 coh)])^2
   void* grid;            // complex [G, Mp]
+  int blocks_per_sm;     // launch shape: resident blocks per SM (0: as many as fit)
 };
 
 // ------------------------------------------------------------------ CLAP --
@@ -47,6 +48,8 @@ struct ClapArgs {
   double g7[7];            // 7-tap Gaussian of the |H| smoothing
   void* win_out;           // complex [W, n_win*n_win, Mp]
   int64_t w_lo, w_n;       // windows w_lo .. w_lo + w_n - 1 (w_n = 0: all windows)
+  int nw_block;            // launch shape: warps (interferograms) per block, 4 or 8 (0: 8 in FP32, 4 in FP64)
+  int blocks_per_sm;       // launch shape: resident blocks per SM (0: as many as fit)
 };
 
 struct OverlapArgs {

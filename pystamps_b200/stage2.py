@@ -346,7 +346,9 @@ class Stage2Context:
         self._keep = []
 
     def autotune(self) -> tuple[int, list[float]]:
-        """Pick the fastest topofit shape (lanes per PS) for this patch."""
+        """Pick the fastest launch shapes for this patch (ps2_autotune: topofit
+        lanes per PS, CLAP warps and blocks per SM, binning blocks per SM);
+        returns the topofit lanes and the time of each lane candidate."""
         lanes = ctypes.c_int32(0)
         ms = (ctypes.c_double * 4)()
         check(self._lib.ps2_autotune(self._ctx, ctypes.byref(lanes), ms))
@@ -354,6 +356,14 @@ class Stage2Context:
 
     def reset(self) -> None:
         check(self._lib.ps2_reset(self._ctx))
+
+    def launch_shapes(self, set_to=None) -> list[int]:
+        """[topofit lanes, CLAP warps per block, CLAP blocks per SM, binning
+        blocks per SM] (ps2_launch_shapes; 0 = built-in rule); set_to pins them."""
+        get = (ctypes.c_int32 * 4)()
+        st = None if set_to is None else (ctypes.c_int32 * 4)(*[int(v) for v in set_to])
+        check(self._lib.ps2_launch_shapes(self._ctx, get, st))
+        return list(get) if set_to is None else [int(v) for v in set_to]
 
     def step(self) -> dict:
         """One iteration under the stop rule (ps2_step)."""
