@@ -36,9 +36,10 @@ Fixtures (all seeded):
                          stage2_topofit_row_invariant,
                          stage2_topofit_coh_row_invariant and stage2_histogram
                          (pystamps/kernels/accelerated.py:410-509) with the
-                         python provider, on the reference's own random case and
-                         on seeded 400 x 40 rows with zero columns, in complex64
-                         and complex128.
+                         python provider, on the reference's own random case, on
+                         seeded 400 x 40 rows with zero columns and on 160 rows
+                         with two near-equal peaks (several near-max
+                         candidates), in complex64 and complex128.
 * stage3_select.npz   -- ported.stage3_select_ps after the Python stage 2 on a
                          10,000 PS x 8 ifg patch over a 40 x 40 grid: the
                          select1.mat variables (ix, keep_ix, ph_patch2,
@@ -314,7 +315,28 @@ def make_registry(ported) -> None:
     out["t1_cpx"] = cpx.astype(np.complex128)
     out["t1_bp"] = bp.astype(np.float64)
     out["t1_ntw"] = np.float64(4.94)
-    for name in ("t0", "t1"):
+    # rows with two peaks of nearly equal height: antisymmetric bperp per row
+    # and two opposite phase ramps, the second weaker by up to 1e-4, so the
+    # trials +m and -m are local maxima within 2e-4 of each other (both refined,
+    # the better one kept); the last rows put the ramps at the end trials
+    # (-n, +n), the case the reference settles by the coarse coherence
+    rng = np.random.default_rng(78)
+    n, m = 160, 40
+    half = np.sort(rng.uniform(5.0, 300.0, m // 2))
+    b = np.concatenate([-half[::-1], half])
+    bp = (1.0 + 0.02 * rng.uniform(-0.5, 0.5, n))[:, None] * b[None, :]
+    q = (np.pi / 4) / (bp.max(axis=1) - bp.min(axis=1))
+    n_half = int(np.ceil(8 * 4.94))
+    mstar = rng.integers(3, 30, n) + rng.uniform(-0.2, 0.2, n)
+    mstar[-8:] = n_half
+    a2 = 1.0 - rng.uniform(1e-6, 1e-4, n)
+    ph = (q * mstar)[:, None] * bp
+    cpx = np.exp(1j * ph) + a2[:, None] * np.exp(-1j * ph)
+    cpx += 1e-7 * (rng.standard_normal((n, m)) + 1j * rng.standard_normal((n, m)))
+    out["t2_cpx"] = cpx.astype(np.complex128)
+    out["t2_bp"] = bp.astype(np.float64)
+    out["t2_ntw"] = np.float64(4.94)
+    for name in ("t0", "t1", "t2"):
         c128, b64, ntw = out[name + "_cpx"], out[name + "_bp"], float(out[name + "_ntw"])
         brow = out.get(name + "_bprow", np.tile(b64[0], (b64.shape[0], 1)))
         for prec, c, b, br in (("d", c128, b64, brow), ("s", c128.astype(np.complex64), b64.astype(np.float32),

@@ -20,7 +20,9 @@ the same patch:
     of the best trial and refines each (ported.py:2433-2478), the native driver
     the first argmax (native_stage2.rs:1253), which this library follows. Rows
     with more than one such candidate are counted and left out of K_ps, C_ps,
-    coh_ps, coh_ps_save and ph_res;
+    coh_ps, coh_ps_save and ph_res, and gamma_change_save (the rms of the
+    first iteration's coherence) is compared with the reference's rms taken
+    with this library's coherence on those rows;
   - D4 (random-phase histogram): Nr and Nr_max_nz_ix are the native driver's
     (argmax-only, FP64, native_stage2.rs:1310-1512), so they are checked against
     the oracle's restatement of that rule, bit for bit, not against the Python
@@ -124,6 +126,11 @@ def test_pm1_round_trip_matches_reference_pm1(cuda_lib, golden, oracle, tmp_path
         atol, rtol = tol[k in F64]
         if k in PEAK_RULE_KEYS:
             a, b = a[~multi], b[~multi]
+        if k == "gamma_change_save":
+            # the rms of the first iteration's coherence over every row: the
+            # reference's with this library's coherence on the D1 rows
+            mix = np.where(multi, np.asarray(pm["coh_ps"]).reshape(-1), np.asarray(d["pm_coh_ps"]).reshape(-1))
+            b = np.sqrt(np.mean(mix * mix)).reshape(b.shape)
         if k == "C_ps":
             # C = arg of the sum of the M residual phasors. Their inputs differ
             # by ~1e-6 between the implementations (this library's FP32 CLAP,

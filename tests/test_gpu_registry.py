@@ -7,10 +7,11 @@ Topofit follows the registry's rule (ported._ps_topofit_single): zero columns
 skipped, near-max candidates within 2e-4, each refined, the reference's
 choice. complex128 inputs run the FP64 kernel (the reference's double path):
 K, C and coh within 1e-9 on every row (the reference's own native-vs-python
-test allows 1e-10 on its 6 x 5 case, checked here at that bound). complex64
-inputs run the FP32 kernel: K within 1e-4 relative and coh within 1e-5 on at
-least 99 % of the rows (the others are rows whose candidate set is decided by
-rounding). The histogram is exact.
+test allows 1e-10 on its 6 x 5 case, checked here at that bound), including
+160 rows built with two near-equal peaks so that several candidates are
+refined. complex64 inputs run the FP32 kernel: K within 1e-4 relative and coh
+within 1e-5 on at least 99 % of the rows (95 % of the near-tie rows: the
+others are rows whose choice f32 rounding decides). The histogram is exact.
 """
 import numpy as np
 import pytest
@@ -39,8 +40,11 @@ def _brow(reg, case):
     return reg[case + "_bprow"] if case + "_bprow" in reg else np.tile(bp[0], (bp.shape[0], 1))
 
 
-@pytest.mark.parametrize("case", ["t0", "t1"])
+@pytest.mark.parametrize("case", ["t0", "t1", "t2"])
 def test_topofit_generic_and_row_invariant_fp64_match_python_provider(K, reg, case):
+    """t2: rows with two near-equal peaks (trials +m and -m within 2e-4), each
+    refined and the better kept, and rows whose two candidates are the end
+    trials (kept by the coarse coherence)."""
     cpx, bp, ntw = reg[case + "_cpx"], reg[case + "_bp"], float(reg[case + "_ntw"])
     atol = 1e-10 if case == "t0" else 1e-9
     for kind, b in (("gen", bp), ("row", _brow(reg, case))):
@@ -55,7 +59,7 @@ def test_topofit_generic_and_row_invariant_fp64_match_python_provider(K, reg, ca
 
 
 def test_topofit_coh_row_invariant_matches_python_provider(K, reg):
-    for case in ("t0", "t1"):
+    for case in ("t0", "t1", "t2"):
         cpx, ntw = reg[case + "_cpx"], float(reg[case + "_ntw"])
         ref = reg[case + "_cohrow"]
         got = K.run_stage2_topofit_coh_row_invariant_kernel(cpx, _brow(reg, case), ntw)
@@ -66,25 +70,28 @@ def test_topofit_coh_row_invariant_matches_python_provider(K, reg):
         assert np.all(_same(got[full], ref[full], 1e-9)), case
 
 
-def test_topofit_fp32_matches_python_provider_single_precision(K, reg):
-    cpx, bp, ntw = reg["t1_cpx"].astype(np.complex64), reg["t1_bp"].astype(np.float32), float(reg["t1_ntw"])
+@pytest.mark.parametrize("case,frac", [("t1", 0.99), ("t2", 0.95)])
+def test_topofit_fp32_matches_python_provider_single_precision(K, reg, case, frac):
+    """t2's two candidates per row differ by as little as 1e-6 in coherence,
+    which f32 rounding in either implementation can reorder: 95 % of its rows
+    must agree, 99 % of t1's."""
+    cpx, bp, ntw = reg[case + "_cpx"].astype(np.complex64), reg[case + "_bp"].astype(np.float32), float(reg[case + "_ntw"])
     Kg, Cg, hg, rg = K.run_stage2_topofit_kernel(cpx, bp, ntw)
-    Kr, hr = reg["t1s_gen_K"], reg["t1s_gen_coh"]
+    Kr, hr = reg[case + "s_gen_K"], reg[case + "s_gen_coh"]
     assert np.array_equal(np.isnan(Kg), np.isnan(Kr))
     ok = ~np.isnan(Kr)
     dK = np.abs(Kg - Kr)[ok] / np.maximum(np.abs(Kr[ok]), 1e-3)
     dh = np.abs(hg - hr)[ok]
     agree = (dK <= 1e-4) & (dh <= 1e-5)
-    print(f"FP32 registry topofit: {int(agree.sum())} of {ok.sum()} rows within tolerance")
-    assert agree.mean() >= 0.99, np.flatnonzero(~agree)
+    print(f"FP32 registry topofit {case}: {int(agree.sum())} of {ok.sum()} rows within tolerance")
+    assert agree.mean() >= frac, np.flatnonzero(~agree)
 
 
-def test_topofit_golden_rows_all_candidates(K, golden):
+def test_topofit_golden_rows_all_rows(K, golden):
     """The 96 rows of topofit_rows.npz (ported._ps_topofit_single in complex128),
-    every row including those with several near-max candidates."""
+    every row."""
     d = golden("topofit_rows.npz")
     Kg, Cg, hg, rg = K.run_stage2_topofit_kernel(d["cpx"], d["bperp"], float(d["n_trial_wraps"]))
-    assert (d["n_candidates"] > 1).sum() > 0
     np.testing.assert_allclose(Kg, d["K"], rtol=0, atol=1e-9)
     np.testing.assert_allclose(hg, d["coh"], rtol=0, atol=1e-9)
     np.testing.assert_allclose(np.angle(np.exp(1j * (Cg - d["C"]))), 0, atol=1e-9)
