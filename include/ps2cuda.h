@@ -166,14 +166,14 @@ int ps2_import_state(ps2_ctx* ctx, const void* buf, int64_t bytes);
  * a multiple of 8, power-of-two PS count, precision; a process-wide table):
  * the FP32 topofit with 4, 8, 16 and 32 lanes per PS (ms_per_candidate: NULL
  * or [4]; *chosen_lanes the winner), CLAP with 8 or 4 warps per block and as
- * many or one resident block per SM, binning with as many, 4 or 2 resident
- * blocks per SM. The CLAP and binning shapes give bit-identical results; the
+ * many or one resident block per SM, binning with 16 blocks per SM queued or
+ * 3 or 2 (a persistent grid). The CLAP and binning shapes give bit-identical results; the
  * lane width changes the order of the topofit's partial sums. */
 int ps2_autotune(ps2_ctx* ctx, int32_t* chosen_lanes, double* ms_per_candidate);
 /* Reads (get: NULL or [4]) and/or pins (set: NULL or [4]) the launch shapes of
  * the context: topofit lanes per PS (0 = rule from n_ifg, or 4/8/16/32), CLAP
- * warps per block (0 = default, 4 or 8; FP64 runs 4), CLAP and binning resident
- * blocks per SM (0 = as many as fit). For callers that keep their own tuning
+ * warps per block (0 = default, 4 or 8; FP64 runs 4), CLAP resident blocks per
+ * SM (0 = as many as fit), binning blocks per SM (0 = 16 queued). For callers that keep their own tuning
  * table. */
 int ps2_launch_shapes(ps2_ctx* ctx, int32_t* get, const int32_t* set);
 /* Number of kernel launches issued by the last iterate/run call. */

@@ -1055,7 +1055,7 @@ int ps2_autotune(ps2_ctx* c, int32_t* chosen_lanes, double* ms_per_candidate) {
   {
     DevBuf g2;
     CK(g2.alloc(csz(c) * c->G * c->Mp));
-    const int bpss[3] = {0, 4, 2};
+    const int bpss[3] = {0, 3, 2};
     double best_ms = 1e300;
     for (int b = 0; b < 3; ++b) {
       BinArgs ba = bin_args(c, 0, c->K[0].p);

@@ -146,195 +146,26 @@ __device__ __forceinline__ void bin_task(const BinArgs& a, const int64_t task, c
     a.bp_row_inv ? bin_task_t<R, 0, true>(a, task, lane) : bin_task_t<R, 0, false>(a, task, lane);
 }
 
-// The single-patch binning kernel: the same warp tasks and the same
-// sequential row sums as bin_task_t, with each warp's rows staged through
-// shared memory by asynchronous copies (cp.async). A warp walks its tasks'
-// rows in chunks of kBinRows and keeps kBinStages - 1 chunks in flight while it
-// sums the current one, so the phase and bperp rows stream without holding
-// them in registers. Every lane copies and reads only its own interferogram
-// column; the per-row scalars (K, w or coh) are copied by the first lanes and
-// read by all after a warp barrier.
-constexpr int kBinRows = 8;
-constexpr int kBinStages = 3;
-constexpr int kBinWarps = 4;
-
 template <typename R>
-struct BinStage {
-  float2 ph[kBinRows][32];
-  float bp[kBinRows][32];
-  R k[kBinRows];
-  R w[kBinRows];  // mode 0: weights; mode 1: previous coherence
-};
-
-__device__ __forceinline__ void cp_async_4(void* smem, const void* gmem) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(smem))),
-               "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_8(void* smem, const void* gmem) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(smem))),
-               "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N));
-}
-template <typename R>
-__device__ __forceinline__ void cp_async_r(R* smem, const R* gmem) {
-  if constexpr (sizeof(R) == 8)
-    cp_async_8(smem, gmem);
-  else
-    cp_async_4(smem, gmem);
-}
-
-// psquare_weighting lookup (native_stage2.rs:1674-1682) of one coherence
-template <typename R>
-__device__ __forceinline__ R psquare_weight(const BinArgs& a, const R cohv) {
-  const double v = __dmul_rn(static_cast<double>(cohv), 1000.0);
-  double r = v >= 0.0 ? floor(__dadd_rn(v, 0.5)) : ceil(__dsub_rn(v, 0.5));
-  r = fmin(fmax(r, 0.0), static_cast<double>(a.lut_len - 1));
-  const int ix = isnan(r) ? 0 : static_cast<int>(r);
-  const double t = 1.0 - a.lut[ix];
-  return static_cast<R>(t * t);
-}
-
-// A position in a warp's sequence of row chunks: task, first row, rows.
-struct BinPos {
-  int64_t task;
-  int r0, nr, s1;
-};
-
-template <typename R, int MODE, bool ROWINV>
-__device__ __forceinline__ void bin_issue(const BinArgs& a, const BinPos& q, BinStage<R>& st, const int lane,
-                                          const int64_t ntask) {
-  if (q.task < ntask) {
-    const int chunk = static_cast<int>(q.task % a.nchunk);
-    const int c = chunk * 32 + lane;
-    const int64_t M = a.M;
-    const float2* ph = static_cast<const float2*>(a.ph_nm);
-    if (c < a.M) {
-      for (int i = 0; i < q.nr; ++i) {
-        const int64_t s = q.r0 + i;
-        cp_async_8(&st.ph[i][lane], ph + s * M + c);
-        if (MODE != 3 && !ROWINV) cp_async_4(&st.bp[i][lane], a.bp + s * M + c);
-      }
-    }
-    if (MODE != 3 && lane < q.nr) {
-      cp_async_r(&st.k[lane], static_cast<const R*>(a.K) + q.r0 + lane);
-      cp_async_r(&st.w[lane], static_cast<const R*>(MODE == 1 ? a.coh : a.w) + q.r0 + lane);
-    }
-  }
-  cp_async_commit();
-}
-
-template <typename R>
-__device__ __forceinline__ BinPos bin_first(const BinArgs& a, const int64_t task, const int64_t ntask) {
-  BinPos q{task, 0, 0, 0};
-  if (task < ntask) {
-    const int64_t cell = task / a.nchunk;
-    q.r0 = a.cell_start[cell];
-    q.s1 = a.cell_start[cell + 1];
-    q.nr = q.s1 - q.r0 < kBinRows ? q.s1 - q.r0 : kBinRows;
-  }
-  return q;
-}
-
-template <typename R>
-__device__ __forceinline__ BinPos bin_next(const BinArgs& a, const BinPos& q, const int64_t step, const int64_t ntask) {
-  if (q.r0 + q.nr < q.s1) {
-    BinPos n = q;
-    n.r0 = q.r0 + q.nr;
-    n.nr = n.s1 - n.r0 < kBinRows ? n.s1 - n.r0 : kBinRows;
-    return n;
-  }
-  return bin_first<R>(a, q.task + step, ntask);
-}
-
-template <typename R, int MODE, bool ROWINV>
-__device__ __forceinline__ void bin_warp_async(const BinArgs& a, BinStage<R>* stages, const int64_t first_task,
-                                               const int64_t step, const int lane) {
-  using C = typename CT<R>::C;
+__global__ void __launch_bounds__(256) k_bin(BinArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
   const int64_t ntask = a.G * a.nchunk;
-  R* __restrict__ W = static_cast<R*>(a.w);
-  C* __restrict__ grid = static_cast<C*>(a.grid);
-  BinPos issue_pos = bin_first<R>(a, first_task, ntask);
-  BinPos cur = issue_pos;
-#pragma unroll
-  for (int p = 0; p < kBinStages - 1; ++p) {
-    bin_issue<R, MODE, ROWINV>(a, issue_pos, stages[p], lane, ntask);
-    if (issue_pos.task < ntask) issue_pos = bin_next<R>(a, issue_pos, step, ntask);
-  }
-  R ax = R(0), ay = R(0);
-  for (int64_t e = 0; cur.task < ntask; ++e) {
-    bin_issue<R, MODE, ROWINV>(a, issue_pos, stages[(e + kBinStages - 1) % kBinStages], lane, ntask);
-    if (issue_pos.task < ntask) issue_pos = bin_next<R>(a, issue_pos, step, ntask);
-    cp_async_wait<kBinStages - 1>();
-    __syncwarp();
-    const BinStage<R>& st = stages[e % kBinStages];
-    const int chunk = static_cast<int>(cur.task % a.nchunk);
-    const int c = chunk * 32 + lane;
-    const bool active = c < a.M;
-    const bool write_w = MODE == 1 && chunk == 0 && lane == 0;
-    for (int i = 0; i < cur.nr; ++i) {
-      const R wv = MODE == 3 ? R(1) : (MODE == 1 ? psquare_weight<R>(a, st.w[i]) : st.w[i]);
-      if (write_w) W[cur.r0 + i] = wv;
-      if (!active) continue;
-      const float2 v = st.ph[i][lane];
-      if (MODE == 3) {
-        ax = add_rn(ax, static_cast<R>(v.x));
-        ay = add_rn(ay, static_cast<R>(v.y));
-      } else {
-        const R bv = ROWINV ? static_cast<R>(a.bp[c]) : static_cast<R>(st.bp[i][lane]);
-        const R phs = -(bv * st.k[i]);
-        R sn, cs;
-        sincos_r(phs, &sn, &cs);
-        const C r = cmul_rn(mk(static_cast<R>(v.x), static_cast<R>(v.y)), mk(cs, sn));
-        ax = add_rn(ax, mul_rn(r.x, wv));
-        ay = add_rn(ay, mul_rn(r.y, wv));
-      }
-    }
-    __syncwarp();
-    if (cur.r0 + cur.nr >= cur.s1) {  // the task's last chunk: its cell column is complete
-      const int64_t cell = cur.task / a.nchunk;
-      if (c < a.Mp) grid[cell * a.Mp + c] = active ? mk(ax, ay) : mk(R(0), R(0));
-      ax = R(0);
-      ay = R(0);
-    }
-    cur = bin_next<R>(a, cur, step, ntask);
-  }
-  cp_async_wait<0>();
-}
-
-template <typename R>
-__global__ void __launch_bounds__(32 * kBinWarps) k_bin(BinArgs a) {
-  __shared__ BinStage<R> stages[kBinWarps][kBinStages];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int64_t gw = static_cast<int64_t>(blockIdx.x) * kBinWarps + wib;
-  const int64_t nw = static_cast<int64_t>(gridDim.x) * kBinWarps;
-  BinStage<R>* st = stages[wib];
-  if (a.mode == 3)
-    bin_warp_async<R, 3, false>(a, st, gw, nw, lane);
-  else if (a.mode == 1)
-    a.bp_row_inv ? bin_warp_async<R, 1, true>(a, st, gw, nw, lane) : bin_warp_async<R, 1, false>(a, st, gw, nw, lane);
-  else
-    a.bp_row_inv ? bin_warp_async<R, 0, true>(a, st, gw, nw, lane) : bin_warp_async<R, 0, false>(a, st, gw, nw, lane);
+  for (int64_t task = gw; task < ntask; task += nw) bin_task<R>(a, task, lane);
 }
 
 cudaError_t launch_bin(const BinArgs& a, bool fp64, int sm_count, cudaStream_t st) {
   const int64_t warps = a.G * a.nchunk;
-  int64_t blocks = (warps + kBinWarps - 1) / kBinWarps;
-  int per_sm = 0;
-  cudaError_t e = fp64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bin<double>, 32 * kBinWarps, 0)
-                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bin<float>, 32 * kBinWarps, 0);
-  if (e != cudaSuccess) return e;
-  if (a.blocks_per_sm > 0 && a.blocks_per_sm < per_sm) per_sm = a.blocks_per_sm;
-  const int64_t cap = static_cast<int64_t>(sm_count) * (per_sm > 0 ? per_sm : 1);
+  int64_t blocks = (warps + 7) / 8;
+  // 16 blocks per SM (registers allow about three resident), or the launch shape's cap
+  const int64_t cap = static_cast<int64_t>(sm_count) * (a.blocks_per_sm > 0 ? a.blocks_per_sm : 16);
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
   if (fp64)
-    k_bin<double><<<static_cast<unsigned>(blocks), 32 * kBinWarps, 0, st>>>(a);
+    k_bin<double><<<static_cast<unsigned>(blocks), 256, 0, st>>>(a);
   else
-    k_bin<float><<<static_cast<unsigned>(blocks), 32 * kBinWarps, 0, st>>>(a);
+    k_bin<float><<<static_cast<unsigned>(blocks), 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 
