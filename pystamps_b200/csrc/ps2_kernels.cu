@@ -785,18 +785,32 @@ __device__ __forceinline__ void overlap_elem(const OverlapArgs& a, const int64_t
     if (c < a.M && a.nwi > 0 && a.nwj > 0) {
       const int a1 = max(0, i / a.n_inc - 4), b1 = min(a.nwi - 1, i / a.n_inc + 1);
       const int a2 = max(0, j / a.n_inc - 4), b2 = min(a.nwj - 1, j / a.n_inc + 1);
+      // the (at most 6) candidate windows along j, their offsets and validity
+      int lj6[6];
+      bool okj[6];
+#pragma unroll
+      for (int w = 0; w < 6; ++w) {
+        const int ix2 = a2 + w;
+        const int lj = j - min(ix2 * a.n_inc, a.n_j - nw);
+        okj[w] = ix2 <= b2 && lj >= 0 && lj < nw;
+        lj6[w] = lj;
+      }
       for (int ix1 = a1; ix1 <= b1; ++ix1) {
         const int i1 = min(ix1 * a.n_inc, a.n_i - nw);
         const int li = i - i1;
         if (li < 0 || li >= nw) continue;
-        for (int ix2 = a2; ix2 <= b2; ++ix2) {
-          const int j1 = min(ix2 * a.n_inc, a.n_j - nw);
-          const int lj = j - j1;
-          if (lj < 0 || lj >= nw) continue;
-          const C v = win[((static_cast<int64_t>(ix1) * a.nwj + ix2) * nw2 + li * nw + lj) * a.Mp + c];
-          sx += static_cast<double>(v.x);
-          sy += static_cast<double>(v.y);
-        }
+        // one row of covering windows: every load issued before the ordered sum
+        C v[6];
+#pragma unroll
+        for (int w = 0; w < 6; ++w)
+          v[w] = okj[w] ? win[((static_cast<int64_t>(ix1) * a.nwj + a2 + w) * nw2 + li * nw + lj6[w]) * a.Mp + c]
+                        : mk(R(0), R(0));
+#pragma unroll
+        for (int w = 0; w < 6; ++w)
+          if (okj[w]) {
+            sx += static_cast<double>(v[w].x);
+            sy += static_cast<double>(v[w].y);
+          }
       }
     }
     C f = mk(static_cast<R>(sx), static_cast<R>(sy));
