@@ -435,8 +435,12 @@ int enqueue_iteration(ps2_ctx* c, bool later, bool force_continue, cudaEvent_t* 
   CK(cudaMemsetAsync(c->hist.p, 0, sizeof(int32_t) * PS2_COH_BINS, c->st));
   CK(cudaMemsetAsync(c->n_invalid.p, 0, sizeof(int32_t), c->st));
   CK(cudaMemsetAsync(c->rms_partial.p, 0, sizeof(double) * c->topo_blocks, c->st));
-  const int mode = (later && c->psquare) ? 1 : 0;
-  CK(launch_bin(bin_args(c, mode, c->K[0].p), fp64, c->sm_count, c->st));
+  if (later && c->psquare) {
+    // the P-square weights of this iteration, then binning with them (mode 0)
+    CK(launch_psquare_weights(bin_args(c, 1, c->K[0].p), c->N, fp64, c->sm_count, c->st));
+    ++launched;
+  }
+  CK(launch_bin(bin_args(c, 0, c->K[0].p), fp64, c->sm_count, c->st));
   ++launched;
   if (ev) CK(cudaEventRecord(ev[1], c->st));
   CK(launch_clap(clap_args(c, c->grid.p, c->win.p), fp64, c->twf, c->twd, c->sm_count, c->st));
@@ -2398,7 +2402,8 @@ int ps2_shard_bin(ps2_ctx* c, void* d_grid) {
   CK(cudaMemsetAsync(c->hist.p, 0, sizeof(int32_t) * PS2_COH_BINS, c->st));
   CK(cudaMemsetAsync(c->n_invalid.p, 0, sizeof(int32_t), c->st));
   CK(cudaMemsetAsync(c->rms_partial.p, 0, sizeof(double) * c->topo_blocks, c->st));
-  CK(launch_bin(bin_args(c, (later && c->psquare) ? 1 : 0, c->K[0].p), fp64, c->sm_count, c->st));
+  if (later && c->psquare) CK(launch_psquare_weights(bin_args(c, 1, c->K[0].p), c->N, fp64, c->sm_count, c->st));
+  CK(launch_bin(bin_args(c, 0, c->K[0].p), fp64, c->sm_count, c->st));
   CK(cudaMemcpyAsync(d_grid, c->grid.p, csz(c) * c->G * c->Mp, cudaMemcpyDeviceToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
   return PS2_OK;

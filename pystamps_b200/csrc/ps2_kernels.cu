@@ -134,6 +134,30 @@ __device__ __forceinline__ void bin_task_t(const BinArgs& a, const int64_t task,
   }
 }
 
+// The P-square weights of every row from its previous coherence and the table
+// of the last update (psquare_weighting's lookup, native_stage2.rs:1674-1682),
+// the same function bin_weight applies in mode 1, as one elementwise pass ahead
+// of binning: the binning warps then read w (mode 0) instead of each lane of
+// each interferogram chunk repeating the lookup and its dependent table load.
+template <typename R>
+__global__ void __launch_bounds__(256) k_psquare_weights(BinArgs a, int64_t N) {
+  const R* __restrict__ coh = static_cast<const R*>(a.coh);
+  R* __restrict__ W = static_cast<R*>(a.w);
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; s < N; s += stride)
+    W[s] = bin_weight<R, 1>(a, W, coh, static_cast<int>(s));
+}
+
+cudaError_t launch_psquare_weights(const BinArgs& a, int64_t N, bool fp64, int sm_count, cudaStream_t st) {
+  if (N <= 0) return cudaSuccess;
+  const int64_t blocks = std::min<int64_t>((N + 255) / 256, static_cast<int64_t>(sm_count) * 16);
+  if (fp64)
+    k_psquare_weights<double><<<static_cast<unsigned>(blocks), 256, 0, st>>>(a, N);
+  else
+    k_psquare_weights<float><<<static_cast<unsigned>(blocks), 256, 0, st>>>(a, N);
+  return cudaGetLastError();
+}
+
 // The weighting mode and the row invariance of bperp are compile-time in the
 // task body (no per-element branches on them).
 template <typename R>
@@ -1136,6 +1160,8 @@ __device__ __forceinline__ void prefetch_rows(const void* ph, const float* bp, c
   }
 }
 
+constexpr int kTopoLoadCols = 8;  // columns whose loads a lane issues together in the prologue
+
 // The work of block `vb` of a launch of `nvb` blocks over one patch: PS
 // groups s0 = (vb * 4 + warp) * G + k * nvb * 4 * G. The batched kernel runs
 // the same virtual blocks, so a patch's per-block rms partials, and with them
@@ -1168,20 +1194,26 @@ __device__ __forceinline__ void topofit_vblock_t(const TopoArgs& a, const int mp
   double rms_acc = 0.0;
   int inv_acc = 0;
   const int64_t step = static_cast<int64_t>(nvb) * 4 * G;
+  // the cell of this lane's next PS is loaded one pass ahead, so the
+  // filtered-grid gather of a pass does not wait on it
+  const int64_t s_first = (static_cast<int64_t>(vb) * 4 + wib) * G + g;
+  int64_t cell_next = (LOOP && s_first < a.N) ? a.cell_of[s_first] : 0;
   for (int64_t s0 = (static_cast<int64_t>(vb) * 4 + wib) * G; s0 < a.N; s0 += step) {
     const int64_t s = s0 + g;
     const bool active = s < a.N;
-    const int64_t cell = (active && LOOP) ? a.cell_of[s] : 0;
+    const int64_t cell = cell_next;
+    if (LOOP) cell_next = s + step < a.N ? a.cell_of[s + step] : 0;
     prefetch_rows<G, ROWINV>(LOOP ? static_cast<const void*>(ph_nm) : static_cast<const void*>(cpx), a.bp, s0 + step,
                              a.N, M, lane);
     bool zero = false, nonzero = false;
     float mn = __int_as_float(0x7f800000), mx = -mn;
-    // four columns per round with their global loads issued first
-    for (int k0c = 0; k0c < ncl; k0c += 4) {
-      float2 fv[4], pv[4];
-      float bv[4];
+    // kTopoLoadCols columns per round with their global loads issued first
+    constexpr int PR = kTopoLoadCols;
+    for (int k0c = 0; k0c < ncl; k0c += PR) {
+      float2 fv[PR], pv[PR];
+      float bv[PR];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
+      for (int i = 0; i < PR; ++i) {
         const int c = gl + L * (k0c + i);
         fv[i] = make_float2(0.f, 0.f);
         pv[i] = make_float2(0.f, 0.f);
@@ -1197,7 +1229,7 @@ __device__ __forceinline__ void topofit_vblock_t(const TopoArgs& a, const int mp
         }
       }
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
+      for (int i = 0; i < PR; ++i) {
         const int c = gl + L * (k0c + i);
         if (k0c + i >= ncl) break;
         float2 v = make_float2(0.f, 0.f);
@@ -1298,9 +1330,12 @@ __device__ __forceinline__ void topofit_vblock_t(const TopoArgs& a, const int mp
     oy = group_sum<L>(oy);
     const float2 oc = make_float2(ox, -oy);
     double mopt = 0.0, dl = 0.0;
+    float den_w = 0.f;  // sum |z|: |residual| = |z| (a rotation), the refined coherence's denominator
     for (int k = 0; k < ncl; ++k) {
       const int c = gl + L * k;
-      const double wgt = static_cast<double>(hypotf(cs.zx[c], cs.zy[c]));
+      const float wf = hypotf(cs.zx[c], cs.zy[c]);
+      den_w += wf;
+      const double wgt = static_cast<double>(wf);
       const double wb = __dmul_rn(wgt, static_cast<double>(cs.bp[c]));
       dl = __dadd_rn(dl, __dmul_rn(wb, wb));
       const float2 q = cmul_rn(make_float2(cs.rx[c], cs.ry[c]), oc);
@@ -1310,13 +1345,12 @@ __device__ __forceinline__ void topofit_vblock_t(const TopoArgs& a, const int mp
     dl = group_sum<L>(dl);
     if (dl == 0.0) dl = 1.0;
     const float K1 = static_cast<float>(static_cast<double>(k0) + mopt / dl);
-    float mx2 = 0.f, my2 = 0.f, den2 = 0.f;
+    float mx2 = 0.f, my2 = 0.f, den2 = den_w;
     for (int k = 0; k < ncl; ++k) {
       const int c = gl + L * k;
       const float2 r = cmul_rn(make_float2(cs.zx[c], cs.zy[c]), cis_neg_anchor(K1 * cs.bp[c]));
       mx2 += r.x;
       my2 += r.y;
-      den2 += hypotf(r.x, r.y);
       if (active && c < a.M) {
         if (resid) resid[s * M + c] = invalid ? make_float2(0.f, 0.f) : r;
         if (ph_res) ph_res[s * M + c] = invalid ? 0.f : atan2f(r.y, r.x);

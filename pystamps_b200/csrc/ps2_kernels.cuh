@@ -197,6 +197,8 @@ struct ClapBwdArgs {
 
 // ---------------------------------------------------------- launchers -----
 cudaError_t launch_bin(const BinArgs& a, bool fp64, int sm_count, cudaStream_t st);
+// w[s] = (1 - lut[round(1000 coh[s])])^2 for s < N (a.coh, a.lut, a.lut_len, a.w)
+cudaError_t launch_psquare_weights(const BinArgs& a, int64_t N, bool fp64, int sm_count, cudaStream_t st);
 cudaError_t launch_clap(const ClapArgs& a, bool fp64, const Twiddles32f& tf, const Twiddles32d& td, int sm_count,
                         cudaStream_t st);
 cudaError_t launch_overlap(const OverlapArgs& a, bool fp64, cudaStream_t st);
