@@ -1900,7 +1900,7 @@ struct BatchPlan {
   std::vector<PatchDev> patch;
   std::vector<int64_t> bin_prefix, clap_prefix, ov_prefix;
   std::vector<int32_t> units[4];  // (patch, virtual block) pairs per lane class 4, 8, 16, 32
-  int mpad_max[4] = {0, 0, 0, 0};
+  size_t smem_max[4] = {0, 0, 0, 0};
 };
 
 int lane_class(int L) { return L == 4 ? 0 : L == 8 ? 1 : L == 16 ? 2 : 3; }
@@ -1962,7 +1962,7 @@ int ps2_batch_run(ps2_ctx* const* ctxs, int64_t n, ps2_iter_stats* last) {
     d.nvb = nvb;
     d.lanes = L;
     const int cls = lane_class(L);
-    plan.mpad_max[cls] = std::max(plan.mpad_max[cls], mpad);
+    plan.smem_max[cls] = std::max(plan.smem_max[cls], topofit_smem_bytes(L, mpad, d.topo.n_half));
     for (int vb = 0; vb < nvb; ++vb) {
       plan.units[cls].push_back(static_cast<int32_t>(p));
       plan.units[cls].push_back(vb);
@@ -2019,7 +2019,7 @@ int ps2_batch_run(ps2_ctx* const* ctxs, int64_t n, ps2_iter_stats* last) {
     for (int cls = 0; cls < 4; ++cls) {
       if (plan.units[cls].empty()) continue;
       CK(launch_batch_topofit(b, lanes_of[cls], reinterpret_cast<const int32_t*>(base + o_cls[cls]),
-                              static_cast<int>(plan.units[cls].size() / 2), plan.mpad_max[cls], c0->sm_count, st));
+                              static_cast<int>(plan.units[cls].size() / 2), plan.smem_max[cls], c0->sm_count, st));
     }
     CK(launch_batch_finalize(b, st));
     return PS2_OK;

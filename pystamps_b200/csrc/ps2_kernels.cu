@@ -20,6 +20,7 @@
 
 #include "ps2_device.cuh"
 #include "ps2_kernels.cuh"
+#include "trial_interp_taps.h"
 
 namespace ps2 {
 
@@ -1184,6 +1185,208 @@ __device__ __forceinline__ void sweep_trial_pairs(const ColumnSmem& cs, const fl
   }
 }
 
+// ---- sampled trial sweep ---------------------------------------------------
+// Only the argmax of |S_m|^2 over the trials leaves the sweep (the refinement
+// recomputes K and the coherence exactly), and |S_m| = |T(m)| for the trial sum
+// centred on the middle of the PS's bperp range,
+//   T(m) = sum_c z_c e^{-j phi_c m},  phi_c = (bp_c - mid) (pi/4) / range,
+// whose phases span exactly [-pi/8, pi/8]: T is band-limited to a quarter of
+// the trial rate. It is evaluated exactly (same recurrences as the full sweep)
+// at every 4th trial, m = 4k for |k| <= 16 NB, and between the samples by
+// 20-tap fractional-delay filters (trial_interp_taps.h: error at most 6.8e-8 of
+// sum |z_c|, below the FP32 rounding of the sums), so the sweep costs 16 NB + ~8
+// magnitude steps instead of n_half. The samples stay in registers until the
+// sweep ends (the column store's rotation slots, which the sample region
+// overlays, are read until then).
+constexpr int kMaxSampleBlocks = 2;
+
+// Number of 16-magnitude sample blocks for n_half, or 0 where the full sweep
+// is the cheaper (n_half <= 16 NB + 8) or the samples would exceed three blocks.
+__host__ __device__ inline int trial_sample_blocks(int n_half) {
+  const int ks = n_half / kTrialStride + (kInterpTapLo + kInterpTaps);  // floor(n/4) + 11 > the top tap
+  const int nb = (ks + 15) / 16;
+  if (nb < 2 || nb > kMaxSampleBlocks || 16 * nb + 8 >= n_half) return 0;
+  return nb;
+}
+
+// Samples the filters read: T(4k) for k in [-kn, kp], kn = ceil(n/4) - tap_lo,
+// kp = floor(n/4) + the top tap; kept at samp[kn + k].
+__host__ __device__ inline int trial_samples_below(int n_half) { return (n_half + 3) / 4 - kInterpTapLo; }
+__host__ __device__ inline int trial_samples_count(int n_half) {
+  return trial_samples_below(n_half) + n_half / 4 + (kInterpTapLo + kInterpTaps - 1) + 1;
+}
+
+// Per-PS slot of the column store in floats: z (2), rotation (2) and bp
+// columns, with the sample array over the rotation columns when it fits there
+// and after bp otherwise; padded so the groups of a warp start in different
+// banks.
+__host__ __device__ inline int topofit_sample_offset(int mpad, int n_half) {
+  const int nb = trial_sample_blocks(n_half);
+  return (nb == 0 || trial_samples_count(n_half) <= mpad) ? 2 * mpad : 5 * mpad;
+}
+__host__ __device__ inline int topofit_stride(int L, int mpad, int n_half) {
+  const int nb = trial_sample_blocks(n_half);
+  int need = 5 * mpad;
+  if (nb > 0) {
+    const int top = topofit_sample_offset(mpad, n_half) + 2 * trial_samples_count(n_half);
+    need = top > need ? top : need;
+  }
+  return ((need + 31) / 32) * 32 + (L % 32);
+}
+
+// One block of 16 sample magnitudes |k| = k0 .. k0+15 (the body of
+// sweep_trial_pairs<16> with the centred phase per sample a_c = (bp_c - mid) qa
+// and rotation e^{-j a_c} in the column store). Returns the lane's 32/L
+// group-summed slots (slot idx < 16: T(4 (k0+idx)); else T(-4 (k0+idx-16))),
+// the first of them at slot `base`.
+template <int L>
+__device__ __forceinline__ void sweep_sample_block(const ColumnSmem& cs, const float qa, const float mid,
+                                                   const int ncl, const int gl, const int k0,
+                                                   float2 (&out)[32 / L], int& base) {
+  constexpr int H = 8;
+  float2 P[H], Q[H], R[H], U[H];
+#pragma unroll
+  for (int i = 0; i < H; ++i) {
+    P[i] = make_float2(0.f, 0.f);
+    Q[i] = make_float2(0.f, 0.f);
+    R[i] = make_float2(0.f, 0.f);
+    U[i] = make_float2(0.f, 0.f);
+  }
+#pragma unroll 2
+  for (int k = 0; k < ncl; ++k) {
+    const int c = gl + L * k;
+    const float x = cs.zx[c], y = cs.zy[c], rx = cs.rx[c], ry = cs.ry[c];
+    constexpr int A = H / 2 - 1;
+    const float2 a0 = cis_neg_anchor((cs.bp[c] - mid) * qa * static_cast<float>(k0 + 2 * A));
+    const float a1x = fmaf(a0.x, rx, -a0.y * ry), a1y = fmaf(a0.x, ry, a0.y * rx);
+    const float r2x = fmaf(rx, rx, -ry * ry), r2y = 2.f * rx * ry;
+    const float2 X = make_float2(x, x), Y = make_float2(y, y);
+    const float2 Cp = make_float2(2.f * r2x, 2.f * r2x), Cn = make_float2(-2.f * r2x, -2.f * r2x);
+    const float2 UAx = make_float2(a0.x, a1x), UAy = make_float2(a0.y, a1y);
+    const float2 UBx = make_float2(fmaf(a0.x, r2x, -a0.y * r2y), fmaf(a1x, r2x, -a1y * r2y));
+    const float2 UBy = make_float2(fmaf(a0.x, r2y, a0.y * r2x), fmaf(a1x, r2y, a1y * r2x));
+    P[A] = __ffma2_rn(X, UAx, P[A]);
+    Q[A] = __ffma2_rn(X, UAy, Q[A]);
+    R[A] = __ffma2_rn(Y, UAx, R[A]);
+    U[A] = __ffma2_rn(Y, UAy, U[A]);
+    float2 Vx = UAx, Vy = UAy, Wx = UBx, Wy = UBy;
+#pragma unroll
+    for (int i = A + 1; i < H; ++i) {
+      P[i] = __ffma2_rn(X, Wx, P[i]);
+      Q[i] = __ffma2_rn(X, Wy, Q[i]);
+      R[i] = __ffma2_rn(Y, Wx, R[i]);
+      U[i] = __ffma2_rn(Y, Wy, U[i]);
+      if (i + 1 < H) {
+        const float2 nx = __ffma2_rn(((i - A) & 1) ? Cn : Cp, Wx, Vx);
+        const float2 ny = __ffma2_rn(((i - A) & 1) ? Cn : Cp, Wy, Vy);
+        Vx = Wx;
+        Vy = Wy;
+        Wx = nx;
+        Wy = ny;
+      }
+    }
+    Vx = UBx;
+    Vy = UBy;
+    Wx = UAx;
+    Wy = UAy;
+#pragma unroll
+    for (int i = A; i > 0; --i) {
+      const float2 nx = __ffma2_rn(((A - i) & 1) ? Cp : Cn, Wx, Vx);
+      const float2 ny = __ffma2_rn(((A - i) & 1) ? Cp : Cn, Wy, Vy);
+      Vx = Wx;
+      Vy = Wy;
+      Wx = nx;
+      Wy = ny;
+      P[i - 1] = __ffma2_rn(X, Wx, P[i - 1]);
+      Q[i - 1] = __ffma2_rn(X, Wy, Q[i - 1]);
+      R[i - 1] = __ffma2_rn(Y, Wx, R[i - 1]);
+      U[i - 1] = __ffma2_rn(Y, Wy, U[i - 1]);
+    }
+  }
+  // the chain's sign s_i is common to a slot's four sums: T itself carries it,
+  // so undo it here (s_{A+j} = -1 for j mod 4 in {2, 3}; A = 3)
+  float2 S[32];
+#pragma unroll
+  for (int i = 0; i < H; ++i) {
+    const float s = (((i - 3) & 3) >= 2) ? -1.f : 1.f;
+    S[2 * i] = make_float2(s * (P[i].x - U[i].x), s * (Q[i].x + R[i].x));
+    S[2 * i + 1] = make_float2(s * (P[i].y - U[i].y), s * (Q[i].y + R[i].y));
+    S[16 + 2 * i] = make_float2(s * (P[i].x + U[i].x), s * (R[i].x - Q[i].x));
+    S[16 + 2 * i + 1] = make_float2(s * (P[i].y + U[i].y), s * (R[i].y - Q[i].y));
+  }
+  group_transpose_reduce<32, L>(S, gl, base);
+#pragma unroll
+  for (int j = 0; j < 32 / L; ++j) out[j] = S[j];
+}
+
+// Sampled sweep of a group: NB sample blocks, the samples the filters read
+// written to `samp` (T(4k) at samp[kn + k]), then every trial t = n_half + m evaluated (exact
+// at m = 4k, interpolated between) and the first maximum of |T|^2 kept in
+// trial order. Lanes take chunks of 3 sample periods (12 trials) in turn and
+// hold the 22 samples a chunk's filters read in registers.
+template <int L, int NB>
+__device__ __forceinline__ void sampled_sweep(const ColumnSmem& cs, float2* samp, const float qa, const float mid,
+                                              const int ncl, const int gl, const int n_half, const float2 s0,
+                                              float& best_sq, int& best_t) {
+  constexpr int NO = 32 / L;
+  const int kn = trial_samples_below(n_half), kp = trial_samples_count(n_half) - 1 - kn;
+  float2 held[NB][NO];
+  int bases[NB];
+#pragma unroll
+  for (int b = 0; b < NB; ++b) sweep_sample_block<L>(cs, qa, mid, ncl, gl, 1 + 16 * b, held[b], bases[b]);
+  __syncwarp();  // every lane of the warp is done with the rotation columns
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+#pragma unroll
+    for (int j = 0; j < NO; ++j) {
+      const int idx = bases[b] + j;
+      const int k = idx < 16 ? 1 + 16 * b + idx : -(1 + 16 * b + idx - 16);
+      if (k >= -kn && k <= kp) samp[kn + k] = held[b][j];
+    }
+  }
+  if (gl == 0) samp[kn] = s0;
+  __syncwarp();
+  constexpr int CP = 3, NWIN = CP + kInterpTaps - 1;
+  const int klo = -((n_half + 3) / 4), khi = n_half / 4;  // floor(-n/4), floor(n/4)
+  const int nch = (khi - klo + CP) / CP;
+  best_sq = -1.f;
+  best_t = 0x7fffffff;
+  for (int ch = gl; ch < nch; ch += L) {
+    const int kb = klo + ch * CP;
+    float2 win[NWIN];  // T(4 (kb + kInterpTapLo + i))
+#pragma unroll
+    for (int i = 0; i < NWIN; ++i) {
+      const int k = kb + kInterpTapLo + i;
+      win[i] = (k >= -kn && k <= kp) ? samp[kn + k] : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int pp = 0; pp < CP; ++pp) {
+      const int k = kb + pp;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int m = 4 * k + r;
+        float2 v;
+        if (r == 0) {
+          v = win[pp - kInterpTapLo];
+        } else {
+          v = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int i = 0; i < kInterpTaps; ++i) {
+            const float h = kInterpTaps_c[r - 1][i];
+            v = __ffma2_rn(make_float2(h, h), win[pp + i], v);
+          }
+        }
+        const float sq = v.x * v.x + v.y * v.y;
+        const int t = n_half + m;
+        if (m >= -n_half && m <= n_half && (sq > best_sq || (sq == best_sq && t < best_t))) {
+          best_sq = sq;
+          best_t = t;
+        }
+      }
+    }
+  }
+}
+
 // L2 prefetch of the rows a warp reads on its next pass (the PS group s0n ..
 // s0n+G-1): the phase rows and, unless bperp is row invariant, the bperp rows,
 // one 128-byte line per lane per instruction, all inside the arrays.
@@ -1220,9 +1423,11 @@ __device__ __forceinline__ void topofit_vblock_t(const TopoArgs& a, const int mp
   for (int i = tid; i < kCohBins; i += blockDim.x) sh_hist[i] = 0;
   __syncthreads();
   // per-PS slot stride = L (mod 32) floats so the groups of a warp hit different banks
-  const int stride = ((5 * mpad + 31) / 32) * 32 + (L % 32);
+  const int stride = topofit_stride(L, mpad, a.n_half);
   float* base_ptr = reinterpret_cast<float*>(smem_raw) + static_cast<int64_t>(wib * G + g) * stride;
   ColumnSmem cs{base_ptr, base_ptr + mpad, base_ptr + 2 * mpad, base_ptr + 3 * mpad, base_ptr + 4 * mpad};
+  const int nb = trial_sample_blocks(a.n_half);
+  float2* samp = reinterpret_cast<float2*>(base_ptr + topofit_sample_offset(mpad, a.n_half));
   const float2* __restrict__ ph_nm = static_cast<const float2*>(a.ph_nm);
   const float2* __restrict__ filt = static_cast<const float2*>(a.filt);
   const float2* __restrict__ cpx = static_cast<const float2*>(a.cpx);
@@ -1310,9 +1515,13 @@ __device__ __forceinline__ void topofit_vblock_t(const TopoArgs& a, const int mp
     mx = group_max<L>(mx);
     float range = mx - mn;
     if (!(range != 0.f) || invalid) range = 1.f;
+    // sampled sweep: rotation e^{-j a_c} per sample step, a_c = (bp_c - mid) qa;
+    // full sweep: e^{-j theta_c} per trial, theta_c = bp_c / range * pi/4
+    const float mid = (nb > 0 && !invalid && mx >= mn) ? 0.5f * (mn + mx) : 0.f;
+    const float qa = (kQuarterPiF / range) * static_cast<float>(kTrialStride);
     for (int k = 0; k < ncl; ++k) {
       const int c = gl + L * k;
-      const float t = (cs.bp[c] / range) * kQuarterPiF;
+      const float t = nb > 0 ? (cs.bp[c] - mid) * qa : (cs.bp[c] / range) * kQuarterPiF;
       float sn, cn;
       sincosf(t, &sn, &cn);
       cs.rx[c] = cn;
@@ -1332,22 +1541,26 @@ __device__ __forceinline__ void topofit_vblock_t(const TopoArgs& a, const int mp
     s0y = group_sum<L>(s0y);
     best_sq = s0x * s0x + s0y * s0y;
     int best_t = a.n_half;
-    int m0 = 1;
-    for (; a.n_half - m0 + 1 >= 16; m0 += 16)
-      sweep_trial_pairs<16, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
-    if (a.n_half - m0 + 1 >= 8) {
-      sweep_trial_pairs<8, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
-      m0 += 8;
+    if (nb == 2) {
+      sampled_sweep<L, 2>(cs, samp, qa, mid, ncl, gl, a.n_half, make_float2(s0x, s0y), best_sq, best_t);
+    } else {
+      int m0 = 1;
+      for (; a.n_half - m0 + 1 >= 16; m0 += 16)
+        sweep_trial_pairs<16, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
+      if (a.n_half - m0 + 1 >= 8) {
+        sweep_trial_pairs<8, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
+        m0 += 8;
+      }
+      if (a.n_half - m0 + 1 >= 4) {
+        sweep_trial_pairs<4, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
+        m0 += 4;
+      }
+      if (a.n_half - m0 + 1 >= 2) {
+        sweep_trial_pairs<2, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
+        m0 += 2;
+      }
+      if (a.n_half - m0 + 1 >= 1) sweep_pairs<1, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
     }
-    if (a.n_half - m0 + 1 >= 4) {
-      sweep_trial_pairs<4, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
-      m0 += 4;
-    }
-    if (a.n_half - m0 + 1 >= 2) {
-      sweep_trial_pairs<2, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
-      m0 += 2;
-    }
-    if (a.n_half - m0 + 1 >= 1) sweep_pairs<1, L>(cs, qr, ncl, gl, m0, a.n_half, best_sq, best_t);
     // first maximum over the group (argmax_first_f32, :1526-1536)
 #pragma unroll
     for (int o = L / 2; o > 0; o >>= 1) {
@@ -1358,6 +1571,8 @@ __device__ __forceinline__ void topofit_vblock_t(const TopoArgs& a, const int mp
         best_t = ot;
       }
     }
+    if (best_t == 0x7fffffff) best_t = a.n_half;  // no finite |T|^2: the m = 0 trial, as the full sweep keeps
+    __syncwarp();  // the sample array overlays the rotation slots written next
     // refine_candidate (:1259-1303) with FP64 normal-equation sums; the
     // rotation slots of the column store now hold z e^{-j k0 bp}
     const float k0 = kQuarterPiF / range * static_cast<float>(best_t - a.n_half);
@@ -1656,9 +1871,8 @@ int topofit_lanes(int M) {
   return L;
 }
 
-size_t topofit_smem_bytes(int L, int mpad) {
-  const int stride = ((5 * mpad + 31) / 32) * 32 + (L % 32);
-  return static_cast<size_t>(4 * (32 / L)) * stride * sizeof(float);
+size_t topofit_smem_bytes(int L, int mpad, int n_half) {
+  return static_cast<size_t>(4 * (32 / L)) * topofit_stride(L, mpad, n_half) * sizeof(float);
 }
 
 // Columns per PS padded to a multiple of 2L (zero columns): each lane holds an
@@ -1668,7 +1882,7 @@ int topofit_mpad(int L, int M) { return ((M + 2 * L - 1) / (2 * L)) * (2 * L); }
 template <int L>
 static cudaError_t topofit_geometry_l(const TopoArgs& a, int grid_cap, size_t* smem, int* blocks_out) {
   const int mpad = topofit_mpad(L, a.M);
-  const size_t sm = topofit_smem_bytes(L, mpad);
+  const size_t sm = topofit_smem_bytes(L, mpad, a.n_half);
   cudaError_t e = kernel_attributes_once(sm);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -2780,9 +2994,8 @@ cudaError_t launch_batch_overlap(const BatchArgs& b, int64_t total, int sm_count
 }
 
 template <int L>
-static cudaError_t batch_topofit_l(const BatchArgs& b, const int32_t* units, int n_units, int mpad_max, int sm_count,
+static cudaError_t batch_topofit_l(const BatchArgs& b, const int32_t* units, int n_units, size_t sm, int sm_count,
                                    cudaStream_t st) {
-  const size_t sm = topofit_smem_bytes(L, mpad_max);
   cudaError_t e = kernel_attributes_once(sm);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -2793,14 +3006,14 @@ static cudaError_t batch_topofit_l(const BatchArgs& b, const int32_t* units, int
   return cudaGetLastError();
 }
 
-cudaError_t launch_batch_topofit(const BatchArgs& b, int L, const int32_t* units, int n_units, int mpad_max,
+cudaError_t launch_batch_topofit(const BatchArgs& b, int L, const int32_t* units, int n_units, size_t smem,
                                  int sm_count, cudaStream_t st) {
   if (n_units <= 0) return cudaSuccess;
   switch (L) {
-    case 4: return batch_topofit_l<4>(b, units, n_units, mpad_max, sm_count, st);
-    case 8: return batch_topofit_l<8>(b, units, n_units, mpad_max, sm_count, st);
-    case 16: return batch_topofit_l<16>(b, units, n_units, mpad_max, sm_count, st);
-    case 32: return batch_topofit_l<32>(b, units, n_units, mpad_max, sm_count, st);
+    case 4: return batch_topofit_l<4>(b, units, n_units, smem, sm_count, st);
+    case 8: return batch_topofit_l<8>(b, units, n_units, smem, sm_count, st);
+    case 16: return batch_topofit_l<16>(b, units, n_units, smem, sm_count, st);
+    case 32: return batch_topofit_l<32>(b, units, n_units, smem, sm_count, st);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -218,7 +218,7 @@ cudaError_t launch_gather_widen(const float* src, double* dst, const int32_t* pe
 cudaError_t launch_scatter_narrow(const double* src, float* dst, const int32_t* perm, int64_t n, int64_t words,
                                   cudaStream_t st);
 cudaError_t launch_reduce_ab(const double* part, int n, double* out, cudaStream_t st);
-size_t topofit_smem_bytes(int L, int mpad);
+size_t topofit_smem_bytes(int L, int mpad, int n_half);
 cudaError_t topofit_geometry(const TopoArgs& a, int grid_cap, int* L_out, int* mpad_out, int* blocks_out);
 cudaError_t launch_batch_reset(const BatchArgs& b, cudaStream_t st);
 cudaError_t launch_s3_clap(const S3ClapArgs& a, const Twiddles32f& tf, int sm_count, cudaStream_t st);
@@ -248,7 +248,7 @@ cudaError_t launch_batch_bin(const BatchArgs& b, int64_t total, int sm_count, cu
 cudaError_t launch_batch_clap(const BatchArgs& b, int64_t total, const Twiddles32f& tf, int sm_count,
                               cudaStream_t st);
 cudaError_t launch_batch_overlap(const BatchArgs& b, int64_t total, int sm_count, cudaStream_t st);
-cudaError_t launch_batch_topofit(const BatchArgs& b, int L, const int32_t* units, int n_units, int mpad_max,
+cudaError_t launch_batch_topofit(const BatchArgs& b, int L, const int32_t* units, int n_units, size_t smem,
                                  int sm_count, cudaStream_t st);
 cudaError_t launch_batch_finalize(const BatchArgs& b, cudaStream_t st);
 cudaError_t launch_batch_continue(cudaGraphConditionalHandle h, const int* n_active, cudaStream_t st);
