@@ -262,6 +262,23 @@ def _sensitivity(oracle, patch, g, o):
     return np.median(np.abs(g["coh_ps"] - o["coh_ps"])), np.median(np.abs(o64["coh_ps"] - o["coh_ps"]))
 
 
+def _perturbed_spread(oracle, patch, o, eps=1e-6, seeds=(1, 2, 3)):
+    """The reference algorithm's own divergence: the oracle run again with its
+    input phases rotated by eps * N(0, 1) rad (about the size of the per-
+    iteration FP32 differences the teacher-forced tests bound), against its
+    unperturbed run. Returns the largest median and 90th percentile of
+    |d gamma| over the seeds."""
+    med, p90 = 0.0, 0.0
+    nr = np.concatenate([o["Nr_base"], [o["Nr_max_nz_ix"]]])
+    for sd in seeds:
+        rng = np.random.default_rng(sd)
+        ph = patch["ph"] * np.exp(1j * eps * rng.standard_normal(patch["ph"].shape)).astype(patch["ph"].dtype)
+        op = oracle.stage2_run(dict(patch, ph=ph, nr_override=nr))
+        d = np.abs(op["coh_ps"] - o["coh_ps"])
+        med, p90 = max(med, float(np.median(d))), max(p90, float(np.quantile(d, 0.9)))
+    return med, p90
+
+
 @pytest.mark.parametrize("seed", [101, 103])
 def test_stage2_loop_free_running_against_oracle(S, oracle, seed):
     """Whole loop to convergence, GPU and oracle each on their own state.
@@ -270,10 +287,15 @@ def test_stage2_loop_free_running_against_oracle(S, oracle, seed):
     two trajectories separate: a PS whose best and runner-up trials are within
     rounding of each other takes a different K, and round(1000 coh) in the
     P-square table moves weights by whole table steps, after which the binned
-    grid and every neighbour's filtered phase differ. Measured on this shape,
-    the median |d gamma| after convergence is 1.2e-7 to 2.5e-4 depending on
-    the seed. The bounds: same iteration count, cells and invalid rows, median
-    |d gamma| <= 5e-4, 90% of PS within 1e-3."""
+    grid and every neighbour's filtered phase differ. How far depends on the
+    seed (median |d gamma| from 1e-7 to 3e-4 on this shape), and the oracle run
+    against itself with its input phases rotated by 1e-6 rad separates by as
+    much (seeds 101 and 103: median 5e-4, 90th percentile 3e-3, twice the
+    GPU's). The bounds: same iteration count, cells and invalid rows; the
+    GPU's median and 90th percentile |d gamma| within 1.5x the largest of
+    three such perturbed oracle runs (plus 1e-6 and 1e-5, the scale of one
+    iteration's FP32 differences, for seeds whose perturbed runs do not
+    separate)."""
     from pystamps_b200 import synth
 
     patch = synth.make_patch(6000, 16, 32, 41, seed=seed, n_rand=20_000)
@@ -282,9 +304,11 @@ def test_stage2_loop_free_running_against_oracle(S, oracle, seed):
     assert g["i_loop"] == o["i_loop"]
     d = np.abs(g["coh_ps"] - o["coh_ps"])
     d_gpu, d_ref = _sensitivity(oracle, patch, g, o)
-    print(f"seed {seed}: median |dgamma| {d_gpu:.2e} (oracle FP32 vs FP64 {d_ref:.2e}), p90 {np.quantile(d, 0.9):.2e}")
-    assert d_gpu <= 5e-4, (d_gpu, d_ref)
-    assert np.quantile(d, 0.9) <= 1e-3
+    p_med, p_p90 = _perturbed_spread(oracle, patch, o)
+    print(f"seed {seed}: median |dgamma| {d_gpu:.2e} (oracle FP32 vs FP64 {d_ref:.2e}, oracle vs oracle with "
+          f"1e-6 rad input rotations {p_med:.2e}), p90 {np.quantile(d, 0.9):.2e} (perturbed oracle {p_p90:.2e})")
+    assert d_gpu <= 1.5 * p_med + 1e-6, (d_gpu, p_med)
+    assert np.quantile(d, 0.9) <= 1.5 * p_p90 + 1e-5, (np.quantile(d, 0.9), p_p90)
     np.testing.assert_array_equal(np.isnan(g["K_ps"]), np.isnan(o["K_ps"]))
     np.testing.assert_allclose(g["Nr"], o["Nr"], rtol=5e-2)  # cumulative scaling of a chaotic history
 
