@@ -519,7 +519,7 @@ def run_ours(args, rank: int, world: int, dist):
                     "nontie_dK_m_max": float(np.nanmax(np.delete(dk1, tie_rows))),
                     "note": "PS above the bounds classified by an FP64 trial search of their rows "
                             "(pystamps_b200.precision.classify_ties): argmax ties (best and runner-up trial "
-                            "within 1e-6 relative) and refinement wrap ties (a residual angle within 1e-4 rad "
+                            "within 1e-6 of max(best, 0.5)) and refinement wrap ties (a residual angle within 1e-4 rad "
                             "of +-pi)"},
                 "converged": {"iterations_fp32": a["i_loop"], "iterations_fp64": b["i_loop"],
                               "dgamma_median": float(np.median(d)), "dgamma_p99": float(np.quantile(d, 0.99)),

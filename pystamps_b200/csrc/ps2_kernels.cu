@@ -1545,7 +1545,7 @@ __device__ __forceinline__ void topofit_vblock_t(const TopoArgs& a, const int mp
       const int c = gl + L * k;
       const float t = nb > 0 ? (cs.bp[c] - mid) * qa : (cs.bp[c] / range) * kQuarterPiF;
       float sn, cn;
-      sincosf(t, &sn, &cn);
+      sincos_cw(t, &sn, &cn);
       cs.rx[c] = cn;
       cs.ry[c] = -sn;
     }
@@ -1614,7 +1614,10 @@ __device__ __forceinline__ void topofit_vblock_t(const TopoArgs& a, const int mp
     float den_w = 0.f;  // sum |z|: |residual| = |z| (a rotation), the refined coherence's denominator
     for (int k = 0; k < ncl; ++k) {
       const int c = gl + L * k;
-      const float wf = hypotf(cs.zx[c], cs.zy[c]);
+      // in the loop |z| is that of a product of two unit (or zero) phasors, with
+      // no overflow or underflow to guard against: sqrt(x^2 + y^2) is within an
+      // ulp of hypotf at a third of its cost; standalone rows take any magnitude
+      const float wf = LOOP ? sqrtf(fmaf(cs.zx[c], cs.zx[c], cs.zy[c] * cs.zy[c])) : hypotf(cs.zx[c], cs.zy[c]);
       den_w += wf;
       const double wgt = static_cast<double>(wf);
       const double wb = __dmul_rn(wgt, static_cast<double>(cs.bp[c]));

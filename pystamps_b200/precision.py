@@ -20,8 +20,19 @@ import numpy as np
 from . import stage2 as S
 from . import synth
 
-ARGMAX_TIE_REL = 1e-6  # best and runner-up trial coherence this close (relative): an argmax tie
-WRAP_TIE_RAD = 1e-4    # a refinement residual angle this close to +-pi: a wrap tie
+ARGMAX_TIE_REL = 1e-6    # best and runner-up trial coherence this close (relative): an argmax tie ...
+ARGMAX_TIE_FLOOR = 0.5   # ... taken relative to max(best, 0.5): an FP32 trial coherence carries an
+                         # error of roughly fixed size (its phasor and summation rounding over the
+                         # columns), so below coherence 0.5 the rule is an absolute 5e-7
+WRAP_TIE_RAD = 1e-4      # a refinement residual angle this close to +-pi: a wrap tie
+
+
+def is_argmax_tie(best, second):
+    """Best and runner-up trial coherence within ARGMAX_TIE_REL of max(best,
+    ARGMAX_TIE_FLOOR): an FP32 evaluation of the trials may pick either (for
+    example two trials at 0.23912255 and 0.23912231 of a 2,000,000 x 150 patch)."""
+    best = np.asarray(best, np.float64)
+    return (best - np.asarray(second, np.float64)) <= ARGMAX_TIE_REL * np.maximum(best, ARGMAX_TIE_FLOOR)
 
 
 def trial_values(n_trial_wraps: float) -> np.ndarray:
@@ -70,7 +81,7 @@ def wrap_distance(ph_nm, ph_patch, bperp, n_trial_wraps: float, best_ix=None) ->
 
 def classify_ties(ph_nm, ph_patch, bperp, n_trial_wraps: float) -> dict:
     """Tie classes of the given rows (few rows: every trial in FP64):
-    argmax ties (best and runner-up trial within ARGMAX_TIE_REL relative) and
+    argmax ties (best and runner-up trial within is_argmax_tie) and
     wrap ties (a refinement residual angle within WRAP_TIE_RAD of +-pi). Rows
     that are neither are genuine FP32/FP64 differences."""
     ph_nm = np.atleast_2d(ph_nm)
@@ -84,7 +95,7 @@ def classify_ties(ph_nm, ph_patch, bperp, n_trial_wraps: float) -> dict:
     srt = np.sort(coh, axis=1)
     best = srt[:, -1]
     second = srt[:, -2] if coh.shape[1] > 1 else np.zeros(coh.shape[0])
-    argmax_tie = (best - second) <= ARGMAX_TIE_REL * np.maximum(best, 1e-30)
+    argmax_tie = is_argmax_tie(best, second)
     wrap_tie = wrap_distance(ph_nm, ph_patch, bp, n_trial_wraps, np.argmax(coh, axis=1)) < WRAP_TIE_RAD
     return {"argmax_tie": argmax_tie, "wrap_tie": wrap_tie, "tie": argmax_tie | wrap_tie}
 
