@@ -167,14 +167,18 @@ int ps2_import_state(ps2_ctx* ctx, const void* buf, int64_t bytes);
  * the FP32 topofit with 4, 8, 16 and 32 lanes per PS (ms_per_candidate: NULL
  * or [4]; *chosen_lanes the winner), CLAP with 8 or 4 warps per block and as
  * many or one resident block per SM, binning with 16 blocks per SM queued or
- * 3 or 2 (a persistent grid). The CLAP and binning shapes give bit-identical results; the
- * lane width changes the order of the topofit's partial sums. */
+ * 3 or 2 (a persistent grid), and the CLAP form (window stack or fused window
+ * blocks, each timed with its second pass). The CLAP and binning shapes give
+ * bit-identical results (the two CLAP forms wherever their FP64 sums are
+ * exact); the lane width changes the order of the topofit's partial sums. */
 int ps2_autotune(ps2_ctx* ctx, int32_t* chosen_lanes, double* ms_per_candidate);
-/* Reads (get: NULL or [4]) and/or pins (set: NULL or [4]) the launch shapes of
+/* Reads (get: NULL or [5]) and/or pins (set: NULL or [5]) the launch shapes of
  * the context: topofit lanes per PS (0 = rule from n_ifg, or 4/8/16/32), CLAP
  * warps per block (0 = default, 4 or 8; FP64 runs 4), CLAP resident blocks per
- * SM (0 = as many as fit), binning blocks per SM (0 = 16 queued). For callers that keep their own tuning
- * table. */
+ * SM (0 = as many as fit), binning blocks per SM (0 = 16 queued), CLAP form
+ * (0 = each window into a window stack, then the overlap-add pass; 1 = blocks
+ * of 4 x 4 windows summed into FP64 partials, then a combine pass: no window
+ * stack). For callers that keep their own tuning table. */
 int ps2_launch_shapes(ps2_ctx* ctx, int32_t* get, const int32_t* set);
 /* Number of kernel launches issued by the last iterate/run call. */
 int64_t ps2_last_launch_count(const ps2_ctx* ctx);

@@ -194,7 +194,7 @@ std::vector<double> window_weight_scaled(int n_win, int n_ex) {
 // per block and resident blocks per SM, binning's resident blocks per SM
 // (0 everywhere: the built-in rules).
 struct TuneShape {
-  int lanes = 0, clap_nw = 0, clap_bps = 0, bin_bps = 0;
+  int lanes = 0, clap_nw = 0, clap_bps = 0, bin_bps = 0, clap_fused = 0;
 };
 std::mutex g_tune_mu;
 std::vector<std::pair<int64_t, TuneShape>> g_tune_cache;
@@ -239,7 +239,7 @@ struct ps2_ctx {
   double g7[7], g7sum = 0.0;
   Twiddles32f twf;
   Twiddles32d twd;
-  DevBuf ph_nm, bp, amp, perm, cell_start, cell_of, w0, K[2], w, coh, C, nopt, grid, win, filt, low_pass, wscaled,
+  DevBuf ph_nm, bp, amp, perm, cell_start, cell_of, w0, K[2], w, coh, C, nopt, grid, win, wpart, filt, low_pass, wscaled,
       taps, lut, nr0, nr_scaled, state, stats, hist, n_invalid, rms_partial, ph_res, scratch, stage;
   // differentiable coherence (ps2_coherence_forward / _backward): own buffers,
   // the loop state above is left untouched
@@ -265,6 +265,7 @@ struct ps2_ctx {
   int64_t graph_body_launches = 0;
   int topo_lanes = 0;  // 0: rule from n_ifg; else chosen by ps2_autotune
   int clap_nw = 0, clap_bps = 0, bin_bps = 0;  // launch shapes (0: built-in rules)
+  int clap_fused = 0;  // CLAP form: 0 window stack + overlap-add pass, 1 window blocks into partials + combine
   int topo_blocks = 0;
   int64_t iters_done = 0;  // since load/reset
   double* h_stats = nullptr;  // pinned [8]
@@ -343,6 +344,23 @@ OverlapArgs overlap_args(ps2_ctx* c, const void* win, void* filt) {
   o.n_inc = c->n_inc;
   o.nwi = c->nwi;
   o.nwj = c->nwj;
+  return o;
+}
+
+// The loop's CLAP in the context's form: windows into the window stack and
+// the overlap-add pass, or window blocks into the partials and the combine
+// pass (the same sums in another association: the forms agree to the last bit
+// wherever the FP64 partial sums are exact, as they are for the window values
+// of a patch). The adjoint keeps the window stack its backward pass reads.
+ClapArgs clap_args_loop(ps2_ctx* c, const void* grid, int fused) {
+  ClapArgs a = clap_args(c, grid, fused ? nullptr : c->win.p);
+  if (fused) a.part = c->wpart.p;
+  return a;
+}
+
+OverlapArgs overlap_args_loop(ps2_ctx* c, void* filt, int fused) {
+  OverlapArgs o = overlap_args(c, fused ? nullptr : c->win.p, filt);
+  if (fused) o.part = c->wpart.p;
   return o;
 }
 
@@ -443,8 +461,8 @@ int enqueue_iteration(ps2_ctx* c, bool later, bool force_continue, cudaEvent_t* 
   CK(launch_bin(bin_args(c, 0, c->K[0].p), fp64, c->sm_count, c->st));
   ++launched;
   if (ev) CK(cudaEventRecord(ev[1], c->st));
-  CK(launch_clap(clap_args(c, c->grid.p, c->win.p), fp64, c->twf, c->twd, c->sm_count, c->st));
-  OverlapArgs ov = overlap_args(c, c->win.p, c->filt.p);
+  CK(launch_clap(clap_args_loop(c, c->grid.p, c->clap_fused), fp64, c->twf, c->twd, c->sm_count, c->st));
+  OverlapArgs ov = overlap_args_loop(c, c->filt.p, c->clap_fused);
   ov.normalize = fp64 ? 0 : 1;
   CK(launch_overlap(ov, fp64, c->st));
   launched += 2;
@@ -604,7 +622,7 @@ void ps2_destroy(ps2_ctx* c) {
   cudaSetDevice(c->device);
   if (c->st) cudaStreamSynchronize(c->st);
   DevBuf* bufs[] = {&c->ph_nm, &c->bp, &c->amp, &c->perm, &c->cell_start, &c->cell_of, &c->w0, &c->K[0], &c->K[1],
-                    &c->w, &c->coh, &c->C, &c->nopt, &c->grid, &c->win, &c->filt, &c->low_pass, &c->wscaled,
+                    &c->w, &c->coh, &c->C, &c->nopt, &c->grid, &c->win, &c->wpart, &c->filt, &c->low_pass, &c->wscaled,
                     &c->taps, &c->lut, &c->nr0, &c->nr_scaled, &c->state, &c->stats, &c->hist, &c->n_invalid,
                     &c->rms_partial, &c->ph_res, &c->scratch, &c->stage, &c->ad_ph, &c->ad_K, &c->ad_w,
                     &c->ad_coh, &c->ad_grid, &c->ad_win, &c->ad_filt, &c->ad_gfilt, &c->ad_gph, &c->ad_gK,
@@ -774,7 +792,10 @@ int ps2_load_patch(ps2_ctx* c, const ps2_patch_desc* d) {
   CK(c->grid.alloc(Cz * G * c->Mp));
   CK(c->filt.alloc(Cz * G * c->Mp));
   const int64_t W = static_cast<int64_t>(nwi) * nwj;
+  // CLAP's window stack (two-pass form) and window-block partial sums (fused
+  // form, complex FP64): the launch shapes choose the form
   CK(c->win.alloc(Cz * std::max<int64_t>(W, 1) * c->n_win * c->n_win * c->Mp));
+  CK(c->wpart.alloc(sizeof(double) * 2 * clap_part_elems(nwi, nwj, c->n_win, c->Mp)));
   if (W == 0) CK(cudaMemsetAsync(c->filt.p, 0, Cz * G * c->Mp, c->st));
   std::vector<double> ws = window_weight_scaled(c->n_win, 32);
   CK(c->wscaled.alloc(sizeof(double) * ws.size()));
@@ -796,6 +817,7 @@ int ps2_load_patch(ps2_ctx* c, const ps2_patch_desc* d) {
     c->clap_nw = ts.clap_nw;
     c->clap_bps = ts.clap_bps;
     c->bin_bps = ts.bin_bps;
+    c->clap_fused = ts.clap_fused;
   }
   CK(cudaMemsetAsync(c->filt.p, 0, Cz * G * c->Mp, c->st));
   CK(c->rms_partial.alloc(sizeof(double) * c->topo_blocks));
@@ -1035,25 +1057,35 @@ int ps2_autotune(ps2_ctx* c, int32_t* chosen_lanes, double* ms_per_candidate) {
   } else if (chosen_lanes) {
     *chosen_lanes = 0;
   }
-  // CLAP warps per block and resident blocks per SM, into the window scratch
-  // (the loop recomputes it every iteration)
+  // CLAP form, warps per block and resident blocks per SM, each timed with its
+  // second pass (overlap-add or combine) into the filtered grid the loop
+  // rewrites every iteration
   {
     const int nws[2] = {8, 4}, bpss[2] = {0, 1};
     double best_ms = 1e300;
-    for (int a = 0; a < (c->fp64 ? 1 : 2); ++a)
-      for (int b = 0; b < 2; ++b) {
-        ClapArgs ca = clap_args(c, c->grid.p, c->win.p);
-        ca.nw_block = c->fp64 ? 0 : nws[a];
-        ca.blocks_per_sm = bpss[b];
-        double ms = 0;
-        rc = timed([&] { return launch_clap(ca, c->fp64, c->twf, c->twd, c->sm_count, c->st); }, &ms);
-        if (rc) return rc;
-        if (ms < best_ms) {
-          best_ms = ms;
-          best.clap_nw = ca.nw_block;
-          best.clap_bps = bpss[b];
+    for (int f = 0; f < 2; ++f)
+      for (int a = 0; a < (c->fp64 ? 1 : 2); ++a)
+        for (int b = 0; b < 2; ++b) {
+          ClapArgs ca = clap_args_loop(c, c->grid.p, f);
+          ca.nw_block = c->fp64 ? 0 : nws[a];
+          ca.blocks_per_sm = bpss[b];
+          OverlapArgs ov = overlap_args_loop(c, c->filt.p, f);
+          ov.normalize = c->fp64 ? 0 : 1;
+          double ms = 0;
+          rc = timed(
+              [&] {
+                const cudaError_t e = launch_clap(ca, c->fp64, c->twf, c->twd, c->sm_count, c->st);
+                return e != cudaSuccess ? e : launch_overlap(ov, c->fp64, c->st);
+              },
+              &ms);
+          if (rc) return rc;
+          if (ms < best_ms) {
+            best_ms = ms;
+            best.clap_nw = ca.nw_block;
+            best.clap_bps = bpss[b];
+            best.clap_fused = f;
+          }
         }
-      }
   }
   // binning resident blocks per SM, mode 0 into a scratch grid
   {
@@ -1078,6 +1110,7 @@ int ps2_autotune(ps2_ctx* c, int32_t* chosen_lanes, double* ms_per_candidate) {
   c->clap_nw = best.clap_nw;
   c->clap_bps = best.clap_bps;
   c->bin_bps = best.bin_bps;
+  c->clap_fused = best.clap_fused;
   drop_loop_graph(c);  // the captured loop holds the previous shapes
   tune_store(tune_key(c->M, c->N, c->fp64), best);
   if (chosen_lanes && !c->fp64) *chosen_lanes = best.lanes;
@@ -1091,16 +1124,19 @@ int ps2_launch_shapes(ps2_ctx* c, int32_t* get, const int32_t* set) {
     get[1] = c->clap_nw;
     get[2] = c->clap_bps;
     get[3] = c->bin_bps;
+    get[4] = c->clap_fused;
   }
   if (set) {
     if (!(set[0] == 0 || set[0] == 4 || set[0] == 8 || set[0] == 16 || set[0] == 32) ||
-        !(set[1] == 0 || set[1] == 4 || set[1] == 8) || set[2] < 0 || set[3] < 0)
-      return set_err(PS2_ERR_INVALID_ARG, "ps2_launch_shapes: lanes 0/4/8/16/32, CLAP warps 0/4/8, blocks per SM >= 0");
+        !(set[1] == 0 || set[1] == 4 || set[1] == 8) || set[2] < 0 || set[3] < 0 || (set[4] != 0 && set[4] != 1))
+      return set_err(PS2_ERR_INVALID_ARG,
+                     "ps2_launch_shapes: lanes 0/4/8/16/32, CLAP warps 0/4/8, blocks per SM >= 0, CLAP form 0/1");
     if (c->fp64 && set[1] == 8) return set_err(PS2_ERR_UNSUPPORTED, "ps2_launch_shapes: FP64 CLAP runs 4 warps");
     c->topo_lanes = set[0];
     c->clap_nw = set[1];
     c->clap_bps = set[2];
     c->bin_bps = set[3];
+    c->clap_fused = set[4];
     drop_loop_graph(c);
   }
   return PS2_OK;
@@ -1949,8 +1985,8 @@ int ps2_batch_run(ps2_ctx* const* ctxs, int64_t n, ps2_iter_stats* last) {
     ps2_ctx* c = ctxs[p];
     PatchDev& d = plan.patch[p];
     d.bin = bin_args(c, 0, c->K[0].p);
-    d.clap = clap_args(c, c->grid.p, c->win.p);
-    d.ov = overlap_args(c, c->win.p, c->filt.p);
+    d.clap = clap_args_loop(c, c->grid.p, c->clap_fused);
+    d.ov = overlap_args_loop(c, c->filt.p, c->clap_fused);
     d.ov.normalize = 1;
     d.topo = topo_args(c, c->K[0].p, c->C.p, c->coh.p);
     d.fin = finalize_args(c, false);
@@ -1968,7 +2004,9 @@ int ps2_batch_run(ps2_ctx* const* ctxs, int64_t n, ps2_iter_stats* last) {
       plan.units[cls].push_back(vb);
     }
     plan.bin_prefix.push_back(plan.bin_prefix.back() + c->G * c->nchunk);
-    plan.clap_prefix.push_back(plan.clap_prefix.back() + static_cast<int64_t>(c->nwi) * c->nwj * (c->Mp / 4));
+    const int64_t clap_units = c->clap_fused ? static_cast<int64_t>(clap_block_count(c->nwi)) * clap_block_count(c->nwj)
+                                             : static_cast<int64_t>(c->nwi) * c->nwj;
+    plan.clap_prefix.push_back(plan.clap_prefix.back() + clap_units * (c->Mp / 4));
     plan.ov_prefix.push_back(plan.ov_prefix.back() + c->G * c->Mp);
     cap_iter = std::max<int64_t>(cap_iter, std::max<int64_t>(c->max_iter, 1) + 1);
   }
@@ -2432,14 +2470,22 @@ int ps2_shard_filter(ps2_ctx* c, const void* d_grid, int64_t cell_lo, int64_t ce
       }
     }
     if (ix_lo >= 0) {
-      ClapArgs ca = clap_args(c, c->grid.p, c->win.p);
-      ca.w_lo = ix_lo * c->nwj;
-      ca.w_n = (ix_hi - ix_lo + 1) * c->nwj;
+      ClapArgs ca = clap_args_loop(c, c->grid.p, c->clap_fused);
+      if (c->clap_fused) {
+        // whole window blocks: every block holding one of those windows, so each
+        // partial the combine reads is the one a whole-patch pass computes
+        const int64_t nbj = clap_block_count(c->nwj), b_lo = ix_lo / 4, b_hi = ix_hi / 4;
+        ca.w_lo = b_lo * nbj;
+        ca.w_n = (b_hi - b_lo + 1) * nbj;
+      } else {
+        ca.w_lo = ix_lo * c->nwj;
+        ca.w_n = (ix_hi - ix_lo + 1) * c->nwj;
+      }
       CK(launch_clap(ca, fp64, c->twf, c->twd, c->sm_count, c->st));
     }
   }
   if (cell_hi > cell_lo) {
-    OverlapArgs ov = overlap_args(c, c->win.p, c->filt.p);
+    OverlapArgs ov = overlap_args_loop(c, c->filt.p, c->clap_fused);
     ov.normalize = fp64 ? 0 : 1;
     ov.cell_lo = cell_lo;
     ov.cell_n = cell_hi - cell_lo;

@@ -685,58 +685,172 @@ __device__ __forceinline__ void clap_store_tiles(const ClapArgs& a, const Tile* 
   }
 }
 
-// One block-task of CLAP: window task / ngroups, interferograms
-// NW * (task % ngroups) + warp, ngroups = ceil(Mp / NW).
+// Interferogram groups of a CLAP unit (window or window block): a task is
+// (unit, group), group g holding interferograms NW * g .. NW * g + NW - 1.
 template <typename R, int NW>
 __device__ __forceinline__ int clap_groups(const ClapArgs& a) {
   return (a.Mp + NW - 1) / NW;
 }
 
+// Window (ix1, ix2) of interferograms NW * g + warp through the block's
+// tiles: clap_windows' corner (native_stage2.rs:957-995) returned in i1, j1;
+// on exit the tiles hold the weighted filtered window (rows, columns < nw).
 template <typename R, int NW, int NWIN = 0>
-__device__ __forceinline__ void clap_task(const ClapArgs& a, const int64_t task,
-                                          ClapTileT<R, ClapShape<NW>::kPad>* tiles, const typename CT<R>::C* twf,
-                                          const typename CT<R>::C* twi, const R* lp, const R* wt, const R (&g7)[7]) {
+__device__ __forceinline__ void clap_compute_window(const ClapArgs& a, const int ix1, const int ix2, const int g,
+                                                    ClapTileT<R, ClapShape<NW>::kPad>* tiles,
+                                                    const typename CT<R>::C* twf, const typename CT<R>::C* twi,
+                                                    const R* lp, const R* wt, const R (&g7)[7], int& i1, int& j1) {
   using C = typename CT<R>::C;
   constexpr int NT = 32 * NW;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nw = NWIN > 0 ? NWIN : a.n_win, nw2 = nw * nw;
   const int n_inc = nw / 4 > 1 ? nw / 4 : 1;
-  const int ngroups = clap_groups<R, NW>(a);
   const C* __restrict__ grid = static_cast<const C*>(a.grid);
-  C* __restrict__ out = static_cast<C*>(a.win_out);
   auto& T = tiles[warp];
-  {
-    const int64_t wi = a.w_lo + task / ngroups;
-    const int g = static_cast<int>(task - wi * ngroups);
-    const int ix1 = static_cast<int>(wi / a.nwj), ix2 = static_cast<int>(wi - static_cast<int64_t>(ix1) * a.nwj);
-    // clap_windows (native_stage2.rs:957-995)
-    int i1 = ix1 * n_inc, rs = 0;
-    if (i1 + nw > a.n_i) {
-      rs = i1 + nw - a.n_i;
-      i1 = a.n_i - nw;
-    }
-    int j1 = ix2 * n_inc, cs = 0;
-    if (j1 + nw > a.n_j) {
-      cs = j1 + nw - a.n_j;
-      j1 = a.n_j - nw;
-    }
-    __syncthreads();
-    // zero the padding of the tiles (none for a 32-pixel window)
-    if (NWIN == 0 && nw < 32) {
-      for (int idx = tid; idx < NW * 32 * 32; idx += NT) {
-        const int q = idx >> 10, e = idx & 1023, r = e >> 5, cc = e & 31;
-        if (r >= nw || cc >= nw) {
-          tiles[q].re[r][cc] = R(0);
-          tiles[q].im[r][cc] = R(0);
-        }
+  i1 = ix1 * n_inc;
+  int rs = 0;
+  if (i1 + nw > a.n_i) {
+    rs = i1 + nw - a.n_i;
+    i1 = a.n_i - nw;
+  }
+  j1 = ix2 * n_inc;
+  int cs = 0;
+  if (j1 + nw > a.n_j) {
+    cs = j1 + nw - a.n_j;
+    j1 = a.n_j - nw;
+  }
+  __syncthreads();
+  // zero the padding of the tiles (none for a 32-pixel window)
+  if (NWIN == 0 && nw < 32) {
+    for (int idx = tid; idx < NW * 32 * 32; idx += NT) {
+      const int q = idx >> 10, e = idx & 1023, r = e >> 5, cc = e & 31;
+      if (r >= nw || cc >= nw) {
+        tiles[q].re[r][cc] = R(0);
+        tiles[q].im[r][cc] = R(0);
       }
     }
-    const uint32_t inv_nw = (65536u + static_cast<uint32_t>(nw) - 1u) / static_cast<uint32_t>(nw);
-    clap_load_tiles<R, NW>(a, tiles, grid, i1, j1, g, nw, nw2, inv_nw, tid);
-    __syncthreads();
-    if (NW * g + warp < a.M) clap_window_warp<R, NWIN>(T, lane, a, twf, twi, lp, wt, g7, rs, cs);
-    __syncthreads();
-    clap_store_tiles<R, NW>(a, tiles, out, wi, g, nw, nw2, inv_nw, tid);
+  }
+  const uint32_t inv_nw = (65536u + static_cast<uint32_t>(nw) - 1u) / static_cast<uint32_t>(nw);
+  clap_load_tiles<R, NW>(a, tiles, grid, i1, j1, g, nw, nw2, inv_nw, tid);
+  __syncthreads();
+  if (NW * g + warp < a.M) clap_window_warp<R, NWIN>(T, lane, a, twf, twi, lp, wt, g7, rs, cs);
+  __syncthreads();
+}
+
+// One block-task of the window-stack form: window a.w_lo + task / ngroups; the
+// weighted window goes to win_out for the overlap-add pass.
+template <typename R, int NW, int NWIN = 0>
+__device__ __forceinline__ void clap_task(const ClapArgs& a, const int64_t task,
+                                          ClapTileT<R, ClapShape<NW>::kPad>* tiles, const typename CT<R>::C* twf,
+                                          const typename CT<R>::C* twi, const R* lp, const R* wt, const R (&g7)[7]) {
+  const int ngroups = clap_groups<R, NW>(a);
+  const int nw = NWIN > 0 ? NWIN : a.n_win, nw2 = nw * nw;
+  const int64_t wi = a.w_lo + task / ngroups;
+  const int g = static_cast<int>(task - (wi - a.w_lo) * ngroups);
+  const int ix1 = static_cast<int>(wi / a.nwj), ix2 = static_cast<int>(wi - static_cast<int64_t>(ix1) * a.nwj);
+  int i1, j1;
+  clap_compute_window<R, NW, NWIN>(a, ix1, ix2, g, tiles, twf, twi, lp, wt, g7, i1, j1);
+  const uint32_t inv_nw = (65536u + static_cast<uint32_t>(nw) - 1u) / static_cast<uint32_t>(nw);
+  clap_store_tiles<R, NW>(a, tiles, static_cast<typename CT<R>::C*>(a.win_out), wi, g, nw, nw2, inv_nw,
+                          threadIdx.x);
+}
+
+// ---- overlap-add fused into the window pass (window blocks) -------------------
+// The windows are taken in blocks of 4 x 4 (window rows 4 bi .. 4 bi + 3,
+// columns 4 bj .. 4 bj + 3). A block's windows cover a box of at most
+// clap_box(n_win) = 3 n_inc + n_win cells a side from the corner of its first
+// window; one block-task runs the block's windows in order (ix1, then ix2) for
+// NW interferograms and adds each weighted window into the block's FP64
+// partial sum of the box (part: [block][box row][box column][Mp] of complex
+// FP64; the first window of the block that covers a cell stores instead of
+// adding), so a cell's partial is the reference's ordered sum
+// (native_stage2.rs:1166-1184) over the block's windows. The combine pass
+// adds a cell's block partials (2 x 2 at most for 24-cell windows) in block
+// order and rounds once. The window stack of the two-pass form (1.1 GB for a
+// 256 x 256 x 150 grid) is never written; the partials are 2.7x the grid and a
+// block's box stays in L2 while its windows run.
+constexpr int kClapBlockWin = 4;
+__host__ __device__ inline int clap_box(int n_win) {
+  const int n_inc = n_win / 4 > 1 ? n_win / 4 : 1;
+  return (kClapBlockWin - 1) * n_inc + n_win;
+}
+__host__ __device__ inline int clap_block_rows(int nw_axis) { return (nw_axis + kClapBlockWin - 1) / kClapBlockWin; }
+
+// Add (or store, for a cell no earlier window of the block covered) the
+// weighted window in the tiles to the block partial. Box corner (r0, c0); pi1 /
+// pj1 the corner row / column of the block's previous window row / column
+// (rows < pi1 + nw were covered already), or a value that marks none. One item
+// per (pixel, interferogram): NW consecutive threads write one cell's NW
+// interferograms, 16 * NW contiguous bytes; each thread issues the partial
+// loads of kAccBatch items before any add, so their L2 round trips overlap.
+constexpr int kAccBatch = 6;
+template <typename R, int NW, typename Tile>
+__device__ __forceinline__ void clap_accum_tiles(const ClapArgs& a, const Tile* tiles, double2* __restrict__ part,
+                                                 const int64_t blk, const int box, const int i1, const int j1,
+                                                 const int r0, const int c0, const int pi1, const int pj1,
+                                                 const int g, const int nw, const int nw2, const uint32_t inv_nw,
+                                                 const int tid) {
+  constexpr int NT = 32 * NW;
+  const int n_items = nw2 * NW;
+  for (int b0 = tid; b0 < n_items; b0 += NT * kAccBatch) {
+    double2 old[kAccBatch];
+    int64_t off[kAccBatch];
+    int li[kAccBatch], lj[kAccBatch], qq[kAccBatch];
+    bool live[kAccBatch], first[kAccBatch];
+#pragma unroll
+    for (int u = 0; u < kAccBatch; ++u) {
+      const int idx = b0 + u * NT;
+      const int pix = idx / NW, q = idx - (idx / NW) * NW;
+      const int c = NW * g + q;
+      live[u] = idx < n_items && c < a.M;
+      li[u] = static_cast<int>((static_cast<uint32_t>(pix) * inv_nw) >> 16);
+      lj[u] = pix - li[u] * nw;
+      qq[u] = q;
+      const int ai = i1 + li[u], aj = j1 + lj[u];
+      first[u] = ai >= pi1 + nw && aj >= pj1 + nw;
+      off[u] = ((blk * box + (ai - r0)) * box + (aj - c0)) * a.Mp + c;
+      old[u] = make_double2(0.0, 0.0);
+      if (live[u] && !first[u]) old[u] = part[off[u]];
+    }
+#pragma unroll
+    for (int u = 0; u < kAccBatch; ++u) {
+      if (!live[u]) continue;
+      const double vx = static_cast<double>(tiles[qq[u]].re[li[u]][lj[u]]);
+      const double vy = static_cast<double>(tiles[qq[u]].im[li[u]][lj[u]]);
+      part[off[u]] = first[u] ? make_double2(vx, vy) : make_double2(__dadd_rn(old[u].x, vx), __dadd_rn(old[u].y, vy));
+    }
+  }
+}
+
+// One block-task of the fused form: window block a.w_lo + task / ngroups.
+template <typename R, int NW, int NWIN = 0>
+__device__ __forceinline__ void clap_block_task(const ClapArgs& a, const int64_t task,
+                                                ClapTileT<R, ClapShape<NW>::kPad>* tiles,
+                                                const typename CT<R>::C* twf, const typename CT<R>::C* twi,
+                                                const R* lp, const R* wt, const R (&g7)[7]) {
+  const int ngroups = clap_groups<R, NW>(a);
+  const int nw = NWIN > 0 ? NWIN : a.n_win, nw2 = nw * nw;
+  const int n_inc = nw / 4 > 1 ? nw / 4 : 1;
+  const int box = clap_box(nw);
+  const int nbj = clap_block_rows(a.nwj);
+  const int64_t blk = a.w_lo + task / ngroups;
+  const int g = static_cast<int>(task - (blk - a.w_lo) * ngroups);
+  const int bi = static_cast<int>(blk / nbj), bj = static_cast<int>(blk - static_cast<int64_t>(bi) * nbj);
+  const int ixa = kClapBlockWin * bi, ixb = min(ixa + kClapBlockWin, a.nwi);
+  const int jxa = kClapBlockWin * bj, jxb = min(jxa + kClapBlockWin, a.nwj);
+  const int r0 = min(ixa * n_inc, a.n_i - nw), c0 = min(jxa * n_inc, a.n_j - nw);
+  const uint32_t inv_nw = (65536u + static_cast<uint32_t>(nw) - 1u) / static_cast<uint32_t>(nw);
+  double2* part = static_cast<double2*>(a.part);
+  constexpr int kNone = -(1 << 20);
+  for (int ix1 = ixa; ix1 < ixb; ++ix1) {
+    const int pi1 = ix1 > ixa ? min((ix1 - 1) * n_inc, a.n_i - nw) : kNone;
+    for (int ix2 = jxa; ix2 < jxb; ++ix2) {
+      const int pj1 = ix2 > jxa ? min((ix2 - 1) * n_inc, a.n_j - nw) : kNone;
+      int i1, j1;
+      clap_compute_window<R, NW, NWIN>(a, ix1, ix2, g, tiles, twf, twi, lp, wt, g7, i1, j1);
+      clap_accum_tiles<R, NW>(a, tiles, part, blk, box, i1, j1, r0, c0, pi1, pj1, g, nw, nw2, inv_nw,
+                              threadIdx.x);
+    }
   }
 }
 
@@ -765,18 +879,30 @@ __device__ __forceinline__ ClapSmem<R, NW> clap_smem(unsigned char* raw, const t
   return m;
 }
 
-template <typename R, int NW, int NWIN>
-__global__ void __launch_bounds__(32 * NW) k_clap(ClapArgs a, typename CT<R>::Tw tw) {
+// FUSED: window blocks into the partials (the loop's form); otherwise windows
+// into the window stack. FP32 blocks are held to the registers that let as
+// many of them reside as their shared memory does (two of eight warps, three
+// of four).
+template <typename R, int NW, int NWIN, bool FUSED>
+__global__ void __launch_bounds__(32 * NW, sizeof(R) == 4 ? (NW == 8 ? 2 : 3) : 1)
+    k_clap(ClapArgs a, typename CT<R>::Tw tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const ClapSmem<R, NW> m = clap_smem<R, NW>(smem_raw, tw);
   clap_consts<R>(a, m.lp, m.wt);
   R g7[7];
 #pragma unroll
   for (int i = 0; i < 7; ++i) g7[i] = static_cast<R>(a.g7[i]);
-  const int64_t nwin = a.w_n > 0 ? a.w_n : static_cast<int64_t>(a.nwi) * a.nwj;
-  const int64_t ntask = nwin * clap_groups<R, NW>(a);
-  for (int64_t task = blockIdx.x; task < ntask; task += gridDim.x)
-    clap_task<R, NW, NWIN>(a, task, m.tiles, m.twf, m.twi, m.lp, m.wt, g7);
+  // units: window blocks (fused) or windows (window stack)
+  const int64_t nunit = a.w_n > 0 ? a.w_n
+                        : FUSED ? static_cast<int64_t>(clap_block_rows(a.nwi)) * clap_block_rows(a.nwj)
+                                : static_cast<int64_t>(a.nwi) * a.nwj;
+  const int64_t ntask = nunit * clap_groups<R, NW>(a);
+  for (int64_t task = blockIdx.x; task < ntask; task += gridDim.x) {
+    if constexpr (FUSED)
+      clap_block_task<R, NW, NWIN>(a, task, m.tiles, m.twf, m.twi, m.lp, m.wt, g7);
+    else
+      clap_task<R, NW, NWIN>(a, task, m.tiles, m.twf, m.twi, m.lp, m.wt, g7);
+  }
 }
 
 template <typename R, int NW>
@@ -786,18 +912,27 @@ static size_t clap_smem_bytes() {
 
 template <typename R, int NW, int NWIN>
 static cudaError_t launch_clap_nwin(const ClapArgs& a, const typename CT<R>::Tw& tw, int sm_count, cudaStream_t st) {
-  const int64_t nwin = a.w_n > 0 ? a.w_n : static_cast<int64_t>(a.nwi) * a.nwj;
-  const int64_t ntask = nwin * ((a.Mp + NW - 1) / NW);
+  if (a.nwi <= 0 || a.nwj <= 0) return cudaSuccess;
+  const int64_t nunit = a.w_n > 0 ? a.w_n
+                        : a.part ? static_cast<int64_t>(clap_block_rows(a.nwi)) * clap_block_rows(a.nwj)
+                                 : static_cast<int64_t>(a.nwi) * a.nwj;
+  const int64_t ntask = nunit * ((a.Mp + NW - 1) / NW);
   if (ntask <= 0) return cudaSuccess;
   const size_t sm = clap_smem_bytes<R, NW>();
   cudaError_t e = kernel_attributes_once(sm);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clap<R, NW, NWIN>, 32 * NW, sm);
+  if (a.part)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clap<R, NW, NWIN, true>, 32 * NW, sm);
+  else
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clap<R, NW, NWIN, false>, 32 * NW, sm);
   if (e != cudaSuccess) return e;
   if (a.blocks_per_sm > 0 && a.blocks_per_sm < per_sm) per_sm = a.blocks_per_sm;
   const int64_t blocks = std::min<int64_t>(ntask, static_cast<int64_t>(sm_count) * (per_sm > 0 ? per_sm : 1));
-  k_clap<R, NW, NWIN><<<static_cast<unsigned>(blocks), 32 * NW, sm, st>>>(a, tw);
+  if (a.part)
+    k_clap<R, NW, NWIN, true><<<static_cast<unsigned>(blocks), 32 * NW, sm, st>>>(a, tw);
+  else
+    k_clap<R, NW, NWIN, false><<<static_cast<unsigned>(blocks), 32 * NW, sm, st>>>(a, tw);
   return cudaGetLastError();
 }
 
@@ -873,13 +1008,63 @@ __device__ __forceinline__ void overlap_elem(const OverlapArgs& a, const int64_t
   }
 }
 
+// Fused form: the cell's block partials (those whose boxes hold the cell: 2 x 2
+// at most for 24-cell windows) added in block order in FP64, then rounded and
+// normalised as overlap_elem does.
+template <typename R>
+__device__ __forceinline__ void combine_elem(const OverlapArgs& a, const int64_t idx) {
+  using C = typename CT<R>::C;
+  const double2* __restrict__ part = static_cast<const double2*>(a.part);
+  C* __restrict__ filt = static_cast<C*>(a.filt);
+  const int nw = a.n_win, box = clap_box(nw);
+  const int64_t cell = idx / a.Mp;
+  const int c = static_cast<int>(idx - cell * a.Mp);
+  const int i = static_cast<int>(cell / a.n_j), j = static_cast<int>(cell - static_cast<int64_t>(i) * a.n_j);
+  double sx = 0.0, sy = 0.0;
+  if (c < a.M && a.nwi > 0 && a.nwj > 0) {
+    const int nbi = clap_block_rows(a.nwi), nbj = clap_block_rows(a.nwj);
+    // blocks whose boxes [corner of the first window, corner of the last + nw)
+    // hold (i, j), in block order: the box corners do not decrease along an
+    // axis, and no box that holds i starts before block (i - nw) / (4 n_inc) - 1
+    const int bj_lo = max(0, (j - nw) / (kClapBlockWin * a.n_inc) - 1);
+    for (int bi = max(0, (i - nw) / (kClapBlockWin * a.n_inc) - 1); bi < nbi; ++bi) {
+      const int r0 = min(kClapBlockWin * bi * a.n_inc, a.n_i - nw);
+      if (r0 > i) break;
+      const int r1 = min((min(kClapBlockWin * bi + kClapBlockWin, a.nwi) - 1) * a.n_inc, a.n_i - nw) + nw;
+      if (i >= r1) continue;
+      for (int bj = bj_lo; bj < nbj; ++bj) {
+        const int c0 = min(kClapBlockWin * bj * a.n_inc, a.n_j - nw);
+        if (c0 > j) break;
+        const int c1 = min((min(kClapBlockWin * bj + kClapBlockWin, a.nwj) - 1) * a.n_inc, a.n_j - nw) + nw;
+        if (j >= c1) continue;
+        const int64_t blk = static_cast<int64_t>(bi) * nbj + bj;
+        const double2 p = part[((blk * box + (i - r0)) * box + (j - c0)) * a.Mp + c];
+        sx = __dadd_rn(sx, p.x);
+        sy = __dadd_rn(sy, p.y);
+      }
+    }
+  }
+  C f = mk(static_cast<R>(sx), static_cast<R>(sy));
+  if constexpr (sizeof(R) == 4) {
+    if (a.normalize) {
+      const float mag = hypotf(f.x, f.y);
+      if (mag != 0.f) f = make_float2(f.x / mag, f.y / mag);
+    }
+  }
+  filt[idx] = f;
+}
+
 template <typename R>
 __global__ void __launch_bounds__(256) k_overlap(OverlapArgs a) {
   const int64_t cells = a.cell_n > 0 ? a.cell_n : static_cast<int64_t>(a.n_i) * a.n_j;
   const int64_t total = cells * a.Mp, base = a.cell_lo * a.Mp;
   for (int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
-       idx += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    overlap_elem<R>(a, base + idx);
+       idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    if (a.part)
+      combine_elem<R>(a, base + idx);
+    else
+      overlap_elem<R>(a, base + idx);
+  }
 }
 
 cudaError_t launch_overlap(const OverlapArgs& a, bool fp64, cudaStream_t st) {
@@ -1894,6 +2079,13 @@ int topofit_lanes(int M) {
   int L = 4;
   while (L < 32 && L * 24 < M) L *= 2;
   return L;
+}
+
+int clap_block_count(int nw_axis) { return clap_block_rows(nw_axis); }
+
+int64_t clap_part_elems(int nwi, int nwj, int n_win, int Mp) {
+  const int64_t box = clap_box(n_win);
+  return std::max<int64_t>(static_cast<int64_t>(clap_block_rows(nwi)) * clap_block_rows(nwj), 1) * box * box * Mp;
 }
 
 size_t topofit_smem_bytes(int L, int mpad, int n_half) {
@@ -2939,7 +3131,10 @@ __global__ void __launch_bounds__(128) k_batch_clap(BatchArgs b, Twiddles32f tw)
       for (int i = 0; i < 7; ++i) g7[i] = static_cast<float>(a.g7[i]);
       cur = p;
     }
-    clap_task<float, 4>(a, u - b.clap_prefix[p], m.tiles, m.twf, m.twi, m.lp, m.wt, g7);
+    if (a.part)
+      clap_block_task<float, 4>(a, u - b.clap_prefix[p], m.tiles, m.twf, m.twi, m.lp, m.wt, g7);
+    else
+      clap_task<float, 4>(a, u - b.clap_prefix[p], m.tiles, m.twf, m.twi, m.lp, m.wt, g7);
   }
 }
 
@@ -2949,7 +3144,10 @@ __global__ void __launch_bounds__(256) k_batch_overlap(BatchArgs b) {
        u += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int p = find_patch(b.ov_prefix, b.P, u);
     if (!b.active[p]) continue;
-    overlap_elem<float>(b.patch[p].ov, u - b.ov_prefix[p]);
+    if (b.patch[p].ov.part)
+      combine_elem<float>(b.patch[p].ov, u - b.ov_prefix[p]);
+    else
+      overlap_elem<float>(b.patch[p].ov, u - b.ov_prefix[p]);
   }
 }
 
@@ -3742,12 +3940,18 @@ cudaError_t kernel_attributes_once(size_t dynamic_smem) {
     const cudaError_t r = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const cudaError_t steps[] = {
         r,
-        r == cudaSuccess ? opt_in_smem(k_clap<float, 8, 0>, optin) : r,
-        r == cudaSuccess ? opt_in_smem(k_clap<double, 4, 0>, optin) : r,
-        r == cudaSuccess ? opt_in_smem(k_clap<float, 8, 24>, optin) : r,
-        r == cudaSuccess ? opt_in_smem(k_clap<float, 4, 0>, optin) : r,
-        r == cudaSuccess ? opt_in_smem(k_clap<float, 4, 24>, optin) : r,
-        r == cudaSuccess ? opt_in_smem(k_clap<double, 4, 24>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<float, 8, 0, false>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<double, 4, 0, false>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<float, 8, 24, false>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<float, 4, 0, false>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<float, 4, 24, false>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<double, 4, 24, false>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<float, 8, 0, true>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<double, 4, 0, true>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<float, 8, 24, true>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<float, 4, 0, true>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<float, 4, 24, true>, optin) : r,
+        r == cudaSuccess ? opt_in_smem(k_clap<double, 4, 24, true>, optin) : r,
         r == cudaSuccess ? opt_in_smem(k_topofit_f32<4>, optin) : r,
         r == cudaSuccess ? opt_in_smem(k_topofit_f32<8>, optin) : r,
         r == cudaSuccess ? opt_in_smem(k_topofit_f32<16>, optin) : r,

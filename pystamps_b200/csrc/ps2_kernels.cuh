@@ -46,14 +46,16 @@ struct ClapArgs {
   const double* low_pass;  // [32*32] natural FFT order (device)
   const double* wscaled;   // [n_win*n_win] pyramid weight / 1024 (device)
   double g7[7];            // 7-tap Gaussian of the |H| smoothing
-  void* win_out;           // complex [W, n_win*n_win, Mp]
-  int64_t w_lo, w_n;       // windows w_lo .. w_lo + w_n - 1 (w_n = 0: all windows)
+  void* win_out;           // complex [W, n_win*n_win, Mp] (window-stack form)
+  void* part;              // complex FP64 [window blocks, box, box, Mp] (fused form; win_out unused)
+  int64_t w_lo, w_n;       // windows (window blocks in the fused form) w_lo .. w_lo + w_n - 1 (w_n = 0: all)
   int nw_block;            // launch shape: warps (interferograms) per block, 4 or 8 (0: 8 in FP32, 4 in FP64)
   int blocks_per_sm;       // launch shape: resident blocks per SM (0: as many as fit)
 };
 
 struct OverlapArgs {
-  const void* win_out;  // complex [W, n_win*n_win, Mp]
+  const void* win_out;  // complex [W, n_win*n_win, Mp] (window-stack form)
+  const void* part;     // complex FP64 block partials of the fused form (win_out unused)
   void* filt;           // complex [G, Mp]
   int n_i, n_j, M, Mp, n_win, n_inc, nwi, nwj;
   int normalize;        // 1 (FP32 stage-2 loop): store f/|f|, the unit patch phase the topofit reads
@@ -219,6 +221,10 @@ cudaError_t launch_scatter_narrow(const double* src, float* dst, const int32_t* 
                                   cudaStream_t st);
 cudaError_t launch_reduce_ab(const double* part, int n, double* out, cudaStream_t st);
 size_t topofit_smem_bytes(int L, int mpad, int n_half);
+// complex FP64 elements of the fused CLAP's window-block partials
+int64_t clap_part_elems(int nwi, int nwj, int n_win, int Mp);
+// window blocks per axis (4 windows a side) of the fused CLAP
+int clap_block_count(int nw_axis);
 cudaError_t topofit_geometry(const TopoArgs& a, int grid_cap, int* L_out, int* mpad_out, int* blocks_out);
 cudaError_t launch_batch_reset(const BatchArgs& b, cudaStream_t st);
 cudaError_t launch_s3_clap(const S3ClapArgs& a, const Twiddles32f& tf, int sm_count, cudaStream_t st);

@@ -128,13 +128,16 @@ def halo_exchange(grid, plan, rank: int, n_cells: int, group=None) -> None:
 class ShardRank:
     """One rank's rows of a patch on one GPU, with the four shard calls."""
 
-    def __init__(self, p: PreparedPatch, lo: int, hi: int, *, device: int = 0, precision: str = "fp32"):
+    def __init__(self, p: PreparedPatch, lo: int, hi: int, *, device: int = 0, precision: str = "fp32",
+                 shapes=None):
         import torch
 
         self.lo, self.hi = int(lo), int(hi)
         self.sub, self.rows = shard_patch(p, lo, hi)
         self.ctx = Stage2Context(device)
         self.ctx.load(self.sub, precision)
+        if shapes is not None:  # launch shapes pinned (Stage2Context.launch_shapes)
+            self.ctx.launch_shapes(shapes)
         fp64 = self.ctx.precision == PRECISION_FP64
         mp = (p.n_ifg + 3) // 4 * 4
         self.grid = torch.zeros(p.n_i * p.n_j * mp * 2, dtype=torch.float64 if fp64 else torch.float32,
@@ -196,7 +199,7 @@ def iterate_shards(ranks: Sequence, sum_grids: Callable, sum_stats: Callable, n_
 
 
 def run_sharded_local(p: PreparedPatch, n_shards: int, *, device: int = 0, precision: str = "fp32",
-                      keys=("K_ps", "C_ps", "coh_ps", "N_opt"), exchange: str = "halo") -> dict:
+                      keys=("K_ps", "C_ps", "coh_ps", "N_opt"), exchange: str = "halo", shapes=None) -> dict:
     """All shards of a patch as contexts of this process on one GPU (ranks
     emulated: the halo slices copied between the ranks' grids, or the grids
     summed in rank order). Returns the per-PS keys in the whole patch's row
@@ -204,7 +207,7 @@ def run_sharded_local(p: PreparedPatch, n_shards: int, *, device: int = 0, preci
     import torch
 
     ranges = split_cells(p.grid_lin, p.n_i * p.n_j, n_shards)
-    ranks = [ShardRank(p, lo, hi, device=device, precision=precision) for lo, hi in ranges]
+    ranks = [ShardRank(p, lo, hi, device=device, precision=precision, shapes=shapes) for lo, hi in ranges]
     plan = halo_plan(ranges, p.n_i, p.n_j, p.clap_window)
     try:
         def sum_grids(gs):

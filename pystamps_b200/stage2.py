@@ -359,9 +359,10 @@ class Stage2Context:
 
     def launch_shapes(self, set_to=None) -> list[int]:
         """[topofit lanes, CLAP warps per block, CLAP blocks per SM, binning
-        blocks per SM] (ps2_launch_shapes; 0 = built-in rule); set_to pins them."""
-        get = (ctypes.c_int32 * 4)()
-        st = None if set_to is None else (ctypes.c_int32 * 4)(*[int(v) for v in set_to])
+        blocks per SM, CLAP form (0 window stack, 1 fused window blocks)]
+        (ps2_launch_shapes; 0 = built-in rule); set_to pins them."""
+        get = (ctypes.c_int32 * 5)()
+        st = None if set_to is None else (ctypes.c_int32 * 5)(*[int(v) for v in set_to])
         check(self._lib.ps2_launch_shapes(self._ctx, get, st))
         return list(get) if set_to is None else [int(v) for v in set_to]
 

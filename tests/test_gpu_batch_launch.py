@@ -52,6 +52,31 @@ def test_batch_matches_each_patch_alone(cuda_lib):
     assert n_launch == 8 * max(iters)
 
 
+def test_batch_with_both_clap_forms_matches_each_patch_alone(cuda_lib):
+    """Patches of one batch may use different CLAP forms (the context's launch
+    shape): window stack or fused window blocks, each as it runs alone."""
+    from pystamps_b200 import batch
+    from pystamps_b200 import stage2 as S
+
+    preps = _patches()[:4]
+    forms = [1, 0, 1, 1]
+    alone = []
+    for p, f in zip(preps, forms):
+        with S.Stage2Context() as c:
+            c.load(p, "fp32")
+            c.launch_shapes([0, 0, 0, 0, f])
+            c.run()
+            alone.append(c.download(KEYS))
+    with batch.Batch(preps) as b:
+        for c, f in zip(b.ctxs, forms):
+            c.launch_shapes([0, 0, 0, 0, f])
+        b.run()
+        together = b.download(KEYS)
+    for k, (a, t) in enumerate(zip(alone, together)):
+        for key in KEYS:
+            np.testing.assert_array_equal(t[key], a[key], err_msg=f"patch {k} {key}")
+
+
 def test_batch_rerun_after_reset_is_identical(cuda_lib):
     from pystamps_b200 import batch
 

@@ -7,18 +7,24 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("n_shards,row_variant,precision", [(3, True, "fp32"), (2, False, "fp32"), (4, True, "fp64")])
-def test_shards_match_one_context(cuda_lib, n_shards, row_variant, precision):
+@pytest.mark.parametrize("n_shards,row_variant,precision,clap_form",
+                         [(3, True, "fp32", 0), (2, False, "fp32", 0), (4, True, "fp64", 0), (3, True, "fp32", 1),
+                          (2, True, "fp64", 1)])
+def test_shards_match_one_context(cuda_lib, n_shards, row_variant, precision, clap_form):
+    """clap_form 1: every context runs the fused CLAP (window blocks): a shard
+    computes the whole blocks that hold its windows."""
     from pystamps_b200 import shard, stage2, synth
 
     patch = synth.make_patch(6000, 12, 30, 41, seed=77, n_rand=3000, gamma_max_iterations=6, row_variant=row_variant)
     prep = stage2.prepare_patch(patch)
     keys = ("K_ps", "C_ps", "coh_ps", "N_opt", "ph_grid")
+    shapes = [0, 0, 0, 0, clap_form]
     with stage2.Stage2Context() as c:
         c.load(prep, precision)
+        c.launch_shapes(shapes)
         st = c.run()
         one = c.download(keys)
-    got = shard.run_sharded_local(prep, n_shards, precision=precision, keys=keys)
+    got = shard.run_sharded_local(prep, n_shards, precision=precision, keys=keys, shapes=shapes)
     assert got["i_loop"] == one["i_loop"] == st["i_loop"]
     for k in ("K_ps", "C_ps", "coh_ps", "N_opt"):
         np.testing.assert_array_equal(got[k], one[k], err_msg=k)
