@@ -46,7 +46,7 @@ FP32_LANES_PER_SM = 128
 # capture (dram__bytes_read.sum + dram__bytes_write.sum) of the full-scale shape
 # with 250,000 PS x 150 ifg (256x256 grid): 537.4 MB per launch; the reported
 # traffic scales it by N x M.
-TOPOFIT_TRAFFIC_BYTES_PER_PS_IFG = 537.4e6 / (250_000 * 150)
+TOPOFIT_TRAFFIC_BYTES_PER_PS_IFG = 537.9e6 / (250_000 * 150)
 
 
 def parse():
