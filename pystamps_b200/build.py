@@ -9,7 +9,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 SOURCES = [CSRC / "ps2_kernels.cu", CSRC / "ps2_api.cu"]
-HEADERS = [CSRC / "ps2_kernels.cuh", CSRC / "ps2_device.cuh", CSRC / "interp10_taps.h", CSRC / "trial_interp_taps.h", CSRC / "sincos_poly.h",
+HEADERS = [CSRC / "ps2_kernels.cuh", CSRC / "ps2_device.cuh", CSRC / "interp10_taps.h", CSRC / "trial_interp_taps.h", CSRC / "sincos_poly.h", CSRC / "atan_poly.h",
            HERE.parent / "include" / "ps2cuda.h"]
 TARGET = HERE / "libps2cuda.so"
 

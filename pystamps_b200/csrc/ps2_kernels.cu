@@ -20,6 +20,7 @@
 
 #include "ps2_device.cuh"
 #include "ps2_kernels.cuh"
+#include "atan_poly.h"
 #include "sincos_poly.h"
 #include "trial_interp_taps.h"
 
@@ -64,6 +65,28 @@ __device__ __forceinline__ void sincos_cw(float x, float* s, float* c) {
   *c = ((q + 1) & 2) ? -c1 : c1;
 }
 __device__ __forceinline__ void sincos_r(float x, float* s, float* c) { sincos_cw(x, s, c); }
+
+// atan2(y, x) in FP32 for the topofit refinement's residual angles: t =
+// min(|x|, |y|) / max(|x|, |y|) in [0, 1], atan t by a minimax polynomial in
+// t^2 (atan_poly.h, fitted by make_atan_poly.py, 4.9e-8), then the octant's
+// reflections and the sign of y. Largest absolute error 3.1e-7 (near +-pi,
+// where an FP32 ulp is 2.4e-7); atan2(+-0, +0) = +-0, atan2(+-0, x < 0) = +-pi.
+__device__ __forceinline__ float atan2_poly(float y, float x) {
+  const float ax = fabsf(x), ay = fabsf(y);
+  const float mn = fminf(ax, ay), mx = fmaxf(ax, ay);
+  const float t = mx > 0.f ? __fdiv_rn(mn, mx) : 0.f;
+  const float u = t * t;
+  float p = fmaf(kAtanA7, u, kAtanA6);
+  p = fmaf(p, u, kAtanA5);
+  p = fmaf(p, u, kAtanA4);
+  p = fmaf(p, u, kAtanA3);
+  p = fmaf(p, u, kAtanA2);
+  p = fmaf(p, u, kAtanA1);
+  float r = fmaf(t * u, p, t);
+  if (ay > ax) r = kHalfPiF - r;
+  if (x < 0.f) r = kPiF - r;
+  return copysignf(r, y);
+}
 __device__ __forceinline__ void sincos_r(double x, double* s, double* c) { sincos(x, s, c); }
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
@@ -1811,7 +1834,7 @@ __device__ __forceinline__ void topofit_vblock_t(const TopoArgs& a, const int mp
       const double wb = __dmul_rn(wgt, static_cast<double>(cs.bp[c]));
       dl = __dadd_rn(dl, __dmul_rn(wb, wb));
       const float2 q = cmul_rn(make_float2(cs.rx[c], cs.ry[c]), oc);
-      mopt = __dadd_rn(mopt, __dmul_rn(wb, __dmul_rn(wgt, static_cast<double>(atan2f(q.y, q.x)))));
+      mopt = __dadd_rn(mopt, __dmul_rn(wb, __dmul_rn(wgt, static_cast<double>(atan2_poly(q.y, q.x)))));
     }
     mopt = group_sum<L>(mopt);
     dl = group_sum<L>(dl);
