@@ -132,7 +132,10 @@ def test_topofit_zero_columns_and_empty_rows(K, oracle):
     assert np.all(rg[cpx == 0] == 0)
 
 
-@pytest.mark.parametrize("m,ntw", [(20, 4.94), (60, 9.94), (150, 9.94), (3, 0.4), (33, 1.0)])
+# n_half = ceil(8 ntw): 40 and 88 take the full trial sweep, 41 .. 87 the
+# sampled one (every 4th trial exact, fractional-delay filters between)
+@pytest.mark.parametrize("m,ntw", [(20, 4.94), (60, 9.94), (150, 9.94), (3, 0.4), (33, 1.0), (60, 5.1),
+                                   (150, 10.8), (150, 10.9), (47, 7.6)])
 def test_topofit_random_rows_argmax_and_ties(K, oracle, m, ntw):
     rng = np.random.default_rng(m)
     n = 4000
@@ -146,6 +149,30 @@ def test_topofit_random_rows_argmax_and_ties(K, oracle, m, ntw):
     good = ~tie
     dK = np.abs(Kg - fr.K) / np.maximum(np.abs(fr.K), 1e-3)
     assert (dK[good] <= K_REL_TOL).mean() >= 0.999, (dK[good] > K_REL_TOL).sum()
+    assert np.abs(hg - fr.coh)[good].max() <= GAMMA_TOL
+
+
+@pytest.mark.parametrize("m,ntw", [(150, 9.94), (60, 5.1), (150, 10.8), (40, 7.6)])
+def test_topofit_peaks_at_the_end_trials(K, oracle, m, ntw):
+    """Rows whose best trial is the first or the last one (m = -n_half or
+    +n_half), where the sampled sweep's filters read samples beyond the trial
+    range, and rows one trial inside them: the same argmax and refined values
+    as the oracle."""
+    rng = np.random.default_rng(int(10 * ntw) + m)
+    n = 2000
+    n_half = math.ceil(8 * ntw)
+    bp = rng.uniform(-300, 300, (n, m))
+    rngbp = bp.max(axis=1) - bp.min(axis=1)
+    step = math.pi / 4 / rngbp  # K of one trial step, per row
+    edge = rng.choice([-n_half, n_half, -(n_half - 1), n_half - 1], n)
+    k = (edge + rng.uniform(-0.2, 0.2, n)) * step
+    cpx = np.exp(1j * (k[:, None] * bp + rng.normal(0, 0.3, (n, m)))).astype(np.complex64)
+    bp32 = bp.astype(np.float32).astype(np.float64)
+    Kg, Cg, hg, _ = K.run_native_topofit_rows(cpx, bp32, ntw)
+    fr = oracle.fit_rows(np.ones((n, m), np.complex64), cpx, bp32, ntw)
+    good = ~_tie_mask(fr.best_coh, fr.second_coh)
+    dK = np.abs(Kg - fr.K) / np.maximum(np.abs(fr.K), 1e-3)
+    assert (dK[good] <= K_REL_TOL).all(), (dK[good] > K_REL_TOL).sum()
     assert np.abs(hg - fr.coh)[good].max() <= GAMMA_TOL
 
 
