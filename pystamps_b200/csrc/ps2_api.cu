@@ -1160,34 +1160,23 @@ int ps2_download(ps2_ctx* c, ps2_outputs* o) {
   const size_t R = rsz(c), Cz = csz(c);
   const int32_t* perm = c->perm.as<int32_t>();
   const bool fp64 = c->fp64;
-  // per-PS vectors: scatter to the caller's order, widen to f64 on the host
-  auto fetch_vec = [&](const void* src, double* dst) -> int {
-    if (!dst) return PS2_OK;
-    CK(c->scratch.alloc(R * N));
-    CK(launch_scatter_rows(src, c->scratch.p, perm, N, R, c->st));
-    if (fp64) {
-      CK(cudaMemcpyAsync(dst, c->scratch.p, R * N, cudaMemcpyDeviceToHost, c->st));
-      CK(cudaStreamSynchronize(c->st));
-    } else {
-      std::vector<float> tmp(N);
-      CK(cudaMemcpyAsync(tmp.data(), c->scratch.p, R * N, cudaMemcpyDeviceToHost, c->st));
-      CK(cudaStreamSynchronize(c->st));
-      for (int64_t i = 0; i < N; ++i) dst[i] = static_cast<double>(tmp[i]);
+  // per-PS vectors: scattered to the caller's order and widened to f64 on the
+  // device, one slice of the scratch each, then copied straight into the
+  // caller's arrays (one synchronisation for all of them)
+  {
+    double* dsts[5] = {o->K_ps, o->C_ps, o->coh_ps, o->coh_ps_save, o->N_opt};
+    const void* srcs[5] = {c->K[0].p, c->C.p, c->coh.p, c->coh.p, c->nopt.p};
+    CK(c->scratch.alloc(sizeof(double) * 5 * N));
+    double* sc = c->scratch.as<double>();
+    for (int k = 0; k < 5; ++k) {
+      if (!dsts[k]) continue;
+      if (fp64 && k < 4)
+        CK(launch_scatter_rows(srcs[k], sc + k * N, perm, N, sizeof(double), c->st));
+      else
+        CK(launch_scatter_widen(srcs[k], k == 4, sc + k * N, perm, N, c->st));
+      CK(cudaMemcpyAsync(dsts[k], sc + k * N, sizeof(double) * N, cudaMemcpyDeviceToHost, c->st));
     }
-    return PS2_OK;
-  };
-  int rc;
-  if ((rc = fetch_vec(c->K[0].p, o->K_ps))) return rc;
-  if ((rc = fetch_vec(c->C.p, o->C_ps))) return rc;
-  if ((rc = fetch_vec(c->coh.p, o->coh_ps))) return rc;
-  if ((rc = fetch_vec(c->coh.p, o->coh_ps_save))) return rc;
-  if (o->N_opt) {
-    std::vector<uint8_t> sorted(N);
-    std::vector<int32_t> hperm(N);
-    CK(cudaMemcpyAsync(sorted.data(), c->nopt.p, N, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaMemcpyAsync(hperm.data(), perm, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
-    for (int64_t s = 0; s < N; ++s) o->N_opt[hperm[s]] = sorted[s] ? 1.0 : 0.0;
   }
   // residual phase and normalised patch phase: recomputed from the final
   // state by the same topofit code (deterministic, bit-identical values)

@@ -3801,6 +3801,31 @@ __global__ void k_scatter_narrow(const double* __restrict__ src, float* __restri
   }
 }
 
+// dst[perm[s]] = double(src[s]): a per-PS vector back in the caller's row
+// order, widened on the device (u8 flags as 0.0 / 1.0)
+__device__ __forceinline__ double widen_elem(const float* p, int64_t s) { return static_cast<double>(p[s]); }
+__device__ __forceinline__ double widen_elem(const uint8_t* p, int64_t s) { return p[s] ? 1.0 : 0.0; }
+template <typename T>
+__global__ void k_scatter_widen(const T* __restrict__ src, double* __restrict__ dst, const int32_t* __restrict__ perm,
+                                int64_t n) {
+  for (int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; s < n;
+       s += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    dst[perm[s]] = widen_elem(src, s);
+}
+
+cudaError_t launch_scatter_widen(const void* src, bool flags, double* dst, const int32_t* perm, int64_t n,
+                                 cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int64_t blocks = std::min<int64_t>((n + 255) / 256, 148 * 16);
+  if (flags)
+    k_scatter_widen<uint8_t><<<static_cast<unsigned>(blocks), 256, 0, st>>>(static_cast<const uint8_t*>(src), dst,
+                                                                             perm, n);
+  else
+    k_scatter_widen<float><<<static_cast<unsigned>(blocks), 256, 0, st>>>(static_cast<const float*>(src), dst, perm,
+                                                                           n);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_gather_widen(const float* src, double* dst, const int32_t* perm, int64_t n, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   const int64_t blocks = std::min<int64_t>((n + 255) / 256, 148 * 16);

@@ -217,6 +217,9 @@ cudaError_t launch_clap_bwd(const ClapBwdArgs& b, bool fp64, const Twiddles32f& 
                             int* blocks_out, cudaStream_t st);
 int clap_bwd_max_blocks(int sm_count, bool fp64);
 cudaError_t launch_gather_widen(const float* src, double* dst, const int32_t* perm, int64_t n, cudaStream_t st);
+// dst[perm[s]] = double(src[s]) for an f32 vector, or 0.0 / 1.0 for a u8 flag vector (flags)
+cudaError_t launch_scatter_widen(const void* src, bool flags, double* dst, const int32_t* perm, int64_t n,
+                                 cudaStream_t st);
 cudaError_t launch_scatter_narrow(const double* src, float* dst, const int32_t* perm, int64_t n, int64_t words,
                                   cudaStream_t st);
 cudaError_t launch_reduce_ab(const double* part, int n, double* out, cudaStream_t st);
