@@ -729,7 +729,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None
-    if world > 1:
+    # the shard mode takes the process group even for one rank when launched by
+    # torchrun (MASTER_ADDR set): the same NCCL all-reduce and exchange calls
+    if world > 1 or (args.shard and "MASTER_ADDR" in os.environ):
         import datetime
 
         import torch
