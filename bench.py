@@ -512,15 +512,16 @@ def run_ours(args, rank: int, world: int, dist):
                     "dgamma_max": float(d1.max()), "dgamma_p9999": float(np.quantile(d1, 0.9999)),
                     "n_dgamma_above_1e-4": int((d1 > 1e-4).sum()), "dK_m_p9999": float(np.nanquantile(dk1, 0.9999)),
                     "n_dK_above_1e-3_m": int((dk1 > 1e-3).sum()),
-                    "n_argmax_ties": int(cls["argmax_tie"].sum()), "n_wrap_ties": int(cls["wrap_tie"].sum()),
+                    "n_argmax_ties": int(cls["argmax_tie"].sum()), "n_fp32_near_ties": int(cls["near_tie"].sum()),
+                    "n_wrap_ties": int(cls["wrap_tie"].sum()),
                     "n_nontie_above_1e-4": int((d1[out_rows] > 1e-4)[nontie].sum()),
                     "n_nontie_above_1e-3_m": int((dk1[out_rows] > 1e-3)[nontie].sum()),
                     "nontie_dgamma_max": float(np.delete(d1, tie_rows).max()),
                     "nontie_dK_m_max": float(np.nanmax(np.delete(dk1, tie_rows))),
                     "note": "PS above the bounds classified by an FP64 trial search of their rows "
                             "(pystamps_b200.precision.classify_ties): argmax ties (best and runner-up trial "
-                            "within 1e-6 of max(best, 0.5)) and refinement wrap ties (a residual angle within 1e-4 rad "
-                            "of +-pi)"},
+                            "within 1e-6 relative), FP32 near ties (within 1e-6 of max(best, 0.5), not argmax "
+                            "ties) and refinement wrap ties (a residual angle within 1e-4 rad of +-pi)"},
                 "converged": {"iterations_fp32": a["i_loop"], "iterations_fp64": b["i_loop"],
                               "dgamma_median": float(np.median(d)), "dgamma_p99": float(np.quantile(d, 0.99)),
                               "dgamma_max": float(d.max()), "dK_m_median": float(np.nanmedian(dk)),

@@ -20,19 +20,27 @@ import numpy as np
 from . import stage2 as S
 from . import synth
 
-ARGMAX_TIE_REL = 1e-6    # best and runner-up trial coherence this close (relative): an argmax tie ...
-ARGMAX_TIE_FLOOR = 0.5   # ... taken relative to max(best, 0.5): an FP32 trial coherence carries an
-                         # error of roughly fixed size (its phasor and summation rounding over the
-                         # columns), so below coherence 0.5 the rule is an absolute 5e-7
+ARGMAX_TIE_REL = 1e-6    # best and runner-up trial coherence this close (relative): an argmax tie
+NEAR_TIE_FLOOR = 0.5     # FP32 near tie: within ARGMAX_TIE_REL of max(best, 0.5) but not an argmax
+                         # tie: an FP32 trial coherence carries an error of roughly fixed size (its
+                         # phasor and summation rounding over the columns), so below coherence 0.5 such
+                         # rows (an absolute gap under 5e-7) flip as easily; counted separately
 WRAP_TIE_RAD = 1e-4      # a refinement residual angle this close to +-pi: a wrap tie
 
 
 def is_argmax_tie(best, second):
-    """Best and runner-up trial coherence within ARGMAX_TIE_REL of max(best,
-    ARGMAX_TIE_FLOOR): an FP32 evaluation of the trials may pick either (for
-    example two trials at 0.23912255 and 0.23912231 of a 2,000,000 x 150 patch)."""
+    """Best and runner-up trial coherence within ARGMAX_TIE_REL relative."""
     best = np.asarray(best, np.float64)
-    return (best - np.asarray(second, np.float64)) <= ARGMAX_TIE_REL * np.maximum(best, ARGMAX_TIE_FLOOR)
+    return (best - np.asarray(second, np.float64)) <= ARGMAX_TIE_REL * np.maximum(best, 1e-30)
+
+
+def is_fp32_tie(best, second):
+    """Argmax ties and FP32 near ties: best and runner-up within ARGMAX_TIE_REL
+    of max(best, NEAR_TIE_FLOOR). An FP32 evaluation of the trials may pick
+    either (for example two trials at 0.23912255 and 0.23912231, 1.007e-6
+    relative, of a 2,000,000 x 150 patch)."""
+    best = np.asarray(best, np.float64)
+    return (best - np.asarray(second, np.float64)) <= ARGMAX_TIE_REL * np.maximum(best, NEAR_TIE_FLOOR)
 
 
 def trial_values(n_trial_wraps: float) -> np.ndarray:
@@ -81,7 +89,8 @@ def wrap_distance(ph_nm, ph_patch, bperp, n_trial_wraps: float, best_ix=None) ->
 
 def classify_ties(ph_nm, ph_patch, bperp, n_trial_wraps: float) -> dict:
     """Tie classes of the given rows (few rows: every trial in FP64):
-    argmax ties (best and runner-up trial within is_argmax_tie) and
+    argmax ties (best and runner-up trial within 1e-6 relative), FP32 near
+    ties (within 1e-6 of max(best, 0.5) but not argmax ties) and
     wrap ties (a refinement residual angle within WRAP_TIE_RAD of +-pi). Rows
     that are neither are genuine FP32/FP64 differences."""
     ph_nm = np.atleast_2d(ph_nm)
@@ -90,14 +99,16 @@ def classify_ties(ph_nm, ph_patch, bperp, n_trial_wraps: float) -> dict:
     bp = bp[None, :] if bp.ndim == 1 else np.atleast_2d(bp)
     if ph_nm.shape[0] == 0:
         e = np.zeros(0, bool)
-        return {"argmax_tie": e, "wrap_tie": e, "tie": e}
+        return {"argmax_tie": e, "near_tie": e, "wrap_tie": e, "tie": e}
     coh = trial_coherences(ph_nm, ph_patch, bp, n_trial_wraps)
     srt = np.sort(coh, axis=1)
     best = srt[:, -1]
     second = srt[:, -2] if coh.shape[1] > 1 else np.zeros(coh.shape[0])
     argmax_tie = is_argmax_tie(best, second)
+    near_tie = is_fp32_tie(best, second) & ~argmax_tie
     wrap_tie = wrap_distance(ph_nm, ph_patch, bp, n_trial_wraps, np.argmax(coh, axis=1)) < WRAP_TIE_RAD
-    return {"argmax_tie": argmax_tie, "wrap_tie": wrap_tie, "tie": argmax_tie | wrap_tie}
+    return {"argmax_tie": argmax_tie, "near_tie": near_tie, "wrap_tie": wrap_tie,
+            "tie": argmax_tie | near_tie | wrap_tie}
 
 
 def study(prep: S.PreparedPatch, k_to_m: float, iterations: int = 8, device: int = 0) -> list[dict]:
