@@ -405,18 +405,30 @@ class Stage2Context:
     def launch_count(self) -> int:
         return int(self._lib.ps2_last_launch_count(self._ctx))
 
-    def download(self, keys=None) -> dict:
-        """pm1.mat variables (native_stage2.rs:1899-1965) in the caller's row order."""
+    def download(self, keys=None, out=None) -> dict:
+        """pm1.mat variables (native_stage2.rs:1899-1965) in the caller's row order.
+        out: optional arrays to fill for the per-PS vectors (K_ps, C_ps,
+        coh_ps, N_opt, coh_ps_save: float64, C-contiguous, n_ps long), for
+        callers that reuse (for example pinned) host buffers across patches."""
         p = self.prepared
         n, m = p.n_ps, p.n_ifg
         fp64 = self.precision == PRECISION_FP64
         want = set(keys) if keys else {"K_ps", "C_ps", "coh_ps", "N_opt", "ph_res", "ph_patch", "ph_grid",
                                         "ph_weight", "coh_ps_save", "Nr"}
+        given = out or {}
         out = {}
         o = _lib.Outputs()
         for k in ("K_ps", "C_ps", "coh_ps", "N_opt", "coh_ps_save"):
             if k in want:
-                out[k] = np.empty(n, dtype=np.float64)
+                g = given.get(k)
+                if g is not None:
+                    if not (isinstance(g, np.ndarray) and g.dtype == np.float64 and g.shape == (n,)
+                            and g.flags.c_contiguous and g.flags.writeable):
+                        raise ValueError(f"download: out[{k!r}] must be a writeable C-contiguous float64 array "
+                                         f"of length {n}")
+                    out[k] = g
+                else:
+                    out[k] = np.empty(n, dtype=np.float64)
                 setattr(o, k, ptr(out[k]))
         cdt, rdt = (np.complex128, np.float64) if fp64 else (np.complex64, np.float32)
         suffix = "_f64" if fp64 else ""

@@ -121,3 +121,20 @@ def test_debug_pm_dumps_one_file_per_iteration(S, patch, tmp_path, monkeypatch):
         np.testing.assert_array_equal(last[k], final[k], err_msg=k)
         np.testing.assert_array_equal(final[k], plain[k], err_msg=k)
     assert int(loadmat(d / "pm1_iter_01.mat")["i_loop"].reshape(-1)[0]) == 1
+
+
+def test_download_into_caller_buffers(S, prep):
+    """download(out=...) fills the caller's float64 arrays (reused, e.g. pinned,
+    host buffers) with the values a plain download returns; wrong buffers are refused."""
+    keys = ["K_ps", "C_ps", "coh_ps", "N_opt"]
+    with S.Stage2Context() as c:
+        c.load(prep)
+        c.iterate(2)
+        ref = c.download(keys)
+        bufs = {k: np.full(prep.n_ps, 7.0) for k in keys}
+        got = c.download(keys, out=bufs)
+        for k in keys:
+            assert got[k] is bufs[k]
+            np.testing.assert_array_equal(bufs[k], ref[k], err_msg=k)
+        with pytest.raises(ValueError, match="float64 array"):
+            c.download(["K_ps"], out={"K_ps": np.zeros(prep.n_ps, np.float32)})
