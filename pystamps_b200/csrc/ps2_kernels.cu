@@ -1109,14 +1109,16 @@ cudaError_t launch_overlap(const OverlapArgs& a, bool fp64, cudaStream_t st) {
 // =============================================================== topofit ==
 // One group of L lanes per PS (L = 4, 8, 16 or 32, chosen from the number of
 // interferograms so a lane owns about 5-10 columns); a warp holds 32/L PS.
-// Column data (psdph z_c, theta_c = bp_c/range*pi/4, e^{-j theta_c}, bp_c)
-// live in shared memory. The trial sweep evaluates
-//   S_m = sum_c z_c e^{-j theta_c m}
-// for the trial pairs +-m, 16 magnitudes |m| at a time (sweep_trial_pairs): the
-// phasor e^{-j theta m} is anchored exactly at the first magnitude of the block
-// and advanced by a complex recurrence, two trials per packed FP32x2 value, so
-// it is re-anchored every 16 steps; the group then reduces its 32 partial sums
-// with a transposing butterfly, each lane ending with 32/L of the trials.
+// Column data (psdph z_c, the per-step rotation, bp_c) live in shared memory.
+// The trial sweep finds the first argmax over the trials of |S_m|,
+//   S_m = sum_c z_c e^{-j theta_c m},  theta_c = bp_c / range * pi/4,
+// 16 magnitudes |m| at a time with the trial pairs +-m sharing one phasor
+// chain, two trials per packed FP32x2 value, the chain started exactly in the
+// middle of the block and run both ways by the three-term recurrence; the group
+// then reduces its partial sums with a transposing butterfly. For n_half in
+// 41 .. 87 it is sampled (sampled_sweep): the centred sum is evaluated at every
+// 4th trial and interpolated between; otherwise every magnitude is swept
+// (sweep_trial_pairs).
 
 constexpr float kQuarterPiF = 3.14159265358979323846f / 4.0f;  // Rust std::f32::consts::PI / 4.0
 
