@@ -135,7 +135,7 @@ def test_topofit_zero_columns_and_empty_rows(K, oracle):
 # n_half = ceil(8 ntw): 40 and 88 take the full trial sweep, 41 .. 87 the
 # sampled one (every 4th trial exact, fractional-delay filters between)
 @pytest.mark.parametrize("m,ntw", [(20, 4.94), (60, 9.94), (150, 9.94), (3, 0.4), (33, 1.0), (60, 5.1),
-                                   (150, 10.8), (150, 10.9), (47, 7.6)])
+                                   (150, 10.8), (150, 10.9), (47, 7.6), (3, 9.94), (5, 10.8)])
 def test_topofit_random_rows_argmax_and_ties(K, oracle, m, ntw):
     rng = np.random.default_rng(m)
     n = 4000
