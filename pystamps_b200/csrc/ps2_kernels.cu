@@ -1487,7 +1487,7 @@ __device__ __forceinline__ void sweep_sample_block(const ColumnSmem& cs, const f
     R[i] = make_float2(0.f, 0.f);
     U[i] = make_float2(0.f, 0.f);
   }
-#pragma unroll 2
+#pragma unroll 3
   for (int k = 0; k < ncl; ++k) {
     const int c = gl + L * k;
     const float x = cs.zx[c], y = cs.zy[c], rx = cs.rx[c], ry = cs.ry[c];
